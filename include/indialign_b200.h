@@ -1,0 +1,141 @@
+/* indialign_b200 -- B200 (sm_100a) implementation of INDIalign's RNA TM-score
+ * superposition search, behind the reference's C ABI.
+ *
+ * The first four entry points and the three structs are drop-ins for the
+ * reference's (indialign_c/api.h:10-46): same names, field order and sizes
+ * (x86-64: 56 / 56 / 104 bytes), same argument meaning and return codes.
+ * Differences a caller can see:
+ *   - the search runs on the GPU; request_cuda and backend_mode are ignored
+ *     (there is no CPU path and no CPU fallback);
+ *   - a CUDA failure returns a negative code (INDIALIGN_E_*) instead of
+ *     silently falling back; the reference has no such case.
+ * Ownership is unchanged: all pointers are caller-owned host memory, the
+ * library reads 3N doubles per coordinate array and N bytes per mask and
+ * writes only *out / outputs[].  Calls are thread-safe (each call takes its
+ * own stream and workspace from an internal pool).
+ */
+#ifndef INDIALIGN_B200_H
+#define INDIALIGN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Replaces NativeConfig (indialign_c/api.h:10-20). */
+typedef struct {
+    int backend_mode;        /* ignored (the reference ignores it too) */
+    int use_fragment_search;
+    int max_iter;
+    int dp_iter;
+    double max_mem_gb;       /* device workspace budget per call */
+    int request_cuda;        /* ignored: always CUDA */
+    double rescue_score_1;   /* trigger rescue if score < this (default 0.5) */
+    double rescue_score_2;   /* trigger dense rescue if score < this (default 0.3) */
+    double early_term_score; /* skip remaining seeds if score >= this (default 0.99) */
+} NativeConfig;
+
+/* Replaces NativePairInput (indialign_c/api.h:22-30). */
+typedef struct {
+    int length;
+    const double *pred_xyz;          /* 3*length, xyz interleaved */
+    const double *native_xyz;        /* 3*length */
+    const uint8_t *valid_mask;       /* length; expected pred_valid & native_valid */
+    const uint8_t *pred_valid_mask;  /* length */
+    const uint8_t *native_valid_mask;/* length */
+    double lnorm;                    /* TM normalisation length */
+} NativePairInput;
+
+/* Replaces NativePairResult (indialign_c/api.h:32-36).  aligned_d =
+ * sum_k pred_k * rotation[3k+d] + translation[d]. */
+typedef struct {
+    double score;
+    double rotation[9];
+    double translation[3];
+} NativePairResult;
+
+enum {
+    INDIALIGN_OK = 0,
+    INDIALIGN_E_LENGTH = -1,   /* length <= 0 (reference behaviour) */
+    INDIALIGN_E_NODEVICE = -2, /* no usable CUDA device */
+    INDIALIGN_E_CUDA = -3,     /* CUDA runtime error (see indialign_last_error) */
+    INDIALIGN_E_INPUT = -4,    /* null pointer or length above 65535 */
+    INDIALIGN_E_DEVICE = -5,   /* device-side error flag (bounded wait / capacity) */
+    INDIALIGN_E_INJECTED = -6  /* failure injected by the test hook */
+};
+
+/* Replaces indialign_default_config (indialign_c/indialign.cpp:272-282). */
+void indialign_default_config(NativeConfig *cfg);
+
+/* Replaces indialign_tmscore_search (indialign_c/indialign.cpp:284-303).
+ * Returns -1 iff length <= 0 (out untouched), 0 on success, another
+ * negative INDIALIGN_E_* code on a CUDA failure (out untouched). */
+int indialign_tmscore_search(const NativePairInput *inp, const NativeConfig *cfg,
+                             NativePairResult *out);
+
+/* Replaces indialign_tmscore_search_batch (indialign_c/indialign.cpp:305-313).
+ * All pairs run in one device pass.  Pairs with length <= 0 are skipped and
+ * their outputs left untouched, as the reference does.  Returns 0, or a
+ * negative code on a CUDA failure (then no output is written). */
+int indialign_tmscore_search_batch(int n_pairs, const NativePairInput *inputs,
+                                   const NativeConfig *cfg, NativePairResult *outputs);
+
+/* Replaces indialign_cuda_available (indialign_c/indialign.cpp:315-321):
+ * 1 when a CUDA device of compute capability 10.x is usable, else 0. */
+int indialign_cuda_available(void);
+
+/* ---- extensions (no counterpart in the reference's api.h) -------------- */
+
+/* Per-call options for the batched entry points.  Zero-initialise. */
+typedef struct {
+    void *stream;            /* cudaStream_t to run on (NULL: library stream) */
+    int device;              /* CUDA device ordinal (-1: current) */
+    int use_graph;           /* capture the stage sequence in a CUDA graph and replay it */
+    int profile;             /* 1: print per-stage device times to stderr */
+    double *stage_ms;        /* optional [INDIALIGN_STAGES] per-stage device ms */
+    long long *counters;     /* optional [INDIALIGN_COUNTERS] work counters */
+    double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
+                                best {score,R,t} after each search stage */
+} IndialignBatchOptions;
+
+/* Stages recorded in stage_best, in search order: seed bank, SS seeds,
+ * gapless threading, local fragment DP, threading DP, dense local fragment
+ * DP, top-k seed, DP refinement, offset DP, weighted refinement. */
+#define INDIALIGN_TRACE_STAGES 10
+
+#define INDIALIGN_STAGES 12
+#define INDIALIGN_COUNTERS 8
+
+/* Batched search with per-call options.  Same inputs and outputs as
+ * indialign_tmscore_search_batch. */
+int indialign_tmscore_search_batch_ex(int n_pairs, const NativePairInput *inputs,
+                                      const NativeConfig *cfg,
+                                      const IndialignBatchOptions *opts,
+                                      NativePairResult *outputs);
+
+/* Device-resident batch: pairs packed back to back on the device.
+ * off[n+1] residue offsets (host array), d_pred/d_nat [3*total] doubles,
+ * d_v/d_pv/d_nv [total] bytes, lnorm[n] (host array); results written to
+ * d_out [n*13] doubles on the device ({score, R[9], t[3]} per pair).  Used by
+ * the torch shim; every pointer named d_* is device memory. */
+int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d_pred,
+                                    const double *d_nat, const uint8_t *d_v,
+                                    const uint8_t *d_pv, const uint8_t *d_nv,
+                                    const double *lnorm, const NativeConfig *cfg,
+                                    const IndialignBatchOptions *opts, double *d_out);
+
+/* Text of the last error on this thread ("" if none). */
+const char *indialign_last_error(void);
+
+/* Test hook: make the next `count` calls fail with INDIALIGN_E_INJECTED
+ * before any device work, to exercise callers' failure paths without a GPU
+ * fault.  0 disarms. */
+void indialign_inject_failure(int count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

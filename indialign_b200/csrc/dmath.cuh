@@ -1,0 +1,240 @@
+// FP64 device math shared by every kernel of the search: the d0 schedule,
+// the Horn-quaternion Kabsch solve (cyclic 4x4 Jacobi), rigid transforms and
+// TM terms.  The eigen-solve keeps the reference's exact sweep schedule
+// (indialign_c/core.h:29-90) so that the rotation returned for a covariance
+// matches the reference's to rounding; covariances are formed from raw
+// moments accumulated in one pass (sum p, sum q, sum p q^T, count) instead of
+// the reference's centroid pass + centred pass (core.h:94-123), which is the
+// same matrix up to FP64 rounding and lets a selection pass and its Kabsch
+// fuse into a single sweep over the residues.
+#pragma once
+#include <stdint.h>
+
+#define IA_DEV __device__ __forceinline__
+
+namespace ia {
+
+__constant__ static const double kD0Mults[6] = {2.0, 1.5, 1.0, 0.75, 0.5, 0.25};
+
+// d0, d0_search and score_d8 from the normalisation length
+// (indialign_c/core.h:12-25).
+IA_DEV void d0_from_length(double L, double &d0, double &d0s, double &sd8) {
+    double Lc = L > 1.0 ? L : 1.0;
+    if (Lc <= 11.0) d0 = 0.3;
+    else if (Lc <= 15.0) d0 = 0.4;
+    else if (Lc <= 19.0) d0 = 0.5;
+    else if (Lc <= 23.0) d0 = 0.6;
+    else d0 = 0.7;
+    if (Lc >= 30.0) d0 = 0.6 * sqrt(Lc - 0.5) - 2.5;
+    if (d0 < 0.3) d0 = 0.3;
+    double m = Lc - 15.0 > 0.0 ? Lc - 15.0 : 0.0;
+    double v = 1.24 * cbrt(m) - 1.8;
+    d0s = v < 4.5 ? 4.5 : (v > 8.0 ? 8.0 : v);
+    sd8 = 1.5 * pow(Lc, 0.3) + 3.5;
+}
+
+// Cutoff list: d0s x {2,1.5,1,.75,.5,.25}, then d0+{1..5} unless within 0.01
+// of an earlier entry (indialign_c/indialign.cpp:54-67).  Returns C <= 11.
+IA_DEV int d0_candidates(double d0, double d0s, double *cand) {
+    int C = 0;
+    for (int c = 0; c < 6; c++) cand[C++] = d0s * kD0Mults[c];
+    for (int c = 1; c <= 5; c++) {
+        double v = d0 + (double)c;
+        bool dup = false;
+        for (int e = 0; e < C; e++) dup |= fabs(cand[e] - v) < 0.01;
+        if (!dup) cand[C++] = v;
+    }
+    return C;
+}
+
+struct Rt {
+    double R[9], t[3];
+};
+
+IA_DEV void set_identity(double *R, double *t) {
+#pragma unroll
+    for (int i = 0; i < 9; i++) R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+    t[0] = t[1] = t[2] = 0.0;
+}
+
+// aligned_d = sum_k p_k R[3k+d] + t_d (indialign_c/core.h:127-132)
+IA_DEV void xform(const double *R, const double *t, double px, double py,
+                  double pz, double &mx, double &my, double &mz) {
+    mx = px * R[0] + py * R[3] + pz * R[6] + t[0];
+    my = px * R[1] + py * R[4] + pz * R[7] + t[1];
+    mz = px * R[2] + py * R[5] + pz * R[8] + t[2];
+}
+
+IA_DEV double dist2(const double *R, const double *t, double px, double py,
+                    double pz, double qx, double qy, double qz) {
+    double mx, my, mz;
+    xform(R, t, px, py, pz, mx, my, mz);
+    double dx = mx - qx, dy = my - qy, dz = mz - qz;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+// One Jacobi rotation of the pair (p,q), skipped when |A[p][q]| < 1e-15
+// (indialign_c/core.h:39-58).  Indices are compile-time so A and V stay in
+// registers.
+template <int p, int q>
+IA_DEV void jacobi_rot(double (&A)[4][4], double (&V)[4][4]) {
+    double apq = A[p][q];
+    if (fabs(apq) < 1e-15) return;
+    double tau = (A[q][q] - A[p][p]) / (2.0 * apq);
+    double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+    double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
+    A[p][p] -= t * apq;
+    A[q][q] += t * apq;
+    A[p][q] = A[q][p] = 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        if (r == p || r == q) continue;
+        double rp = A[r][p], rq = A[r][q];
+        A[r][p] = A[p][r] = c * rp - s * rq;
+        A[r][q] = A[q][r] = s * rp + c * rq;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        double vp = V[r][p], vq = V[r][q];
+        V[r][p] = c * vp - s * vq;
+        V[r][q] = s * vp + c * vq;
+    }
+}
+
+// Horn's 4x4 from the 3x3 covariance H, 8 cyclic Jacobi sweeps, dominant
+// eigenvector (first index on ties) -> rotation (indialign_c/core.h:64-90).
+IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
+    double A[4][4], V[4][4];
+    A[0][0] = H[0][0] + H[1][1] + H[2][2];
+    A[0][1] = A[1][0] = H[1][2] - H[2][1];
+    A[0][2] = A[2][0] = H[2][0] - H[0][2];
+    A[0][3] = A[3][0] = H[0][1] - H[1][0];
+    A[1][1] = H[0][0] - H[1][1] - H[2][2];
+    A[1][2] = A[2][1] = H[0][1] + H[1][0];
+    A[1][3] = A[3][1] = H[2][0] + H[0][2];
+    A[2][2] = -H[0][0] + H[1][1] - H[2][2];
+    A[2][3] = A[3][2] = H[1][2] + H[2][1];
+    A[3][3] = -H[0][0] - H[1][1] + H[2][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
+#pragma unroll 1
+    for (int sweep = 0; sweep < 8; sweep++) {
+        jacobi_rot<0, 1>(A, V);
+        jacobi_rot<0, 2>(A, V);
+        jacobi_rot<0, 3>(A, V);
+        jacobi_rot<1, 2>(A, V);
+        jacobi_rot<1, 3>(A, V);
+        jacobi_rot<2, 3>(A, V);
+    }
+    int best = 0;
+    double bv = A[0][0];
+    if (A[1][1] > bv) { best = 1; bv = A[1][1]; }
+    if (A[2][2] > bv) { best = 2; bv = A[2][2]; }
+    if (A[3][3] > bv) { best = 3; bv = A[3][3]; }
+    double q0, q1, q2, q3;
+    // select the column without dynamic register indexing
+    q0 = best == 0 ? V[0][0] : best == 1 ? V[0][1] : best == 2 ? V[0][2] : V[0][3];
+    q1 = best == 0 ? V[1][0] : best == 1 ? V[1][1] : best == 2 ? V[1][2] : V[1][3];
+    q2 = best == 0 ? V[2][0] : best == 1 ? V[2][1] : best == 2 ? V[2][2] : V[2][3];
+    q3 = best == 0 ? V[3][0] : best == 1 ? V[3][1] : best == 2 ? V[3][2] : V[3][3];
+    double qn = sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+    if (qn < 1e-12) {
+        q0 = 1; q1 = q2 = q3 = 0;
+    } else {
+        q0 /= qn; q1 /= qn; q2 /= qn; q3 /= qn;
+    }
+    R[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3;
+    R[1] = 2 * (q1 * q2 + q0 * q3);
+    R[2] = 2 * (q1 * q3 - q0 * q2);
+    R[3] = 2 * (q1 * q2 - q0 * q3);
+    R[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3;
+    R[5] = 2 * (q2 * q3 + q0 * q1);
+    R[6] = 2 * (q1 * q3 + q0 * q2);
+    R[7] = 2 * (q2 * q3 - q0 * q1);
+    R[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+}
+
+// Raw first and second moments of a selected point set.
+struct Moments {
+    double sp[3], sq[3], h[9], w;
+    IA_DEV void clear() {
+#pragma unroll
+        for (int i = 0; i < 3; i++) sp[i] = sq[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; i++) h[i] = 0.0;
+        w = 0.0;
+    }
+    IA_DEV void add(double px, double py, double pz, double qx, double qy,
+                    double qz) {
+        sp[0] += px; sp[1] += py; sp[2] += pz;
+        sq[0] += qx; sq[1] += qy; sq[2] += qz;
+        h[0] += px * qx; h[1] += px * qy; h[2] += px * qz;
+        h[3] += py * qx; h[4] += py * qy; h[5] += py * qz;
+        h[6] += pz * qx; h[7] += pz * qy; h[8] += pz * qz;
+        w += 1.0;
+    }
+    IA_DEV void add_w(double wi, double px, double py, double pz, double qx,
+                      double qy, double qz) {
+        double wx = wi * px, wy = wi * py, wz = wi * pz;
+        sp[0] += wx; sp[1] += wy; sp[2] += wz;
+        sq[0] += wi * qx; sq[1] += wi * qy; sq[2] += wi * qz;
+        h[0] += wx * qx; h[1] += wx * qy; h[2] += wx * qz;
+        h[3] += wy * qx; h[4] += wy * qy; h[5] += wy * qz;
+        h[6] += wz * qx; h[7] += wz * qy; h[8] += wz * qz;
+        w += wi;
+    }
+    // Butterfly sum over the lanes of `width` (power of two) so that every
+    // lane of the group ends with the group total.
+    IA_DEV void group_sum(int width) {
+        for (int o = 1; o < width; o <<= 1) {
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                sp[i] += __shfl_xor_sync(0xffffffffu, sp[i], o);
+                sq[i] += __shfl_xor_sync(0xffffffffu, sq[i], o);
+            }
+#pragma unroll
+            for (int i = 0; i < 9; i++) h[i] += __shfl_xor_sync(0xffffffffu, h[i], o);
+            w += __shfl_xor_sync(0xffffffffu, w, o);
+        }
+    }
+};
+
+// Kabsch from moments: identity when the weight is below `min_w`
+// (3 points for the plain Kabsch, 1e-12 for the weighted one).
+IA_DEV void kabsch_from_moments(const Moments &m, double min_w, double *R,
+                                double *t) {
+    if (m.w < min_w) {
+        set_identity(R, t);
+        return;
+    }
+    double cP[3], cQ[3], H[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        cP[d] = m.sp[d] / m.w;
+        cQ[d] = m.sq[d] / m.w;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) H[r][c] = m.h[r * 3 + c] - m.sp[r] * cQ[c];
+    cov_to_rotation(H, R);
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+        t[d] = cQ[d] - (cP[0] * R[d] + cP[1] * R[3 + d] + cP[2] * R[6 + d]);
+}
+
+IA_DEV double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+IA_DEV int warp_sum_int(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace ia

@@ -1,0 +1,458 @@
+// NW chains: score matrix + Needleman-Wunsch + traceback + Kabsch + the
+// detailed seed search on the alignment, one warp per chain.
+//
+// Restates nw_dp / nw_traceback (indialign_c/nw.h:10-68), dp_refine_chunk
+// (indialign_c/align.h:54-145) and the score matrices of ss_nw_align /
+// evaluate_ss_seeds (indialign_c/ss.h:56-164).
+//
+// NW layout: the warp sweeps horizontal stripes of 32 rows; lane l owns row
+// s0+l+1 and computes column j at step j+l-1, so each step is one
+// anti-diagonal of the stripe.  H[i-1][j] arrives from lane l-1 by a warp
+// shuffle (lane 0 reads the stripe's top boundary row from memory, written
+// by lane 31 of the previous stripe), H[i][j-1] is the lane's own previous
+// value.  The "reached diagonally" bit that gates the gap penalty travels in
+// the sign bit of H (H >= 0 always; -0.0 encodes a diagonal zero).  Score
+// entries are computed on the fly from the transformed pred row held in
+// registers and the native column in shared memory, never stored.  Trace
+// directions (2 bits/cell) go to a per-warp global scratch block, which stays
+// L2-resident for the sizes of interest, and the traceback walks 32x16-cell
+// tiles held in registers (one coalesced load per tile, shuffles inside).
+#include "dmath.cuh"
+#include "stage.cuh"
+#include "pipeline.h"
+#include "kernels.h"
+#include "sched.cuh"
+
+namespace ia {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---- warp helpers ----------------------------------------------------------
+struct Pts {
+    const double *P;  // pred compact xyz
+    const double *Q;  // native compact xyz
+};
+
+// Kabsch over pairs (P[a+i], Q[b+i]), i < cnt (a window), by the warp.
+IA_DEV void warp_kabsch_window(const Pts &x, int a, int b, int cnt, double *R, double *t) {
+    Moments m;
+    m.clear();
+    for (int i = threadIdx.x & 31; i < cnt; i += 32) {
+        const double *p = x.P + 3 * (a + i), *q = x.Q + 3 * (b + i);
+        m.add(p[0], p[1], p[2], q[0], q[1], q[2]);
+    }
+    m.group_sum(32);
+    kabsch_from_moments(m, 3.0, R, t);
+}
+
+// Aligned pair k (forward order) from the reversed traceback list.
+IA_DEV void al_get(const uint32_t *al, int na, int k, int &pi, int &ni) {
+    uint32_t e = al[na - 1 - k];
+    pi = (int)(e >> 16);
+    ni = (int)(e & 0xffffu);
+}
+
+struct NWParams {
+    int plen, nlen;
+    int smode;
+    double gap;
+    double inv_d0sq;  // 1/d0^2 of the score matrix
+    double cut2;      // SMAT_DP: score only if d2 <= cut2
+    const uint8_t *Lp, *Ln;  // SS labels (compact order)
+};
+
+// Fill the trace of the NW DP for (R,t) and return the aligned pair count;
+// the pairs are written (reversed) to al.
+IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
+                    double *bH, uint32_t *trace, uint32_t *al) {
+    const int lane = threadIdx.x & 31;
+    const int plen = pr.plen, nlen = pr.nlen;
+    const int wpr = (nlen + 15) >> 4;
+    for (int j = lane; j <= nlen; j += 32) bH[j] = 0.0;
+    __syncwarp();
+    for (int s0 = 0; s0 < plen; s0 += 32) {
+        const int i = s0 + lane + 1;
+        const bool row_ok = i <= plen;
+        double mx = 0, my = 0, mz = 0;
+        uint8_t lp = 0;
+        if (row_ok) {
+            const double *p = x.P + 3 * (i - 1);
+            if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], mx, my, mz);
+            if (pr.smode != SMAT_DP) lp = pr.Lp[i - 1];
+        }
+        const bool last = s0 + 32 >= plen;
+        double h_enc = 0.0, up_prev = 0.0;
+        uint32_t acc = 0;
+        uint32_t *trow = trace + (size_t)(i - 1) * wpr;
+        const int nsteps = nlen + 31;
+        for (int step = 0; step < nsteps; step++) {
+            const int j = step - lane + 1;
+            double up_enc = __shfl_up_sync(kFull, h_enc, 1);
+            const bool jok = j >= 1 && j <= nlen;
+            if (lane == 0) up_enc = jok ? bH[j] : 0.0;
+            if (row_ok && jok) {
+                double sc;
+                if (pr.smode == SMAT_SS2) {
+                    sc = (lp == pr.Ln[j - 1]) ? 1.0 : 0.0;
+                } else {
+                    const double *q = x.Q + 3 * (j - 1);
+                    const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    if (pr.smode == SMAT_DP) {
+                        sc = d2 <= pr.cut2 ? 1.0 / (1.0 + d2 * pr.inv_d0sq) : 0.0;
+                    } else {
+                        sc = 1.0 / (1.0 + d2 * pr.inv_d0sq);
+                        if (lp == pr.Ln[j - 1]) sc += 0.5;
+                    }
+                }
+                const double up_v = fabs(up_enc), hl_v = fabs(h_enc);
+                const double diag = up_prev + sc;
+                const double up = up_v + (signbit(up_enc) ? pr.gap : 0.0);
+                const double left = hl_v + (signbit(h_enc) ? pr.gap : 0.0);
+                double nh;
+                uint32_t dir;
+                if (diag >= up && diag >= left) { nh = diag; dir = 0; }
+                else if (left >= up) { nh = left; dir = 2; }
+                else { nh = up; dir = 1; }
+                h_enc = dir == 0 ? -nh : nh;
+                up_prev = up_v;
+                const int jj = j - 1;
+                acc |= dir << (2 * (jj & 15));
+                if ((jj & 15) == 15 || j == nlen) {
+                    trow[jj >> 4] = acc;
+                    acc = 0;
+                }
+                if (lane == 31 && !last) bH[j] = h_enc;
+            }
+        }
+        __syncwarp();
+    }
+    // traceback from (plen, nlen): diag emits a pair, up steps i, else j
+    int i = plen, j = nlen, cnt = 0, rb = -1, cw = -1;
+    uint32_t word = 0;
+    while (i > 0 && j > 0) {
+        const int w = (j - 1) >> 4;
+        if (w != cw || i > rb || i <= rb - 32) {
+            rb = i;
+            cw = w;
+            const int r = rb - lane;
+            word = r >= 1 ? trace[(size_t)(r - 1) * wpr + w] : 0u;
+        }
+        const uint32_t rw = __shfl_sync(kFull, word, rb - i);
+        const uint32_t dir = (rw >> (2 * ((j - 1) & 15))) & 3u;
+        if (dir == 0) {
+            if (lane == 0) al[cnt] = ((uint32_t)(i - 1) << 16) | (uint32_t)(j - 1);
+            cnt++;
+            i--;
+            j--;
+        } else if (dir == 1) {
+            i--;
+        } else {
+            j--;
+        }
+    }
+    __syncwarp();
+    return cnt;
+}
+
+// Kabsch on the aligned pairs + their compact TM (no d8)
+// (indialign_c/align.h:106-124).
+IA_DEV double aligned_kabsch(const Pts &x, const uint32_t *al, int na, double d0, double lnorm,
+                             double *R, double *t) {
+    const int lane = threadIdx.x & 31;
+    Moments m;
+    m.clear();
+    for (int k = lane; k < na; k += 32) {
+        int pi, ni;
+        al_get(al, na, k, pi, ni);
+        const double *p = x.P + 3 * pi, *q = x.Q + 3 * ni;
+        m.add(p[0], p[1], p[2], q[0], q[1], q[2]);
+    }
+    m.group_sum(32);
+    kabsch_from_moments(m, 3.0, R, t);
+    const double d0sq = fmax(d0 * d0, 1e-12);
+    double s = 0.0;
+    for (int k = lane; k < na; k += 32) {
+        int pi, ni;
+        al_get(al, na, k, pi, ni);
+        const double *p = x.P + 3 * pi, *q = x.Q + 3 * ni;
+        s += 1.0 / (1.0 + dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]) / d0sq);
+    }
+    return warp_sum(s) / fmax(lnorm, 1.0);
+}
+
+// alignment_detailed_search without fragments (indialign_c/align.h:15-50,
+// use_frag = false): one all-pairs seed x 6 cutoffs x <= 8 iterations,
+// d8-filtered score.  The all-pairs seed's Kabsch is the (R0,t0) just
+// computed by aligned_kabsch.  Lane groups of 4 run the 6 cutoffs side by
+// side; the first maximum in cutoff order wins.
+IA_DEV double lite_detailed(const Pts &x, const uint32_t *al, int na, const double *R0,
+                            const double *t0, const double *dcut, double d0, double sd8,
+                            double lnorm, double *Ro, double *to) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, sub = lane & 3;
+    const bool grp = g < kDetC;
+    const double cut = dcut[grp ? g : 0];
+    const double cut2 = cut * cut;
+    double R[9], t[3];
+#pragma unroll
+    for (int a = 0; a < 9; a++) R[a] = R0[a];
+#pragma unroll
+    for (int a = 0; a < 3; a++) t[a] = t0[a];
+    bool running = grp;
+    int prev = -1, iter = 0;
+    while (__any_sync(kFull, running)) {
+        Moments m;
+        m.clear();
+        int cnt = 0;
+        if (running) {
+            for (int k = sub; k < na; k += 4) {
+                int pi, ni;
+                al_get(al, na, k, pi, ni);
+                const double *p = x.P + 3 * pi, *q = x.Q + 3 * ni;
+                if (dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]) <= cut2) {
+                    m.add(p[0], p[1], p[2], q[0], q[1], q[2]);
+                    cnt++;
+                }
+            }
+        }
+        m.group_sum(4);
+        cnt += __shfl_xor_sync(kFull, cnt, 1);
+        cnt += __shfl_xor_sync(kFull, cnt, 2);
+        if (running) {
+            if (cnt >= 3) kabsch_from_moments(m, 3.0, R, t);
+            if (cnt == prev || ++iter >= 8) running = false;
+            prev = cnt;
+        }
+    }
+    const double d0sq = fmax(d0 * d0, 1e-12), sd8sq = sd8 * sd8;
+    double s = 0.0;
+    if (grp) {
+        for (int k = sub; k < na; k += 4) {
+            int pi, ni;
+            al_get(al, na, k, pi, ni);
+            const double *p = x.P + 3 * pi, *q = x.Q + 3 * ni;
+            double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
+            if (d2 <= sd8sq) s += 1.0 / (1.0 + d2 / d0sq);
+        }
+    }
+    s += __shfl_xor_sync(kFull, s, 1);
+    s += __shfl_xor_sync(kFull, s, 2);
+    const double score = s / fmax(lnorm, 1.0);
+    // first max over cutoffs 0..5 (strict >, initial -1e30)
+    double bs = kScoreInit;
+    int bg = 0;
+    for (int c = 0; c < kDetC; c++) {
+        double sc = __shfl_sync(kFull, score, 4 * c);
+        if (sc > bs) { bs = sc; bg = c; }
+    }
+#pragma unroll
+    for (int a = 0; a < 9; a++) Ro[a] = __shfl_sync(kFull, R[a], 4 * bg);
+#pragma unroll
+    for (int a = 0; a < 3; a++) to[a] = __shfl_sync(kFull, t[a], 4 * bg);
+    return bs;
+}
+
+// ---- the chain kernel ----------------------------------------------------
+struct ChainCtl {
+    int chunk, task;
+};
+
+__global__ void __launch_bounds__(32 * kChainWarps)
+k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
+        int ntasks, const ScanOut *__restrict__ scan, int *counter, uint32_t *gtrace,
+        size_t trace_words, double *gbh, uint32_t *gal, int pmax, int nmax, int flags) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ ChainCtl ctl;
+    __shared__ uint64_t bar;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool coord_smem = flags & 1, bh_smem = flags & 2, al_smem = flags & 4;
+    const uint32_t pbytes = ((uint32_t)pmax * 24u + 47u) & ~15u;
+    const uint32_t nbytes = ((uint32_t)nmax * 24u + 47u) & ~15u;
+    const uint32_t plb = ((uint32_t)pmax + 47u) & ~15u, nlb = ((uint32_t)nmax + 47u) & ~15u;
+    char *sP = smem, *sQ = sP + (coord_smem ? pbytes : 0);
+    char *sLp = sQ + (coord_smem ? nbytes : 0), *sLn = sLp + (coord_smem ? plb : 0);
+    char *wbase = sLn + (coord_smem ? nlb : 0);
+    const uint32_t bh_bytes = (((uint32_t)nmax + 1u) * 8u + 15u) & ~15u;
+    const uint32_t al_bytes = ((uint32_t)min(pmax, nmax) * 4u + 15u) & ~15u;
+    const int gw = blockIdx.x * kChainWarps + warp;  // global warp slot
+    double *bH = bh_smem ? reinterpret_cast<double *>(wbase + warp * bh_bytes)
+                         : gbh + (size_t)gw * (nmax + 1);
+    char *albase = wbase + (bh_smem ? kChainWarps * bh_bytes : 0);
+    uint32_t *al = al_smem ? reinterpret_cast<uint32_t *>(albase + warp * al_bytes)
+                           : gal + (size_t)gw * min(pmax, nmax);
+    uint32_t *trace = gtrace + (size_t)gw * trace_words;
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncthreads();
+    const int total = scan->total_chunks;
+    int staged = -1;
+    Pts x = {nullptr, nullptr};
+    const uint8_t *Lp = nullptr, *Ln = nullptr;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int c = atomicAdd(counter, 1);
+            int t = -1;
+            if (c < total) {
+                int lo = 0, hi = ntasks;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if (chunk_begin[mid] <= c) lo = mid + 1; else hi = mid;
+                }
+                t = lo - 1;
+            }
+            ctl.chunk = c;
+            ctl.task = t;
+        }
+        __syncthreads();
+        const int c = ctl.chunk, ti = ctl.task;
+        if (c >= total || ti < 0) break;
+        const ChainTask &T = tasks[ti];
+        const PairInfo &I = b.info[T.pair];
+        const int off = I.off, plen = I.plen, nlen = I.nlen;
+        if (T.pair != staged) {
+            const double *gP = b.predc + 3 * (size_t)off, *gQ = b.natc + 3 * (size_t)off;
+            const uint8_t *gLp = reinterpret_cast<const uint8_t *>(b.sspc + off);
+            const uint8_t *gLn = reinterpret_cast<const uint8_t *>(b.ssnc + off);
+            if (coord_smem) {
+                Copy cp[4];
+                char *dst[4] = {sP, sQ, sLp, sLn};
+                cp[0] = plan_copy(gP, (uint32_t)plen * 24u);
+                cp[1] = plan_copy(gQ, (uint32_t)nlen * 24u);
+                cp[2] = plan_copy(gLp, (uint32_t)plen);
+                cp[3] = plan_copy(gLn, (uint32_t)nlen);
+                stage_copies(cp, dst, 4, &bar, phase, b.err);
+                x.P = reinterpret_cast<const double *>(sP + cp[0].lead);
+                x.Q = reinterpret_cast<const double *>(sQ + cp[1].lead);
+                Lp = reinterpret_cast<const uint8_t *>(sLp + cp[2].lead);
+                Ln = reinterpret_cast<const uint8_t *>(sLn + cp[3].lead);
+            } else {
+                x.P = gP; x.Q = gQ; Lp = gLp; Ln = gLn;
+            }
+            staged = T.pair;
+        }
+        const int chain = (c - chunk_begin[ti]) * kChainWarps + warp;
+        if (chain < T.n_chains) {
+            const int gaps = T.gaps;
+            const int si = chain / gaps, g = chain % gaps;
+            const double gap = (gaps == 2 ? g : si) == 0 ? T.gap0 : T.gap1;
+            double R[9], t[3];
+            bool live = true;
+            if (T.start == START_WINDOW) {
+                int flen, ps, ns;
+                window_at(plen, nlen, T.dense, si, flen, ps, ns);
+                warp_kabsch_window(x, ps, ns, flen, R, t);
+            } else {
+                const double *r = T.rt + (size_t)si * kRec;
+                live = r[0] > -1e299;  // start flag: kNegInf = no start
+#pragma unroll
+                for (int a = 0; a < 9; a++) R[a] = r[1 + a];
+#pragma unroll
+                for (int a = 0; a < 3; a++) t[a] = r[10 + a];
+            }
+            NWParams pr;
+            pr.plen = plen;
+            pr.nlen = nlen;
+            pr.smode = T.smode;
+            pr.gap = gap;
+            pr.Lp = Lp;
+            pr.Ln = Ln;
+            if (T.smode == SMAT_SS4) {
+                double d01 = fmax(I.d0 + 1.5, I.d0s);
+                pr.inv_d0sq = 1.0 / (d01 * d01);
+                pr.cut2 = 0.0;
+            } else {
+                double d0dp = fmax(I.d0, 1.0);
+                pr.inv_d0sq = 1.0 / fmax(d0dp * d0dp, 1e-12);
+                pr.cut2 = T.sd8 * T.sd8;
+            }
+            if (T.live && !T.live[si]) live = false;
+            if (T.na_out) {
+                // EMIT: one alignment; aligned coordinates, count and (for
+                // SMAT_DP) the Kabsch on it with its compact score.
+                int na = 0;
+                if (live) na = nw_align(x, pr, R, t, bH, trace, al);
+                if (lane == 0) T.na_out[si] = na;
+                double *aP = T.alP + (size_t)si * T.al_cap * 3;
+                double *aQ = T.alQ + (size_t)si * T.al_cap * 3;
+                for (int k = lane; k < na && k < T.al_cap; k += 32) {
+                    int pi, ni;
+                    al_get(al, na, k, pi, ni);
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        aP[3 * k + d] = x.P[3 * pi + d];
+                        aQ[3 * k + d] = x.Q[3 * ni + d];
+                    }
+                }
+                if (T.smode == SMAT_DP && na >= 3) {
+                    double nR[9], nt[3];
+                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt);
+                    double *o = T.res + (size_t)si * kRec;
+                    if (lane < kRec) o[lane] = lane == 0 ? s : (lane < 10 ? nR[lane - 1] : nt[lane - 10]);
+                }
+            } else {
+                // LITE dp_refine chain (indialign_c/align.h:54-145,
+                // d0_search_lite): best starts at score 0 / identity.
+                double bs = 0.0, bR[9], bt[3];
+                set_identity(bR, bt);
+                for (int it = 0; live && it < T.max_iter; it++) {
+                    const int na = nw_align(x, pr, R, t, bH, trace, al);
+                    if (na < 3) break;  // same transform -> same alignment next time
+                    double nR[9], nt[3], dR[9], dt[3];
+                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt);
+                    double ds = lite_detailed(x, al, na, nR, nt, I.dcut, I.d0, T.sd8, I.lnorm, dR, dt);
+                    if (ds > s) {
+                        s = ds;
+#pragma unroll
+                        for (int a = 0; a < 9; a++) nR[a] = dR[a];
+#pragma unroll
+                        for (int a = 0; a < 3; a++) nt[a] = dt[a];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 9; a++) R[a] = nR[a];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) t[a] = nt[a];
+                    if (s > bs) {
+                        bs = s;
+#pragma unroll
+                        for (int a = 0; a < 9; a++) bR[a] = nR[a];
+#pragma unroll
+                        for (int a = 0; a < 3; a++) bt[a] = nt[a];
+                    }
+                }
+                double *o = T.res + (size_t)chain * kRec;
+                if (lane < kRec) o[lane] = lane == 0 ? (live ? bs : kNegInf)
+                                                     : (lane < 10 ? bR[lane - 1] : bt[lane - 10]);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+size_t chain_smem_bytes(int pmax, int nmax, int flags) {
+    size_t s = 0;
+    if (flags & 1) {
+        s += (((size_t)pmax * 24 + 47) & ~size_t(15)) + (((size_t)nmax * 24 + 47) & ~size_t(15));
+        s += (((size_t)pmax + 47) & ~size_t(15)) + (((size_t)nmax + 47) & ~size_t(15));
+    }
+    if (flags & 2) s += kChainWarps * ((((size_t)nmax + 1) * 8 + 15) & ~size_t(15));
+    if (flags & 4) s += kChainWarps * (((size_t)min(pmax, nmax) * 4 + 15) & ~size_t(15));
+    return s;
+}
+
+void launch_chain(const DevBatch &b, const ChainTask *tasks, const int *chunk_begin, int ntasks,
+                  const ScanOut *scan, int *counter, uint32_t *gtrace, size_t trace_words,
+                  double *gbh, uint32_t *gal, int pmax, int nmax, int flags, int grid,
+                  cudaStream_t st) {
+    size_t sm = chain_smem_bytes(pmax, nmax, flags);
+    k_chain<<<grid, 32 * kChainWarps, sm, st>>>(b, tasks, chunk_begin, ntasks, scan, counter,
+                                                gtrace, trace_words, gbh, gal, pmax, nmax, flags);
+}
+
+const void *chain_kernel_ptr() { return (const void *)k_chain; }
+
+cudaError_t chain_set_attributes() {
+    return cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kChainSmemMax);
+}
+
+}  // namespace ia

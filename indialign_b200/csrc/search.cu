@@ -1,0 +1,893 @@
+// Host side of the search: the C ABI, a pool of per-call contexts (stream +
+// grow-only device workspace), packing of host inputs into the device
+// layout, static result layouts, and the fixed launch sequence that restates
+// do_tmscore_search (indialign_c/indialign.cpp:29-266) stage by stage for a
+// whole batch.  All arithmetic runs in the kernels; the host only packs,
+// plans capacities once per batch and launches.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/indialign_b200.h"
+#include "kernels.h"
+#include "sched.cuh"
+
+namespace ia {
+
+static thread_local std::string g_last_error;
+static std::atomic<int> g_inject{0};
+
+static void set_error(const char *what, cudaError_t e) {
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+#define CK(x)                                 \
+    do {                                      \
+        cudaError_t e_ = (x);                 \
+        if (e_ != cudaSuccess) {              \
+            set_error(#x, e_);                \
+            return INDIALIGN_E_CUDA;          \
+        }                                     \
+    } while (0)
+
+// Grow-only device buffer with 64 bytes of tail padding.
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= cap && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = n < 16 ? 16 : n + n / 8;
+        cudaError_t e = cudaMalloc(&p, want * sizeof(T) + 64);
+        if (e != cudaSuccess) return e;
+        cap = want;
+        return cudaMemset(p, 0, want * sizeof(T) + 64);
+    }
+};
+
+// Static per-stage slot layout (uploaded once per batch).
+struct Layout {
+    int ntasks = 0;
+    std::vector<int> pair, aux;
+    std::vector<long long> base;
+    long long total = 0;  // result records / items
+    const int *d_pair = nullptr, *d_aux = nullptr;
+    const long long *d_base = nullptr;
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sms = 148;
+    DBuf<int> off, len, bitoff, err;
+    DBuf<double> lnorm, pred, nat, dscr, predc, natc;
+    DBuf<uint8_t> v, pv, nv;
+    DBuf<char> sspc, ssnc;
+    DBuf<PairInfo> info;
+    DBuf<PairState> state;
+    DBuf<int> pmap, nmap, vmap, scratch, kv;
+    DBuf<int2> seeds, topk;
+    DBuf<uint32_t> bits, gtrace, gal;
+    DBuf<uint64_t> hashes, fnv_pow;
+    DBuf<BankTask> btasks;
+    DBuf<ChainTask> ctasks;
+    DBuf<int> counts, begins, counter;
+    DBuf<ScanOut> scan;
+    DBuf<double> item_res, chain_res, alP, alQ, thread_rec, off_start, off_res, gbh, out, snap;
+    DBuf<int> lay_i;
+    DBuf<long long> lay_l;
+    std::vector<double> h_pred, h_nat, h_lnorm;
+    std::vector<uint8_t> h_v, h_pv, h_nv;
+    std::vector<int> h_off, h_len, h_bitoff;
+    int fnv_n = 0;
+    cudaEvent_t ev[2 * INDIALIGN_STAGES + 2];
+    bool events = false;
+};
+
+static std::mutex g_pool_mu;
+static std::vector<Ctx *> g_pool;
+static std::once_flag g_attr_once[64];
+
+static int acquire(int device, Ctx **out) {
+    if (device < 0) CK(cudaGetDevice(&device));
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (size_t i = 0; i < g_pool.size(); i++)
+            if (g_pool[i]->device == device) {
+                *out = g_pool[i];
+                g_pool.erase(g_pool.begin() + (long)i);
+                CK(cudaSetDevice(device));
+                return INDIALIGN_OK;
+            }
+    }
+    CK(cudaSetDevice(device));
+    Ctx *c = new Ctx();
+    c->device = device;
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+    cudaError_t attr_err = cudaSuccess;
+    std::call_once(g_attr_once[device & 63], [&]() {
+        attr_err = bank_set_attributes();
+        if (attr_err == cudaSuccess) attr_err = chain_set_attributes();
+    });
+    CK(attr_err);
+    *out = c;
+    return INDIALIGN_OK;
+}
+
+static void release(Ctx *c) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    g_pool.push_back(c);
+}
+
+// detailed-search items bound: max over n' <= n of seeds(n') x 6
+static std::vector<int> g_kdet;
+static int kdet_max(int n) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)g_kdet.size() <= n) {
+        int start = (int)g_kdet.size();
+        g_kdet.resize(n + 1);
+        for (int m = start; m <= n; m++) {
+            int v = arith_seed_count(m, 50, true);
+            g_kdet[m] = m > 0 ? (v > g_kdet[m - 1] ? v : g_kdet[m - 1]) : v;
+        }
+    }
+    return g_kdet[n];
+}
+
+constexpr int kTrace = INDIALIGN_TRACE_STAGES;
+
+struct Cfg {
+    int use_frag, max_iter, dp_iter;
+    double r1, r2, early;
+};
+
+// Host view of per-pair facts after k_prep / k_anchor.
+struct Plan {
+    std::vector<PairInfo> info;
+};
+
+class Runner {
+  public:
+    Runner(Ctx *c, const Cfg &cfg, int n) : c_(c), cfg_(cfg), n_(n) {}
+
+    int build_layouts(const std::vector<PairInfo> &info);
+    int run_stages();
+    DevBatch b;
+    double *snap = nullptr;  // device [n*kTrace*13] or nullptr
+    void mark(int stage) { launch_snapshot(b, snap, stage, kTrace, c_->stream); }
+    int pmax = 0, nmax = 0, Nmax = 0;
+
+  private:
+    int bank(int kind, Layout &L, double *recs = nullptr, int set_iter = -1, double early = -1);
+    int chain(int kind, Layout &L, int iters, double *recs = nullptr, double *recs2 = nullptr,
+              bool reduce = true);
+    int glue(int op, double thr = 0.0, const double *recs = nullptr, const int *idx = nullptr);
+    int dp_full();
+
+    Ctx *c_;
+    Cfg cfg_;
+    int n_;
+    Layout L_pair, L_main, L_detss, L_detdp, L_gapless, L_thread, L_topk, L_localn, L_locald,
+        L_threadch, L_single, L_offdp, L_offslots;
+    long long max_items_ = 0, max_chain_recs_ = 0, n_thread_ = 0, n_off_ = 0;
+    int chain_grid_ = 0, chain_flags_ = 0;
+    size_t trace_words_ = 0;
+};
+
+static void finish_layout(Layout &L) {
+    L.ntasks = (int)L.base.size();
+    long long acc = 0;
+    for (auto &x : L.base) {
+        long long cnt = x;
+        x = acc;
+        acc += cnt;
+    }
+    L.total = acc;
+}
+
+int Runner::build_layouts(const std::vector<PairInfo> &info) {
+    const int n = n_;
+    auto perpair = [&](Layout &L, auto count) {
+        L.base.resize(n);
+        for (int p = 0; p < n; p++) L.base[p] = info[p].status ? 0 : count(info[p]);
+        finish_layout(L);
+    };
+    L_pair.base.assign(0, 0);
+    L_pair.ntasks = n;
+    perpair(L_main, [](const PairInfo &I) { return (long long)I.K * I.C; });
+    perpair(L_detss, [](const PairInfo &I) {
+        int m = I.plen < I.nlen ? I.plen : I.nlen;
+        return (long long)kdet_max(m) * kDetC;
+    });
+    L_detdp.base.resize(2 * n);
+    L_detdp.pair.resize(2 * n);
+    L_detdp.aux.resize(2 * n);
+    for (int p = 0; p < n; p++)
+        for (int g = 0; g < 2; g++) {
+            const PairInfo &I = info[p];
+            int m = I.plen < I.nlen ? I.plen : I.nlen;
+            L_detdp.pair[2 * p + g] = p;
+            L_detdp.aux[2 * p + g] = g;
+            L_detdp.base[2 * p + g] = I.status ? 0 : (long long)kdet_max(m) * kDetC;
+        }
+    finish_layout(L_detdp);
+    perpair(L_gapless, [](const PairInfo &I) {
+        int kr, st, ma;
+        gapless_params(I.N, I.pvsum, I.nvsum, kr, st, ma);
+        return (long long)(kr > 0 ? offsets_count(-kr, kr, st) : 0);
+    });
+    perpair(L_topk, [](const PairInfo &I) { return (long long)I.C; });
+    // threading-DP: one bank slot per (pair, offset)
+    L_thread.pair.clear();
+    L_thread.aux.clear();
+    L_thread.base.clear();
+    L_threadch.base.resize(n);
+    L_threadch.aux.resize(n);
+    for (int p = 0; p < n; p++) {
+        const PairInfo &I = info[p];
+        int cnt = I.status ? 0 : thread_count(I.plen, I.nlen);
+        L_threadch.aux[p] = (int)L_thread.pair.size();
+        L_threadch.base[p] = 2LL * cnt;
+        for (int o = 0; o < cnt; o++) {
+            int ps, ns, ov;
+            thread_at(I.plen, I.nlen, o, ps, ns, ov);
+            L_thread.pair.push_back(p);
+            L_thread.aux.push_back(o);
+            L_thread.base.push_back(ov >= 3 ? (long long)arith_seed_count(ov, 5, true) * kDetC : 0);
+        }
+    }
+    finish_layout(L_thread);
+    finish_layout(L_threadch);
+    n_thread_ = L_thread.ntasks;
+    perpair(L_localn, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 0); });
+    perpair(L_locald, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 1); });
+    perpair(L_single, [](const PairInfo &) { return 2LL; });
+    // offset DP: start slots per (pair, offset)
+    L_offdp.base.resize(n);
+    L_offdp.aux.resize(n);
+    L_offslots.pair.clear();
+    L_offslots.aux.clear();
+    for (int p = 0; p < n; p++) {
+        const PairInfo &I = info[p];
+        int cnt = I.status ? 0 : offdp_count(I.N);
+        L_offdp.aux[p] = (int)L_offslots.pair.size();
+        L_offdp.base[p] = 2LL * cnt;
+        for (int o = 0; o < cnt; o++) {
+            L_offslots.pair.push_back(p);
+            L_offslots.aux.push_back(o);
+        }
+    }
+    finish_layout(L_offdp);
+    L_offslots.ntasks = (int)L_offslots.pair.size();
+    n_off_ = L_offslots.ntasks;
+    for (Layout *L : {&L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk})
+        max_items_ = L->total > max_items_ ? L->total : max_items_;
+    for (Layout *L : {&L_localn, &L_locald, &L_threadch, &L_single, &L_offdp})
+        max_chain_recs_ = L->total > max_chain_recs_ ? L->total : max_chain_recs_;
+    // upload all layouts into one int and one long long arena
+    size_t ni = 0, nl = 0;
+    for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots}) {
+        ni += L->pair.size() + L->aux.size();
+        nl += L->base.size();
+    }
+    CK(c_->lay_i.ensure(ni + 1));
+    CK(c_->lay_l.ensure(nl + 1));
+    std::vector<int> hi;
+    std::vector<long long> hl;
+    hi.reserve(ni);
+    hl.reserve(nl);
+    for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots}) {
+        L->d_pair = L->pair.empty() ? nullptr : c_->lay_i.p + hi.size();
+        hi.insert(hi.end(), L->pair.begin(), L->pair.end());
+        L->d_aux = L->aux.empty() ? nullptr : c_->lay_i.p + hi.size();
+        hi.insert(hi.end(), L->aux.begin(), L->aux.end());
+        L->d_base = L->base.empty() ? nullptr : c_->lay_l.p + hl.size();
+        hl.insert(hl.end(), L->base.begin(), L->base.end());
+        if (L->ntasks == 0 && !L->pair.empty()) L->ntasks = (int)L->pair.size();
+    }
+    if (!hi.empty())
+        CK(cudaMemcpyAsync(c_->lay_i.p, hi.data(), hi.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           c_->stream));
+    if (!hl.empty())
+        CK(cudaMemcpyAsync(c_->lay_l.p, hl.data(), hl.size() * sizeof(long long),
+                           cudaMemcpyHostToDevice, c_->stream));
+    // stage buffers
+    int maxtasks = n > 0 ? 2 * n : 1;
+    if (L_thread.ntasks > maxtasks) maxtasks = L_thread.ntasks;
+    CK(c_->btasks.ensure(maxtasks));
+    CK(c_->ctasks.ensure(maxtasks));
+    CK(c_->counts.ensure(maxtasks));
+    CK(c_->begins.ensure(maxtasks));
+    CK(c_->scan.ensure(1));
+    CK(c_->counter.ensure(1));
+    CK(c_->item_res.ensure((size_t)(max_items_ > 0 ? max_items_ : 1) * kRec));
+    CK(c_->chain_res.ensure((size_t)(max_chain_recs_ > 0 ? max_chain_recs_ : 1) * kRec));
+    CK(c_->thread_rec.ensure((size_t)(n_thread_ > 0 ? n_thread_ : 1) * kRec));
+    CK(c_->off_start.ensure((size_t)(n_off_ > 0 ? n_off_ : 1) * kRec));
+    CK(c_->off_res.ensure((size_t)(n_off_ > 0 ? n_off_ : 1) * kRec));
+    // chain kernel scratch: trace blocks per resident warp
+    pmax = nmax = 1;
+    for (auto &I : info) {
+        if (I.plen > pmax) pmax = I.plen;
+        if (I.nlen > nmax) nmax = I.nlen;
+    }
+    chain_flags_ = 0;
+    if ((size_t)(pmax + nmax) * 25 + 256 <= 96 * 1024) chain_flags_ |= 1;
+    if (nmax <= 512) chain_flags_ |= 2;
+    if ((pmax < nmax ? pmax : nmax) <= 2048) chain_flags_ |= 4;
+    size_t smem = chain_smem_bytes(pmax, nmax, chain_flags_);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel_ptr(), 32 * kChainWarps,
+                                                     smem));
+    if (per_sm < 1) per_sm = 1;
+    trace_words_ = (size_t)pmax * ((nmax + 15) / 16);
+    long long warps = (long long)c_->sms * per_sm * kChainWarps;
+    const size_t budget = (size_t)4 << 30;  // trace scratch budget
+    long long cap = (long long)(budget / (trace_words_ * 4 + 1));
+    if (warps > cap) warps = cap < kChainWarps ? kChainWarps : cap;
+    chain_grid_ = (int)(warps / kChainWarps);
+    if (chain_grid_ < 1) chain_grid_ = 1;
+    size_t nw = (size_t)chain_grid_ * kChainWarps;
+    CK(c_->gtrace.ensure(nw * trace_words_));
+    CK(c_->gbh.ensure((chain_flags_ & 2) ? 1 : nw * (nmax + 1)));
+    CK(c_->gal.ensure((chain_flags_ & 4) ? 1 : nw * (pmax < nmax ? pmax : nmax)));
+    CK(c_->alP.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
+    CK(c_->alQ.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
+    return INDIALIGN_OK;
+}
+
+int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early) {
+    if (L.ntasks <= 0) return INDIALIGN_OK;
+    PlanCtx pc = {};
+    pc.kind = kind;
+    pc.ntasks = L.ntasks;
+    pc.pair = L.d_pair;
+    pc.aux = L.d_aux;
+    pc.base = L.d_base;
+    pc.btasks = c_->btasks.p;
+    pc.counts = c_->counts.p;
+    pc.alP = c_->alP.p;
+    pc.alQ = c_->alQ.p;
+    pc.recs = recs;
+    pc.max_iter = set_iter >= 0 ? set_iter : cfg_.max_iter;
+    pc.early_term = early >= 0 ? early : cfg_.early;
+    launch_plan_bank(b, pc, c_->stream);
+    launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
+    int nmx = Nmax;
+    size_t sm = bank_smem_bytes(nmx);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bank_kernel_ptr(sm <= kBankSmemMax),
+                                                     kBankChunk, sm <= kBankSmemMax ? sm : 0));
+    if (per_sm < 1) per_sm = 1;
+    launch_bank(c_->btasks.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->item_res.p,
+                c_->err.p, nmx, c_->sms * per_sm, c_->stream);
+    launch_reduce_bank(c_->btasks.p, L.ntasks, c_->item_res.p, b.state, c_->stream);
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
+}
+
+int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, bool reduce) {
+    if (L.ntasks <= 0) return INDIALIGN_OK;
+    PlanCtx pc = {};
+    pc.kind = kind;
+    pc.ntasks = L.ntasks;
+    pc.pair = L.d_pair;
+    pc.aux = L.d_aux;
+    pc.base = L.d_base;
+    pc.ctasks = c_->ctasks.p;
+    pc.counts = c_->counts.p;
+    pc.alP = c_->alP.p;
+    pc.alQ = c_->alQ.p;
+    pc.chain_res = c_->chain_res.p;
+    pc.recs = recs;
+    pc.recs2 = recs2;
+    pc.iters = iters;
+    launch_plan_chain(b, pc, c_->stream);
+    launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
+    launch_chain(b, c_->ctasks.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->gtrace.p,
+                 trace_words_, c_->gbh.p, c_->gal.p, pmax, nmax, chain_flags_, chain_grid_,
+                 c_->stream);
+    if (reduce) launch_reduce_chain(b, pc, c_->stream);
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
+}
+
+int Runner::glue(int op, double thr, const double *recs, const int *idx) {
+    GlueArgs a = {};
+    a.op = op;
+    a.thr = thr;
+    a.dp_iter = cfg_.dp_iter;
+    a.recs = recs;
+    a.idx = idx;
+    launch_glue(b, a, c_->stream);
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
+}
+
+// dp_refine with fragment detailed searches (indialign_c/align.h:54-145,
+// d0_search_lite = false): per iteration one NW per gap chain, then the
+// detailed bank on each alignment, then the per-chain update.
+int Runner::dp_full() {
+    int rc;
+    for (int it = 0; it < cfg_.dp_iter; it++) {
+        if ((rc = chain(CH_DP_EMIT, L_pair, 1, nullptr, nullptr, false))) return rc;
+        if ((rc = bank(BK_DET_DP, L_detdp))) return rc;
+        if ((rc = glue(G_DP_STEP))) return rc;
+    }
+    return glue(G_DP_END);
+}
+
+#define RUN(x)                  \
+    do {                        \
+        int rc_ = (x);          \
+        if (rc_) return rc_;    \
+    } while (0)
+
+int Runner::run_stages() {
+    cudaStream_t st = c_->stream;
+    // 2. seed bank (indialign.cpp:90-104)
+    RUN(bank(BK_MAIN, L_main));
+    mark(0);
+    // 2b. SS seeds IA2 + IA4, rescored (indialign.cpp:106-116, ss.h:87-164)
+    launch_ss(b, st);
+    RUN(glue(G_SS_BEGIN));
+    RUN(chain(CH_SS2, L_pair, 1, nullptr, nullptr, false));
+    RUN(bank(BK_DET_SS, L_detss));
+    RUN(glue(G_SS_DET));
+    RUN(dp_full());
+    RUN(glue(G_SS_DP));
+    RUN(glue(G_SS4_START));
+    RUN(chain(CH_SS4, L_pair, 1, nullptr, nullptr, false));
+    RUN(bank(BK_DET_SS, L_detss));
+    RUN(glue(G_SS_DET));
+    RUN(dp_full());
+    RUN(glue(G_SS_DP));
+    launch_rescore(b, REC_SS, 0, st);
+    RUN(glue(G_SS_FINISH));
+    mark(1);
+    // 2c. gapless threading (indialign.cpp:118-123)
+    RUN(bank(BK_GAPLESS, L_gapless, nullptr, 5, 1e300));
+    RUN(glue(G_STAGE_UPDATE));
+    mark(2);
+    // 3. rescue ladder (indialign.cpp:125-152)
+    RUN(glue(G_GATE, cfg_.r1));
+    RUN(chain(CH_LOCAL, L_localn, 0));
+    launch_rescore(b, REC_STAGE, 1, st);
+    RUN(glue(G_STAGE_UPDATE));
+    mark(3);
+    RUN(glue(G_GATE, cfg_.r1));
+    RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p));
+    RUN(chain(CH_THREAD, L_threadch, 1, c_->thread_rec.p));
+    launch_rescore(b, REC_STAGE, 1, st);
+    RUN(glue(G_STAGE_UPDATE));
+    mark(4);
+    RUN(glue(G_GATE, cfg_.r2));
+    RUN(chain(CH_LOCAL, L_locald, 1));
+    launch_rescore(b, REC_STAGE, 1, st);
+    RUN(glue(G_STAGE_UPDATE));
+    mark(5);
+    // 4. top-50% distance seed (indialign.cpp:154-177)
+    launch_topk(b, st);
+    RUN(bank(BK_TOPK, L_topk));
+    RUN(glue(G_STAGE_UPDATE));
+    mark(6);
+    // 5. DP refinement (indialign.cpp:179-228)
+    RUN(glue(G_DPF_BEGIN));
+    RUN(dp_full());
+    launch_rescore(b, REC_DP, 0, st);
+    RUN(glue(G_DPF_UPDATE));
+    launch_rescore(b, REC_TMP, 0, st);
+    RUN(glue(G_TMP_UPDATE));
+    if (cfg_.dp_iter > 0) {
+        RUN(glue(G_IDP_START));
+        RUN(chain(CH_SINGLE, L_single, cfg_.dp_iter));
+        launch_rescore(b, REC_STAGE, 1, st);
+        RUN(glue(G_STAGE_UPDATE));
+        int extra = cfg_.dp_iter < 5 ? 5 - cfg_.dp_iter : 0;
+        if (extra > 0) {
+            RUN(glue(G_EXTRA_START));
+            RUN(chain(CH_SINGLE, L_single, extra));
+            launch_rescore(b, REC_STAGE, 1, st);
+            RUN(glue(G_STAGE_UPDATE));
+        }
+    }
+    mark(7);
+    if (cfg_.dp_iter > 0) {
+        // 5b. DP from offset Kabsch starts (indialign.cpp:229-256)
+        launch_offset_starts(b, c_->off_start.p, L_offslots.d_pair, L_offslots.d_aux,
+                             L_offslots.ntasks, st);
+        RUN(chain(CH_OFFDP, L_offdp, cfg_.dp_iter, c_->off_start.p, c_->off_res.p));
+        launch_rescore_list(b, c_->off_res.p, L_offslots.d_pair, L_offslots.ntasks, st);
+        RUN(glue(G_OFFDP_UPDATE, 0.0, c_->off_res.p, L_offdp.d_aux));
+    }
+    mark(8);
+    // 6. weighted TM refinement (indialign.cpp:258-264)
+    launch_weighted(b, st);
+    mark(9);
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
+}
+
+}  // namespace ia
+
+namespace ia {
+
+static uint64_t fnv_pow_host(int z) {
+    uint64_t r = 1, b = 1099511628211ULL;
+    while (z) {
+        if (z & 1) r *= b;
+        b *= b;
+        z >>= 1;
+    }
+    return r;
+}
+
+static const char *kStageNames[] = {"seed_build", "seed_bank", "ss", "gapless_threading",
+                                    "local_fragment", "threading_dp", "dense_local_fragment",
+                                    "topk_seed", "dp_refine", "offset_dp", "weighted_refine",
+                                    "total"};
+
+// Where a batch's inputs live: host pairs, or device arrays packed back to
+// back (off[] on the host).
+struct Source {
+    std::vector<const NativePairInput *> host;
+    int n_dev = 0;
+    const int *off = nullptr;
+    const double *pred = nullptr, *nat = nullptr, *lnorm = nullptr;
+    const uint8_t *v = nullptr, *pv = nullptr, *nv = nullptr;
+    int n() const { return host.empty() ? n_dev : (int)host.size(); }
+    int len(int p) const { return host.empty() ? off[p + 1] - off[p] : host[p]->length; }
+};
+
+// Inputs -> packed device batch; runs the search; writes {score,R,t} per
+// pair to results (host) or d_out (device).
+static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results, double *d_out,
+                     const IndialignBatchOptions *opts) {
+    const int n = src.n();
+    cudaStream_t st = c->stream;
+    // ---- pack (pair blocks padded to an even residue count) ----
+    c->h_off.resize(n + 1);
+    c->h_len.resize(n);
+    c->h_bitoff.resize(n);
+    int total = 0, Nmax = 1;
+    long long bits = 0;
+    for (int p = 0; p < n; p++) {
+        const int N = src.len(p);
+        c->h_off[p] = total;
+        c->h_len[p] = N;
+        c->h_bitoff[p] = (int)bits;
+        bits += (long long)kMaxBitSeeds * ((N + 31) / 32);
+        total += (N + 1) & ~1;
+        if (N > Nmax) Nmax = N;
+    }
+    c->h_off[n] = total;
+    if (bits > 0x7fffffffLL) {
+        g_last_error = "batch too large";
+        return INDIALIGN_E_INPUT;
+    }
+    const bool on_host = !src.host.empty();
+    c->h_lnorm.resize(n);
+    if (on_host) {
+        c->h_pred.assign(3 * (size_t)total, 0.0);
+        c->h_nat.assign(3 * (size_t)total, 0.0);
+        c->h_v.assign(total, 0);
+        c->h_pv.assign(total, 0);
+        c->h_nv.assign(total, 0);
+        for (int p = 0; p < n; p++) {
+            const NativePairInput *q = src.host[p];
+            const size_t o = c->h_off[p], N = q->length;
+            std::memcpy(&c->h_pred[3 * o], q->pred_xyz, 24 * N);
+            std::memcpy(&c->h_nat[3 * o], q->native_xyz, 24 * N);
+            std::memcpy(&c->h_v[o], q->valid_mask, N);
+            std::memcpy(&c->h_pv[o], q->pred_valid_mask, N);
+            std::memcpy(&c->h_nv[o], q->native_valid_mask, N);
+            c->h_lnorm[p] = q->lnorm;
+        }
+    } else {
+        for (int p = 0; p < n; p++) c->h_lnorm[p] = src.lnorm[p];
+    }
+    // ---- device buffers ----
+    const size_t T = (size_t)total + 2;
+    CK(c->off.ensure(n + 1));
+    CK(c->len.ensure(n));
+    CK(c->bitoff.ensure(n));
+    CK(c->err.ensure(1));
+    CK(c->lnorm.ensure(n));
+    CK(c->pred.ensure(3 * T));
+    CK(c->nat.ensure(3 * T));
+    CK(c->v.ensure(T));
+    CK(c->pv.ensure(T));
+    CK(c->nv.ensure(T));
+    CK(c->info.ensure(n));
+    CK(c->state.ensure(n));
+    CK(c->pmap.ensure(T));
+    CK(c->nmap.ensure(T));
+    CK(c->vmap.ensure(T));
+    CK(c->scratch.ensure(T + n + 1));
+    CK(c->dscr.ensure(T));
+    CK(c->predc.ensure(3 * T));
+    CK(c->natc.ensure(3 * T));
+    CK(c->sspc.ensure(T));
+    CK(c->ssnc.ensure(T));
+    CK(c->seeds.ensure((size_t)n * kMaxSeeds));
+    CK(c->topk.ensure(n));
+    CK(c->bits.ensure((size_t)bits + 1));
+    CK(c->hashes.ensure((size_t)n * kMaxSeeds));
+    CK(c->kv.ensure(2 * T));
+    if (c->fnv_n < Nmax + 1) {
+        std::vector<uint64_t> pw(Nmax + 1);
+        for (int z = 0; z <= Nmax; z++) pw[z] = fnv_pow_host(z);
+        CK(c->fnv_pow.ensure(Nmax + 1));
+        CK(cudaMemcpy(c->fnv_pow.p, pw.data(), pw.size() * 8, cudaMemcpyHostToDevice));
+        c->fnv_n = Nmax + 1;
+    }
+    CK(cudaMemcpyAsync(c->off.p, c->h_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->len.p, c->h_len.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->bitoff.p, c->h_bitoff.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(c->lnorm.p, c->h_lnorm.data(), n * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (on_host) {
+        CK(cudaMemcpyAsync(c->pred.p, c->h_pred.data(), c->h_pred.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->nat.p, c->h_nat.data(), c->h_nat.size() * 8, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->v.p, c->h_v.data(), total, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->pv.p, c->h_pv.data(), total, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(c->nv.p, c->h_nv.data(), total, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), st));
+    DevBatch b;
+    b.n = n;
+    b.off = c->off.p;
+    b.len = c->len.p;
+    b.lnorm = c->lnorm.p;
+    b.pred = c->pred.p;
+    b.nat = c->nat.p;
+    b.v = c->v.p;
+    b.pv = c->pv.p;
+    b.nv = c->nv.p;
+    b.info = c->info.p;
+    b.state = c->state.p;
+    b.pmap = c->pmap.p;
+    b.nmap = c->nmap.p;
+    b.vmap = c->vmap.p;
+    b.scratch = c->scratch.p;
+    b.dscr = c->dscr.p;
+    b.predc = c->predc.p;
+    b.natc = c->natc.p;
+    b.sspc = c->sspc.p;
+    b.ssnc = c->ssnc.p;
+    b.seeds = c->seeds.p;
+    b.topk_seed = c->topk.p;
+    b.bits = c->bits.p;
+    b.bitoff = c->bitoff.p;
+    b.hashes = c->hashes.p;
+    b.kv = c->kv.p;
+    b.fnv_pow = c->fnv_pow.p;
+    b.err = c->err.p;
+    if (!on_host) {
+        // caller's offsets to the device (scratch doubles as staging), repack
+        CK(cudaMemcpyAsync(c->scratch.p, src.off, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+        launch_repack(b, c->scratch.p, src.pred, src.nat, src.v, src.pv, src.nv, st);
+        CK(cudaGetLastError());
+    }
+    const bool prof = (opts && (opts->profile || opts->stage_ms)) || std::getenv("INDIALIGN_PROFILE");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, st));
+    }
+    // ---- seeds ----
+    launch_prep(b, cfg.use_frag, st);
+    launch_anchor(b, st);
+    CK(cudaGetLastError());
+    std::vector<PairInfo> info(n);
+    CK(cudaMemcpyAsync(info.data(), c->info.p, n * sizeof(PairInfo), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    Runner r(c, cfg, n);
+    r.b = b;
+    r.Nmax = Nmax;
+    if (opts && opts->stage_best) {
+        CK(c->snap.ensure((size_t)n * kTrace * kRec));
+        CK(cudaMemsetAsync(c->snap.p, 0, (size_t)n * kTrace * kRec * 8, st));
+        r.snap = c->snap.p;
+    }
+    int rc = r.build_layouts(info);
+    if (rc) return rc;
+    rc = r.run_stages();
+    if (rc) return rc;
+    if (prof) CK(cudaEventRecord(e1, st));
+    // ---- results ----
+    std::vector<PairState> state(n);
+    int err = 0;
+    CK(cudaMemcpyAsync(state.data(), c->state.p, n * sizeof(PairState), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&err, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (prof) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        const char *tag = std::getenv("INDIALIGN_PROFILE_TAG");
+        if ((opts && opts->profile) || std::getenv("INDIALIGN_PROFILE"))
+            std::fprintf(stderr, "[indialign]%s pairs=%d stage=%s ms=%.3f\n", tag ? tag : "", n,
+                         kStageNames[INDIALIGN_STAGES - 1], ms);
+        if (opts && opts->stage_ms) opts->stage_ms[INDIALIGN_STAGES - 1] = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    if (err) {
+        g_last_error = "device error flag " + std::to_string(err);
+        return INDIALIGN_E_DEVICE;
+    }
+    if (opts && opts->stage_best && r.snap)
+        CK(cudaMemcpy(opts->stage_best, r.snap, (size_t)n * kTrace * kRec * 8, cudaMemcpyDeviceToHost));
+    if (d_out) {
+        launch_export(b, d_out, st);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+    } else {
+        for (int p = 0; p < n; p++)
+            std::memcpy(results + 13 * (size_t)p, state[p].rec[REC_BEST], 13 * 8);
+    }
+    return INDIALIGN_OK;
+}
+
+static Cfg make_cfg(const NativeConfig *cfg) {
+    Cfg c;
+    c.use_frag = cfg->use_fragment_search != 0;
+    c.max_iter = cfg->max_iter;
+    c.dp_iter = cfg->dp_iter;
+    c.r1 = cfg->rescue_score_1;
+    c.r2 = cfg->rescue_score_2;
+    c.early = cfg->early_term_score;
+    return c;
+}
+
+static int search_host(int n_pairs, const NativePairInput *inputs, const NativeConfig *cfg,
+                       const IndialignBatchOptions *opts, NativePairResult *outputs) {
+    g_last_error.clear();
+    if (g_inject.load() > 0) {
+        g_inject.fetch_sub(1);
+        g_last_error = "injected failure";
+        return INDIALIGN_E_INJECTED;
+    }
+    if (!inputs || !cfg || !outputs || n_pairs < 0) {
+        g_last_error = "null argument";
+        return INDIALIGN_E_INPUT;
+    }
+    Source src;
+    std::vector<const NativePairInput *> &in = src.host;
+    std::vector<int> ids;
+    for (int p = 0; p < n_pairs; p++) {
+        const NativePairInput *q = &inputs[p];
+        if (q->length <= 0) continue;  // reference: rc -1, output untouched
+        if (q->length > 65535 || !q->pred_xyz || !q->native_xyz || !q->valid_mask ||
+            !q->pred_valid_mask || !q->native_valid_mask) {
+            g_last_error = "pair " + std::to_string(p) + ": null pointer or length > 65535";
+            return INDIALIGN_E_INPUT;
+        }
+        in.push_back(q);
+        ids.push_back(p);
+    }
+    if (in.empty()) return INDIALIGN_OK;
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0) {
+        cudaGetLastError();
+        g_last_error = "no CUDA device";
+        return INDIALIGN_E_NODEVICE;
+    }
+    Ctx *c = nullptr;
+    int rc = acquire(opts ? opts->device : -1, &c);
+    if (rc) return rc;
+    std::vector<double> res(13 * in.size());
+    rc = run_batch(c, make_cfg(cfg), src, res.data(), nullptr, opts);
+    release(c);
+    if (rc) return rc;
+    for (size_t k = 0; k < ids.size(); k++) {
+        NativePairResult *o = &outputs[ids[k]];
+        o->score = res[13 * k];
+        std::memcpy(o->rotation, &res[13 * k + 1], 72);
+        std::memcpy(o->translation, &res[13 * k + 10], 24);
+    }
+    return INDIALIGN_OK;
+}
+
+}  // namespace ia
+
+extern "C" {
+
+void indialign_default_config(NativeConfig *cfg) {
+    cfg->backend_mode = 0;
+    cfg->use_fragment_search = 1;
+    cfg->max_iter = 20;
+    cfg->dp_iter = 1;
+    cfg->max_mem_gb = 20.0;
+    cfg->request_cuda = 0;
+    cfg->rescue_score_1 = 0.5;
+    cfg->rescue_score_2 = 0.3;
+    cfg->early_term_score = 0.99;
+}
+
+int indialign_tmscore_search(const NativePairInput *inp, const NativeConfig *cfg,
+                             NativePairResult *out) {
+    if (!inp) return INDIALIGN_E_INPUT;
+    if (inp->length <= 0) return INDIALIGN_E_LENGTH;
+    return ia::search_host(1, inp, cfg, nullptr, out);
+}
+
+int indialign_tmscore_search_batch(int n_pairs, const NativePairInput *inputs,
+                                   const NativeConfig *cfg, NativePairResult *outputs) {
+    return ia::search_host(n_pairs, inputs, cfg, nullptr, outputs);
+}
+
+int indialign_tmscore_search_batch_ex(int n_pairs, const NativePairInput *inputs,
+                                      const NativeConfig *cfg, const IndialignBatchOptions *opts,
+                                      NativePairResult *outputs) {
+    return ia::search_host(n_pairs, inputs, cfg, opts, outputs);
+}
+
+int indialign_cuda_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return 0;
+    }
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, 0) != cudaSuccess) return 0;
+    return major == 10 ? 1 : 0;
+}
+
+int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d_pred,
+                                    const double *d_nat, const uint8_t *d_v,
+                                    const uint8_t *d_pv, const uint8_t *d_nv,
+                                    const double *lnorm, const NativeConfig *cfg,
+                                    const IndialignBatchOptions *opts, double *d_out) {
+    ia::g_last_error.clear();
+    if (ia::g_inject.load() > 0) {
+        ia::g_inject.fetch_sub(1);
+        ia::g_last_error = "injected failure";
+        return INDIALIGN_E_INJECTED;
+    }
+    if (n_pairs <= 0) return INDIALIGN_OK;
+    if (!off || !d_pred || !d_nat || !d_v || !d_pv || !d_nv || !lnorm || !cfg || !d_out)
+        return INDIALIGN_E_INPUT;
+    for (int p = 0; p < n_pairs; p++) {
+        int L = off[p + 1] - off[p];
+        if (L <= 0 || L > 65535) {
+            ia::g_last_error = "pair " + std::to_string(p) + ": length must be in 1..65535";
+            return INDIALIGN_E_INPUT;
+        }
+    }
+    ia::Source src;
+    src.n_dev = n_pairs;
+    src.off = off;
+    src.pred = d_pred;
+    src.nat = d_nat;
+    src.v = d_v;
+    src.pv = d_pv;
+    src.nv = d_nv;
+    src.lnorm = lnorm;
+    ia::Ctx *c = nullptr;
+    int rc = ia::acquire(opts ? opts->device : -1, &c);
+    if (rc) return rc;
+    rc = ia::run_batch(c, ia::make_cfg(cfg), src, nullptr, d_out, opts);
+    ia::release(c);
+    return rc;
+}
+
+const char *indialign_last_error(void) { return ia::g_last_error.c_str(); }
+
+void indialign_inject_failure(int count) { ia::g_inject.store(count > 0 ? count : 0); }
+
+}  // extern "C"

@@ -336,3 +336,19 @@ int ref_trace_search(const NativePairInput *inp, const NativeConfig *cfg,
 }
 
 }  // extern "C"
+
+#include <algorithm>
+#include <utility>
+
+extern "C" {
+
+// std::sort with the comparator of build_anchor_contact_seeds
+// (indialign_c/seeds.h:237-238): order by count only, descending.
+void ref_std_sort_desc(int *keys, int *idx, int n) {
+    std::vector<std::pair<int, int>> v(n);
+    for (int i = 0; i < n; i++) v[i] = {keys[i], idx[i]};
+    std::sort(v.begin(), v.end(), [](auto &x, auto &y) { return x.first > y.first; });
+    for (int i = 0; i < n; i++) { keys[i] = v[i].first; idx[i] = v[i].second; }
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+"""Golden fixtures for the parity tests, produced by the reference's own build.
+
+Runs here, where the reference sources exist:
+
+    make -C oracle && python tests/golden/make_golden.py
+
+oracle/_ref/libindialign_ref.so is the reference's `make cpu` build compiled
+from its sources (oracle/Makefile); ref_trace_search (oracle/ref_stages.cpp)
+replays its stage order through the reference's own stage functions to record
+the running best after every stage.  Outputs are small .npz files: the packed
+inputs of each case group and the reference's results.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from indialign_b200 import abi, workloads as W  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(ROOT, "oracle", "_ref", "libindialign_ref.so")
+STAGES = os.path.join(ROOT, "oracle", "_ref", "libindialign_ref_stages.so")
+N_STAGES = 10
+
+
+def pack(pairs):
+    lens = [p.pred.shape[0] for p in pairs]
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    cat = lambda f, dt: np.concatenate([np.asarray(f(p), dt).reshape(-1) for p in pairs])
+    return dict(off=off, pred=cat(lambda p: p.pred, np.float64),
+                nat=cat(lambda p: p.native, np.float64), v=cat(lambda p: p.valid, np.uint8),
+                pv=cat(lambda p: p.pred_valid, np.uint8), nv=cat(lambda p: p.native_valid, np.uint8),
+                lnorm=np.array([p.lnorm for p in pairs], np.float64))
+
+
+def run_ref(pairs):
+    ref = abi.bind_reference_abi(ctypes.CDLL(REF))
+    rc, s, R, t = abi.run_batch(ref, pairs)
+    assert rc == 0
+    st = ctypes.CDLL(STAGES)
+    st.ref_trace_search.argtypes = [ctypes.POINTER(abi.NativePairInput),
+                                    ctypes.POINTER(abi.NativeConfig),
+                                    ctypes.POINTER(ctypes.c_double),
+                                    ctypes.POINTER(abi.NativePairResult)]
+    cfg = abi.default_config(ref)
+    pk = abi.PackedInputs(pairs)
+    trace = np.zeros((len(pairs), N_STAGES, 13))
+    for k in range(len(pairs)):
+        res = abi.NativePairResult()
+        buf = np.zeros(N_STAGES * 13)
+        st.ref_trace_search(ctypes.byref(pk.arr[k]), ctypes.byref(cfg),
+                            buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(res))
+        trace[k] = buf.reshape(N_STAGES, 13)
+        assert abs(res.score - s[k]) < 1e-12, (k, res.score, s[k])
+    return s, R, t, trace
+
+
+def edge_pairs():
+    rng = np.random.default_rng(77)
+    out = []
+    x = W.make_trace(40, rng)
+    out.append(W.Pair(x.copy(), x.copy(), *(np.ones(40, np.uint8),) * 3, 40.0))  # identity
+    p = W.make_pair(5, 1.0, rng)                                                  # tiny
+    out.append(p)
+    p = W.make_pair(30, 3.0, rng)
+    p.lnorm = 2.0                                                                 # lnorm <= 2
+    out.append(p)
+    p = W.make_pair(24, 2.0, rng)
+    p.valid = np.zeros(24, np.uint8)                                              # nothing valid
+    out.append(p)
+    p = W.make_pair(36, 4.0, rng, invalid_frac=0.2)
+    p.valid = p.valid.copy()
+    p.valid[p.valid == 1][:3] = 2
+    idx = np.nonzero(p.valid)[0][:4]
+    p.valid[idx] = 2                                                              # byte value 2
+    out.append(p)
+    out.append(W.make_pair(3, 0.5, rng))                                          # N = 3
+    p = W.make_pair(50, 6.0, rng, invalid_frac=0.1)
+    p.lnorm = float(p.valid.sum())                                                # lnorm = valid count
+    out.append(p)
+    p = W.make_pair(45, 2.0, rng)
+    p.pred_valid = p.pred_valid.copy()
+    p.pred_valid[10:20] = 0                                                       # one-sided gap
+    p.valid = (p.pred_valid & p.native_valid).astype(np.uint8)
+    out.append(p)
+    return out
+
+
+def main():
+    groups = {
+        "single": W.single(0),
+        "batch": [p for p in W.batch(64, seed=101) if p.pred.shape[0] <= 110][:12],
+        "hard": [p for p in W.hard(48, seed=202) if p.pred.shape[0] <= 110][:4],
+        "edge": edge_pairs(),
+    }
+    for name, pairs in groups.items():
+        s, R, t, trace = run_ref(pairs)
+        np.savez_compressed(os.path.join(OUT, f"golden_{name}.npz"), score=s, R=R, t=t,
+                            trace=trace, sigma=np.array([p.sigma for p in pairs]), **pack(pairs))
+        print(name, len(pairs), np.round(s, 4))
+    # std::sort tie order of the anchor candidates (count-only comparator)
+    st = ctypes.CDLL(STAGES)
+    rng = np.random.default_rng(5)
+    rows = []
+    for n in (1, 2, 5, 16, 17, 40, 100, 300, 1000):
+        keys = rng.integers(3, 9, size=n).astype(np.int32)
+        idx = np.arange(n, dtype=np.int32)
+        k2, i2 = keys.copy(), idx.copy()
+        st.ref_std_sort_desc(k2.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             i2.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n)
+        rows.append((keys, i2))
+    np.savez_compressed(os.path.join(OUT, "golden_sort.npz"),
+                        **{f"keys{j}": r[0] for j, r in enumerate(rows)},
+                        **{f"order{j}": r[1] for j, r in enumerate(rows)})
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,76 @@
+"""The oracle (oracle/indialign_oracle.c) pinned against the reference.
+
+The golden fixtures hold the reference build's own outputs (see
+tests/golden/make_golden.py); when the reference build itself is present
+(oracle/_ref) the oracle is also compared with it on fresh inputs."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import GoldenPairs, rot_err_deg
+from indialign_b200 import abi, workloads as W
+
+
+def test_oracle_matches_golden(oracle, golden):
+    rc, s, R, t = abi.run_batch(oracle, golden.pairs, prefix="ora_")
+    assert rc == 0
+    # same FP64 algorithm; only reassociation under -ffast-math differs
+    np.testing.assert_allclose(s, golden.score, rtol=0, atol=1e-9)
+    assert rot_err_deg(R, golden.R).max() < 1e-4
+
+
+def test_oracle_stage_trace_matches_golden(oracle, golden):
+    lib = oracle
+    lib.ora_trace_search.argtypes = [ctypes.POINTER(abi.NativePairInput),
+                                     ctypes.POINTER(abi.NativeConfig),
+                                     ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(abi.NativePairResult)]
+    cfg = abi.default_config(lib, "ora_")
+    pk = abi.PackedInputs(golden.pairs)
+    for k in range(pk.n):
+        buf = np.zeros(10 * 13)
+        res = abi.NativePairResult()
+        lib.ora_trace_search(ctypes.byref(pk.arr[k]), ctypes.byref(cfg),
+                             buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                             ctypes.byref(res))
+        tr = buf.reshape(10, 13)
+        ref = golden.trace[k]
+        ran = ref[:, 0] > -1e30
+        assert np.array_equal(tr[:, 0] > -1e30, ran)
+        np.testing.assert_allclose(tr[ran, 0], ref[ran, 0], rtol=0, atol=1e-9)
+
+
+def test_sort_tie_order_matches_std_sort(oracle):
+    """The anchor candidates' tie order (count-only std::sort) is reproduced."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_sort.npz"))
+    oracle.ora_introsort_desc.argtypes = [ctypes.POINTER(ctypes.c_int)] * 2 + [ctypes.c_int]
+    j = 0
+    while f"keys{j}" in z:
+        keys = z[f"keys{j}"].astype(np.int32).copy()
+        idx = np.arange(len(keys), dtype=np.int32)
+        oracle.ora_introsort_desc(keys.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                  idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(keys))
+        np.testing.assert_array_equal(idx, z[f"order{j}"])
+        j += 1
+    assert j >= 5
+
+
+def test_oracle_vs_reference_fresh(oracle, ref):
+    pairs = W.batch(6, 40, 90, seed=909) + W.hard(4, seed=910)[:2]
+    pairs = [p for p in pairs if p.pred.shape[0] <= 100]
+    rc1, s1, R1, _ = abi.run_batch(ref, pairs)
+    rc2, s2, R2, _ = abi.run_batch(oracle, pairs, prefix="ora_")
+    assert rc1 == rc2 == 0
+    np.testing.assert_allclose(s2, s1, rtol=0, atol=1e-9)
+
+
+def test_oracle_length_zero(oracle):
+    inp = abi.NativePairInput()
+    inp.length = 0
+    cfg = abi.default_config(oracle, "ora_")
+    out = abi.NativePairResult()
+    out.score = 7.0
+    assert oracle.ora_tmscore_search(ctypes.byref(inp), ctypes.byref(cfg), ctypes.byref(out)) == -1
+    assert out.score == 7.0

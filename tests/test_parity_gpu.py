@@ -1,0 +1,137 @@
+"""Parity of the CUDA search with the reference, through the C ABI.
+
+Bar (per pair): final TM-score >= reference - 1e-6 after the FP64 same-index
+rescoring the search ends with; |dTM| and the rotation error against the
+reference are reported.  Checked on the golden fixtures (reference outputs
+committed under tests/golden/) and on fresh seeded inputs against the oracle.
+"""
+import ctypes
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import GoldenPairs, rot_err_deg
+import indialign_b200 as ia
+from indialign_b200 import abi, workloads as W
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _report(tag, s, ref):
+    d = s - ref
+    print(f"[{tag}] n={len(s)} min dTM={d.min():.3e} max|dTM|={np.abs(d).max():.3e}")
+
+
+def test_golden_final_scores(golden):
+    s, R, t = ia.search(golden.pairs)
+    _report(golden.name, s, golden.score)
+    assert np.all(s >= golden.score - TOL), np.nonzero(s < golden.score - TOL)
+
+
+def test_golden_stage_trace(golden):
+    n = len(golden.pairs)
+    tr = np.zeros(n * ia.TRACE_STAGES * 13)
+    ia.search(golden.pairs, stage_best=tr)
+    tr = tr.reshape(n, ia.TRACE_STAGES, 13)
+    ref = golden.trace
+    bad = []
+    for k in range(n):
+        for st in range(ia.TRACE_STAGES):
+            if ref[k, st, 0] > -1e30 and abs(tr[k, st, 0] - ref[k, st, 0]) > TOL:
+                bad.append((k, st, tr[k, st, 0], ref[k, st, 0]))
+    assert not bad, bad[:10]
+
+
+def test_fresh_pairs_vs_oracle(oracle):
+    pairs = W.batch(24, 40, 140, seed=4242)
+    s, R, t = ia.search(pairs)
+    rc, so, Ro, to = abi.run_batch(oracle, pairs, prefix="ora_")
+    assert rc == 0
+    _report("fresh", s, so)
+    assert np.all(s >= so - TOL)
+    agree = np.abs(s - so) <= TOL
+    assert rot_err_deg(R[agree], Ro[agree]).max() < 1e-3
+
+
+def test_rotation_is_proper_and_score_is_rescored():
+    pairs = W.batch(8, 40, 120, seed=77)
+    s, R, t = ia.search(pairs)
+    for k, p in enumerate(pairs):
+        M = R[k].reshape(3, 3)
+        assert np.allclose(M @ M.T, np.eye(3), atol=1e-9)
+        assert abs(np.linalg.det(M) - 1) < 1e-9
+        # aligned_d = sum_k p_k R[3k+d] + t_d  ->  x @ M + t
+        moved = p.pred @ M + t[k]
+        L = p.pred.shape[0]
+        d0 = max(0.6 * np.sqrt(L - 0.5) - 2.5, 0.3) if L >= 30 else None
+        if d0 is None:
+            continue
+        d2 = np.sum((moved - p.native) ** 2, 1)
+        tm = np.sum((1 / (1 + d2 / d0 ** 2))[p.valid != 0]) / max(p.lnorm, 1)
+        assert abs(tm - s[k]) < 1e-9
+
+
+def test_identity_pair_scores_one():
+    x = W.make_trace(60, np.random.default_rng(3))
+    one = np.ones(60, np.uint8)
+    s, R, t = ia.search([W.Pair(x, x.copy(), one, one, one, 60.0)])
+    assert s[0] > 0.999999
+
+
+def test_device_entry_matches_host_entry():
+    torch = pytest.importorskip("torch")
+    pairs = W.batch(6, 40, 100, seed=31)
+    s_h, R_h, t_h = ia.search(pairs)
+    lens = [p.pred.shape[0] for p in pairs]
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    cat = lambda f, dt: torch.from_numpy(np.concatenate([np.asarray(f(p), dt).reshape(-1) for p in pairs])).cuda()
+    dp, dn = cat(lambda p: p.pred, np.float64), cat(lambda p: p.native, np.float64)
+    dv, dpv, dnv = (cat(lambda p: p.valid, np.uint8), cat(lambda p: p.pred_valid, np.uint8),
+                    cat(lambda p: p.native_valid, np.uint8))
+    ln = np.array([p.lnorm for p in pairs], np.float64)
+    out = torch.zeros(len(pairs) * 13, dtype=torch.float64, device="cuda")
+    lib = ia.load()
+    cfg = ia.default_config()
+    opts = ia.BatchOptions()
+    opts.device = torch.cuda.current_device()
+    torch.cuda.synchronize()
+    rc = lib.indialign_tmscore_search_device(
+        len(pairs), off.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), dp.data_ptr(), dn.data_ptr(),
+        dv.data_ptr(), dpv.data_ptr(), dnv.data_ptr(),
+        ln.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(cfg), ctypes.byref(opts),
+        out.data_ptr())
+    assert rc == 0, ia.last_error()
+    o = out.cpu().numpy().reshape(-1, 13)
+    np.testing.assert_array_equal(o[:, 0], s_h)
+    np.testing.assert_array_equal(o[:, 1:10], R_h)
+
+
+def test_concurrent_calls_are_independent():
+    a = W.batch(4, 40, 90, seed=5)
+    b = W.batch(4, 40, 90, seed=6)
+    ref_a, ref_b = ia.search(a)[0], ia.search(b)[0]
+    out = {}
+
+    def run(name, pairs):
+        out[name] = ia.search(pairs)[0]
+
+    th = [threading.Thread(target=run, args=(f"a{i}", a)) for i in range(2)] + \
+         [threading.Thread(target=run, args=(f"b{i}", b)) for i in range(2)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    for i in range(2):
+        np.testing.assert_array_equal(out[f"a{i}"], ref_a)
+        np.testing.assert_array_equal(out[f"b{i}"], ref_b)
+
+
+def test_injected_failure_leaves_context_usable():
+    lib = ia.load()
+    lib.indialign_inject_failure(1)
+    with pytest.raises(ia.IndialignError, match="rc=-6"):
+        ia.search(W.single(0))
+    s, _, _ = ia.search(W.single(0))
+    assert s[0] > 0.3
