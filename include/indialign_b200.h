@@ -94,8 +94,16 @@ typedef struct {
     int device;              /* CUDA device ordinal (-1: current) */
     int use_graph;           /* capture the stage sequence in a CUDA graph and replay it */
     int profile;             /* 1: print per-stage device times to stderr */
-    double *stage_ms;        /* optional [INDIALIGN_STAGES] per-stage device ms */
-    long long *counters;     /* optional [INDIALIGN_COUNTERS] work counters */
+    double *stage_ms;        /* optional [INDIALIGN_STAGES] per-stage device ms:
+                                seeds, seed bank, SS, gapless, local fragment,
+                                threading DP, dense local fragment, top-k, DP
+                                refinement, offset DP, weighted, total */
+    long long *counters;     /* optional [INDIALIGN_COUNTERS] work counters: NW cells,
+                                chain residue visits, bank residue visits, bank
+                                items, chains, NW-chain kernel launches, bank
+                                kernel launches, all kernel launches */
+    double *kernel_ms;       /* optional [4]: summed device ms of the NW-chain
+                                kernel and of the bank kernel, their launch counts */
     double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
                                 best {score,R,t} after each search stage */
 } IndialignBatchOptions;
@@ -125,6 +133,10 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
                                     const uint8_t *d_pv, const uint8_t *d_nv,
                                     const double *lnorm, const NativeConfig *cfg,
                                     const IndialignBatchOptions *opts, double *d_out);
+
+/* Measured FP64 FMA throughput of the device in TFLOP/s (the roofline
+ * denominator for the search kernels, which are FP64 SIMT work). */
+int indialign_fp64_peak(int device, double *tflops);
 
 /* Text of the last error on this thread ("" if none). */
 const char *indialign_last_error(void);

@@ -37,6 +37,7 @@ class BatchOptions(ctypes.Structure):
                 ("use_graph", ctypes.c_int), ("profile", ctypes.c_int),
                 ("stage_ms", ctypes.POINTER(ctypes.c_double)),
                 ("counters", ctypes.POINTER(ctypes.c_longlong)),
+                ("kernel_ms", ctypes.POINTER(ctypes.c_double)),
                 ("stage_best", ctypes.POINTER(ctypes.c_double))]
 
 
@@ -72,6 +73,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(NativeConfig),
         ctypes.POINTER(BatchOptions), ctypes.c_void_p]
     lib.indialign_tmscore_search_device.restype = ctypes.c_int
+    lib.indialign_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.indialign_fp64_peak.restype = ctypes.c_int
     if path is None:
         _lib = lib
     return lib
@@ -87,7 +90,8 @@ def last_error() -> str:
 
 def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = False,
            stage_ms: np.ndarray | None = None, counters: np.ndarray | None = None,
-           stage_best: np.ndarray | None = None):
+           stage_best: np.ndarray | None = None, kernel_ms: np.ndarray | None = None,
+           stream: int | None = None):
     """Run the batched search on the GPU.
 
     pairs: objects with .pred/.native (L,3) float64, .valid/.pred_valid/
@@ -106,6 +110,11 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     if counters is not None:
         assert counters.dtype == np.int64 and counters.size >= COUNTERS
         opts.counters = counters.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    if kernel_ms is not None:
+        assert kernel_ms.dtype == np.float64 and kernel_ms.size >= 4
+        opts.kernel_ms = kernel_ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    if stream is not None:
+        opts.stream = ctypes.c_void_p(stream)
     if stage_best is not None:
         assert stage_best.dtype == np.float64 and stage_best.size >= pk.n * TRACE_STAGES * 13
         opts.stage_best = stage_best.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
@@ -114,3 +123,12 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     if rc != 0:
         raise IndialignError(f"indialign_tmscore_search_batch_ex rc={rc}: {last_error()}")
     return abi.results_to_numpy(res, pk.n)
+
+
+def fp64_peak_tflops(device: int = 0) -> float:
+    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
+    v = ctypes.c_double(0.0)
+    rc = load().indialign_fp64_peak(device, ctypes.byref(v))
+    if rc != 0:
+        raise IndialignError(f"indialign_fp64_peak rc={rc}")
+    return v.value

@@ -26,7 +26,7 @@ template <bool SMEM>
 __global__ void __launch_bounds__(kBankChunk)
 k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
        int ntasks, const ScanOut *__restrict__ scan, int *counter,
-       double *__restrict__ item_res, int *err, int nmax) {
+       double *__restrict__ item_res, int *err, int nmax, unsigned long long *ctr) {
     extern __shared__ __align__(16) char smem[];
     __shared__ BankSmem ctl;
     __shared__ uint64_t bar;
@@ -149,7 +149,8 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             }
             if (running) {
                 if (cnt >= 3) kabsch_from_moments(m, 3.0, R, t);
-                if (cnt == prev || ++iter >= T.max_iter) running = false;
+                ++iter;
+                if (cnt == prev || iter >= T.max_iter) running = false;
                 prev = cnt;
             }
         }
@@ -167,6 +168,20 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 if (!T.use_d8 || d2 <= sd8sq) sum += 1.0 / (1.0 + d2 / d0sq);
             }
             score = sum / fmax(T.lnorm, 1.0);
+        }
+        {
+            // residue visits: seed pass + `iter` cutoff passes + score pass
+            unsigned long long visits = active && !skip ? (unsigned long long)(iter + 2) * n : 0ull;
+            unsigned long long items = active ? 1ull : 0ull;
+#pragma unroll
+            for (int o2 = 16; o2 > 0; o2 >>= 1) {
+                visits += __shfl_xor_sync(0xffffffffu, visits, o2);
+                items += __shfl_xor_sync(0xffffffffu, items, o2);
+            }
+            if ((threadIdx.x & 31) == 0 && items) {
+                atomicAdd(ctr + CTR_BANK_RES, visits);
+                atomicAdd(ctr + CTR_BANK_ITEMS, items);
+            }
         }
         if (active) {
             double *o = item_res + (size_t)(T.item_base + li) * kRec;
@@ -237,14 +252,14 @@ size_t bank_smem_bytes(int nmax) {
 
 void launch_bank(const BankTask *tasks, const int *chunk_begin, int ntasks,
                  const ScanOut *scan, int *counter, double *item_res, int *err,
-                 int nmax, int grid, cudaStream_t st) {
+                 int nmax, int grid, unsigned long long *ctr, cudaStream_t st) {
     size_t sm = bank_smem_bytes(nmax);
     if (sm <= kBankSmemMax) {
         k_bank<true><<<grid, kBankChunk, sm, st>>>(tasks, chunk_begin, ntasks, scan, counter,
-                                                   item_res, err, nmax);
+                                                   item_res, err, nmax, ctr);
     } else {
         k_bank<false><<<grid, kBankChunk, 0, st>>>(tasks, chunk_begin, ntasks, scan, counter,
-                                                   item_res, err, nmax);
+                                                   item_res, err, nmax, ctr);
     }
 }
 

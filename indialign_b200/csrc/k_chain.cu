@@ -64,9 +64,10 @@ struct NWParams {
 // Fill the trace of the NW DP for (R,t) and return the aligned pair count;
 // the pairs are written (reversed) to al.
 IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
-                    double *bH, uint32_t *trace, uint32_t *al) {
+                    double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
+    if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
     const int wpr = (nlen + 15) >> 4;
     for (int j = lane; j <= nlen; j += 32) bH[j] = 0.0;
     __syncwarp();
@@ -158,8 +159,9 @@ IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const dou
 // Kabsch on the aligned pairs + their compact TM (no d8)
 // (indialign_c/align.h:106-124).
 IA_DEV double aligned_kabsch(const Pts &x, const uint32_t *al, int na, double d0, double lnorm,
-                             double *R, double *t) {
+                             double *R, double *t, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
+    if (lane == 0) atomicAdd(ctr + CTR_CHAIN_RES, 2ull * (unsigned long long)na);
     Moments m;
     m.clear();
     for (int k = lane; k < na; k += 32) {
@@ -188,7 +190,7 @@ IA_DEV double aligned_kabsch(const Pts &x, const uint32_t *al, int na, double d0
 // side; the first maximum in cutoff order wins.
 IA_DEV double lite_detailed(const Pts &x, const uint32_t *al, int na, const double *R0,
                             const double *t0, const double *dcut, double d0, double sd8,
-                            double lnorm, double *Ro, double *to) {
+                            double lnorm, double *Ro, double *to, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31, g = lane >> 2, sub = lane & 3;
     const bool grp = g < kDetC;
     const double cut = dcut[grp ? g : 0];
@@ -220,10 +222,13 @@ IA_DEV double lite_detailed(const Pts &x, const uint32_t *al, int na, const doub
         cnt += __shfl_xor_sync(kFull, cnt, 2);
         if (running) {
             if (cnt >= 3) kabsch_from_moments(m, 3.0, R, t);
-            if (cnt == prev || ++iter >= 8) running = false;
+            ++iter;
+            if (cnt == prev || iter >= 8) running = false;
             prev = cnt;
         }
     }
+    // residue visits: each active group ran `iter` passes + 1 score pass
+    if (sub == 0 && grp) atomicAdd(ctr + CTR_CHAIN_RES, (unsigned long long)(iter + 1) * na);
     const double d0sq = fmax(d0 * d0, 1e-12), sd8sq = sd8 * sd8;
     double s = 0.0;
     if (grp) {
@@ -332,6 +337,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
         }
         const int chain = (c - chunk_begin[ti]) * kChainWarps + warp;
         if (chain < T.n_chains) {
+            if (lane == 0) atomicAdd(b.ctr + CTR_CHAINS, 1ull);
             const int gaps = T.gaps;
             const int si = chain / gaps, g = chain % gaps;
             const double gap = (gaps == 2 ? g : si) == 0 ? T.gap0 : T.gap1;
@@ -370,7 +376,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 // EMIT: one alignment; aligned coordinates, count and (for
                 // SMAT_DP) the Kabsch on it with its compact score.
                 int na = 0;
-                if (live) na = nw_align(x, pr, R, t, bH, trace, al);
+                if (live) na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
                 if (lane == 0) T.na_out[si] = na;
                 double *aP = T.alP + (size_t)si * T.al_cap * 3;
                 double *aQ = T.alQ + (size_t)si * T.al_cap * 3;
@@ -385,7 +391,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 }
                 if (T.smode == SMAT_DP && na >= 3) {
                     double nR[9], nt[3];
-                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt);
+                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt, b.ctr);
                     double *o = T.res + (size_t)si * kRec;
                     if (lane < kRec) o[lane] = lane == 0 ? s : (lane < 10 ? nR[lane - 1] : nt[lane - 10]);
                 }
@@ -395,11 +401,11 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 double bs = 0.0, bR[9], bt[3];
                 set_identity(bR, bt);
                 for (int it = 0; live && it < T.max_iter; it++) {
-                    const int na = nw_align(x, pr, R, t, bH, trace, al);
+                    const int na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
                     if (na < 3) break;  // same transform -> same alignment next time
                     double nR[9], nt[3], dR[9], dt[3];
-                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt);
-                    double ds = lite_detailed(x, al, na, nR, nt, I.dcut, I.d0, T.sd8, I.lnorm, dR, dt);
+                    double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt, b.ctr);
+                    double ds = lite_detailed(x, al, na, nR, nt, I.dcut, I.d0, T.sd8, I.lnorm, dR, dt, b.ctr);
                     if (ds > s) {
                         s = ds;
 #pragma unroll

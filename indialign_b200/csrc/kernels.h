@@ -33,6 +33,20 @@ struct DevBatch {
     int *kv;               // [2*total] sort records / SS partners
     const uint64_t *fnv_pow;  // [maxN+1] FNV prime powers
     int *err;              // device error word
+    unsigned long long *ctr;  // [kCounters] work counters (see enum Counter)
+};
+
+// Work counters, accumulated on device per batch.
+enum Counter {
+    CTR_NW_CELLS = 0,     // Needleman-Wunsch cells (score + DP)
+    CTR_CHAIN_RES,        // residue visits of Kabsch / refine passes in chains
+    CTR_BANK_RES,         // residue visits of bank refine + score passes
+    CTR_BANK_ITEMS,       // (seed, cutoff) items refined
+    CTR_CHAINS,           // NW chains run
+    CTR_CHAIN_LAUNCHES,   // k_chain launches (host-counted)
+    CTR_BANK_LAUNCHES,    // k_bank launches (host-counted)
+    CTR_LAUNCHES,         // all kernel launches (host-counted)
+    kCounters
 };
 
 // k_misc.cu
@@ -56,7 +70,8 @@ void launch_scan(const int *counts, int *begins, int ntasks, ScanOut *out, int *
 // k_bank.cu
 size_t bank_smem_bytes(int nmax);
 void launch_bank(const BankTask *tasks, const int *chunk_begin, int ntasks, const ScanOut *scan,
-                 int *counter, double *item_res, int *err, int nmax, int grid, cudaStream_t st);
+                 int *counter, double *item_res, int *err, int nmax, int grid,
+                 unsigned long long *ctr, cudaStream_t st);
 void launch_reduce_bank(const BankTask *tasks, int ntasks, const double *item_res,
                         PairState *state, cudaStream_t st);
 cudaError_t bank_set_attributes();

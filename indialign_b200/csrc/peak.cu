@@ -1,0 +1,55 @@
+// FP64 pipe throughput probe: the denominator of the search kernels'
+// roofline.  The search is FP64 SIMT work (score matrices, NW, Kabsch); it
+// uses neither HBM bandwidth nor tensor cores to any extent, so its ceiling
+// is the FP64 FMA rate of the SMs, measured here with independent FMA chains
+// (8 per thread, enough to hide FMA latency at full occupancy).
+#include <cuda_runtime.h>
+
+#include "../../include/indialign_b200.h"
+
+namespace ia {
+
+__global__ void k_fp64_fma(double *out, int iters, double a, double b) {
+    double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
+    double x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; i++) {
+        x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+        x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+    double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+}  // namespace ia
+
+extern "C" int indialign_fp64_peak(int device, double *tflops) {
+    if (!tflops) return INDIALIGN_E_INPUT;
+    if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return INDIALIGN_E_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device < 0 ? 0 : device) != cudaSuccess)
+        return INDIALIGN_E_CUDA;
+    double *d = nullptr;
+    if (cudaMalloc(&d, 64) != cudaSuccess) return INDIALIGN_E_CUDA;
+    const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    ia::k_fp64_fma<<<blocks, threads>>>(d, iters / 8, 0.999999, 1e-7);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 5; r++) {
+        cudaEventRecord(e0);
+        ia::k_fp64_fma<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) best = ms;
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) return INDIALIGN_E_CUDA;
+    *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3) / 1e12;
+    return INDIALIGN_OK;
+}

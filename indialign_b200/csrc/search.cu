@@ -86,12 +86,12 @@ struct Ctx {
     DBuf<double> item_res, chain_res, alP, alQ, thread_rec, off_start, off_res, gbh, out, snap;
     DBuf<int> lay_i;
     DBuf<long long> lay_l;
+    DBuf<unsigned long long> ctr;
+    std::vector<cudaEvent_t> ev_pool;
     std::vector<double> h_pred, h_nat, h_lnorm;
     std::vector<uint8_t> h_v, h_pv, h_nv;
     std::vector<int> h_off, h_len, h_bitoff;
     int fnv_n = 0;
-    cudaEvent_t ev[2 * INDIALIGN_STAGES + 2];
-    bool events = false;
 };
 
 static std::mutex g_pool_mu;
@@ -166,7 +166,38 @@ class Runner {
     int run_stages();
     DevBatch b;
     double *snap = nullptr;  // device [n*kTrace*13] or nullptr
-    void mark(int stage) { launch_snapshot(b, snap, stage, kTrace, c_->stream); }
+    void mark(int stage) {
+        launch_snapshot(b, snap, stage, kTrace, c_->stream);
+        if (snap) launches_++;
+        stage_event(stage + 1);
+    }
+    // timing: events at stage boundaries and around every chain / bank launch
+    bool timing = false;
+    std::vector<std::pair<int, cudaEvent_t>> stage_ev;     // (boundary id, event)
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chain_ev, bank_ev;
+    long long launches_ = 0, chain_launches_ = 0, bank_launches_ = 0;
+    cudaEvent_t new_event() {
+        cudaEvent_t e = nullptr;
+        if (!c_->ev_pool.empty()) {
+            e = c_->ev_pool.back();
+            c_->ev_pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    }
+    void stage_event(int id) {
+        if (!timing) return;
+        cudaEvent_t e = new_event();
+        cudaEventRecord(e, c_->stream);
+        stage_ev.push_back({id, e});
+    }
+    void recycle() {
+        for (auto &x : stage_ev) c_->ev_pool.push_back(x.second);
+        for (auto &x : chain_ev) { c_->ev_pool.push_back(x.first); c_->ev_pool.push_back(x.second); }
+        for (auto &x : bank_ev) { c_->ev_pool.push_back(x.first); c_->ev_pool.push_back(x.second); }
+        stage_ev.clear(); chain_ev.clear(); bank_ev.clear();
+    }
     int pmax = 0, nmax = 0, Nmax = 0;
 
   private:
@@ -367,14 +398,26 @@ int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early) 
     pc.early_term = early >= 0 ? early : cfg_.early;
     launch_plan_bank(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
+    launches_ += 4;
+    bank_launches_++;
     int nmx = Nmax;
     size_t sm = bank_smem_bytes(nmx);
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bank_kernel_ptr(sm <= kBankSmemMax),
                                                      kBankChunk, sm <= kBankSmemMax ? sm : 0));
     if (per_sm < 1) per_sm = 1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        e0 = new_event();
+        e1 = new_event();
+        cudaEventRecord(e0, c_->stream);
+    }
     launch_bank(c_->btasks.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->item_res.p,
-                c_->err.p, nmx, c_->sms * per_sm, c_->stream);
+                c_->err.p, nmx, c_->sms * per_sm, b.ctr, c_->stream);
+    if (timing) {
+        cudaEventRecord(e1, c_->stream);
+        bank_ev.push_back({e0, e1});
+    }
     launch_reduce_bank(c_->btasks.p, L.ntasks, c_->item_res.p, b.state, c_->stream);
     CK(cudaGetLastError());
     return INDIALIGN_OK;
@@ -398,10 +441,22 @@ int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, b
     pc.iters = iters;
     launch_plan_chain(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        e0 = new_event();
+        e1 = new_event();
+        cudaEventRecord(e0, c_->stream);
+    }
     launch_chain(b, c_->ctasks.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->gtrace.p,
                  trace_words_, c_->gbh.p, c_->gal.p, pmax, nmax, chain_flags_, chain_grid_,
                  c_->stream);
+    if (timing) {
+        cudaEventRecord(e1, c_->stream);
+        chain_ev.push_back({e0, e1});
+    }
     if (reduce) launch_reduce_chain(b, pc, c_->stream);
+    launches_ += reduce ? 4 : 3;
+    chain_launches_++;
     CK(cudaGetLastError());
     return INDIALIGN_OK;
 }
@@ -414,6 +469,7 @@ int Runner::glue(int op, double thr, const double *recs, const int *idx) {
     a.recs = recs;
     a.idx = idx;
     launch_glue(b, a, c_->stream);
+    launches_++;
     CK(cudaGetLastError());
     return INDIALIGN_OK;
 }
@@ -444,6 +500,7 @@ int Runner::run_stages() {
     mark(0);
     // 2b. SS seeds IA2 + IA4, rescored (indialign.cpp:106-116, ss.h:87-164)
     launch_ss(b, st);
+    launches_++;
     RUN(glue(G_SS_BEGIN));
     RUN(chain(CH_SS2, L_pair, 1, nullptr, nullptr, false));
     RUN(bank(BK_DET_SS, L_detss));
@@ -457,6 +514,7 @@ int Runner::run_stages() {
     RUN(dp_full());
     RUN(glue(G_SS_DP));
     launch_rescore(b, REC_SS, 0, st);
+    launches_++;
     RUN(glue(G_SS_FINISH));
     mark(1);
     // 2c. gapless threading (indialign.cpp:118-123)
@@ -467,21 +525,25 @@ int Runner::run_stages() {
     RUN(glue(G_GATE, cfg_.r1));
     RUN(chain(CH_LOCAL, L_localn, 0));
     launch_rescore(b, REC_STAGE, 1, st);
+    launches_++;
     RUN(glue(G_STAGE_UPDATE));
     mark(3);
     RUN(glue(G_GATE, cfg_.r1));
     RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p));
     RUN(chain(CH_THREAD, L_threadch, 1, c_->thread_rec.p));
     launch_rescore(b, REC_STAGE, 1, st);
+    launches_++;
     RUN(glue(G_STAGE_UPDATE));
     mark(4);
     RUN(glue(G_GATE, cfg_.r2));
     RUN(chain(CH_LOCAL, L_locald, 1));
     launch_rescore(b, REC_STAGE, 1, st);
+    launches_++;
     RUN(glue(G_STAGE_UPDATE));
     mark(5);
     // 4. top-50% distance seed (indialign.cpp:154-177)
     launch_topk(b, st);
+    launches_++;
     RUN(bank(BK_TOPK, L_topk));
     RUN(glue(G_STAGE_UPDATE));
     mark(6);
@@ -489,19 +551,23 @@ int Runner::run_stages() {
     RUN(glue(G_DPF_BEGIN));
     RUN(dp_full());
     launch_rescore(b, REC_DP, 0, st);
+    launches_++;
     RUN(glue(G_DPF_UPDATE));
     launch_rescore(b, REC_TMP, 0, st);
+    launches_++;
     RUN(glue(G_TMP_UPDATE));
     if (cfg_.dp_iter > 0) {
         RUN(glue(G_IDP_START));
         RUN(chain(CH_SINGLE, L_single, cfg_.dp_iter));
         launch_rescore(b, REC_STAGE, 1, st);
+        launches_++;
         RUN(glue(G_STAGE_UPDATE));
         int extra = cfg_.dp_iter < 5 ? 5 - cfg_.dp_iter : 0;
         if (extra > 0) {
             RUN(glue(G_EXTRA_START));
             RUN(chain(CH_SINGLE, L_single, extra));
             launch_rescore(b, REC_STAGE, 1, st);
+            launches_++;
             RUN(glue(G_STAGE_UPDATE));
         }
     }
@@ -510,13 +576,16 @@ int Runner::run_stages() {
         // 5b. DP from offset Kabsch starts (indialign.cpp:229-256)
         launch_offset_starts(b, c_->off_start.p, L_offslots.d_pair, L_offslots.d_aux,
                              L_offslots.ntasks, st);
+        launches_++;
         RUN(chain(CH_OFFDP, L_offdp, cfg_.dp_iter, c_->off_start.p, c_->off_res.p));
         launch_rescore_list(b, c_->off_res.p, L_offslots.d_pair, L_offslots.ntasks, st);
+        launches_++;
         RUN(glue(G_OFFDP_UPDATE, 0.0, c_->off_res.p, L_offdp.d_aux));
     }
     mark(8);
     // 6. weighted TM refinement (indialign.cpp:258-264)
     launch_weighted(b, st);
+    launches_++;
     mark(9);
     CK(cudaGetLastError());
     return INDIALIGN_OK;
@@ -558,6 +627,13 @@ struct Source {
 static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results, double *d_out,
                      const IndialignBatchOptions *opts) {
     const int n = src.n();
+    cudaStream_t own = c->stream;
+    if (opts && opts->stream) c->stream = static_cast<cudaStream_t>(opts->stream);
+    struct Restore {
+        Ctx *c;
+        cudaStream_t s;
+        ~Restore() { c->stream = s; }
+    } restore{c, own};
     cudaStream_t st = c->stream;
     // ---- pack (pair blocks padded to an even residue count) ----
     c->h_off.resize(n + 1);
@@ -628,6 +704,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     CK(c->bits.ensure((size_t)bits + 1));
     CK(c->hashes.ensure((size_t)n * kMaxSeeds));
     CK(c->kv.ensure(2 * T));
+    CK(c->ctr.ensure(kCounters));
     if (c->fnv_n < Nmax + 1) {
         std::vector<uint64_t> pw(Nmax + 1);
         for (int z = 0; z <= Nmax; z++) pw[z] = fnv_pow_host(z);
@@ -647,6 +724,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaMemcpyAsync(c->nv.p, c->h_nv.data(), total, cudaMemcpyHostToDevice, st));
     }
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(c->ctr.p, 0, kCounters * sizeof(unsigned long long), st));
     DevBatch b;
     b.n = n;
     b.off = c->off.p;
@@ -676,6 +754,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     b.kv = c->kv.p;
     b.fnv_pow = c->fnv_pow.p;
     b.err = c->err.p;
+    b.ctr = c->ctr.p;
     if (!on_host) {
         // caller's offsets to the device (scratch doubles as staging), repack
         CK(cudaMemcpyAsync(c->scratch.p, src.off, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -689,16 +768,20 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaEventCreate(&e1));
         CK(cudaEventRecord(e0, st));
     }
+    Runner r(c, cfg, n);
+    r.b = b;
+    r.Nmax = Nmax;
+    r.timing = opts && (opts->stage_ms || opts->kernel_ms);
+    r.stage_event(0);
     // ---- seeds ----
     launch_prep(b, cfg.use_frag, st);
     launch_anchor(b, st);
+    r.launches_ += 2;
     CK(cudaGetLastError());
     std::vector<PairInfo> info(n);
     CK(cudaMemcpyAsync(info.data(), c->info.p, n * sizeof(PairInfo), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    Runner r(c, cfg, n);
-    r.b = b;
-    r.Nmax = Nmax;
+    r.stage_event(100);  // seeds done
     if (opts && opts->stage_best) {
         CK(c->snap.ensure((size_t)n * kTrace * kRec));
         CK(cudaMemsetAsync(c->snap.p, 0, (size_t)n * kTrace * kRec * 8, st));
@@ -710,9 +793,10 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     if (rc) return rc;
     if (prof) CK(cudaEventRecord(e1, st));
     // ---- results ----
-    std::vector<PairState> state(n);
+    std::vector<PairState> state(d_out ? 0 : n);
     int err = 0;
-    CK(cudaMemcpyAsync(state.data(), c->state.p, n * sizeof(PairState), cudaMemcpyDeviceToHost, st));
+    if (!d_out)
+        CK(cudaMemcpyAsync(state.data(), c->state.p, n * sizeof(PairState), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&err, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (prof) {
@@ -732,6 +816,44 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     }
     if (opts && opts->stage_best && r.snap)
         CK(cudaMemcpy(opts->stage_best, r.snap, (size_t)n * kTrace * kRec * 8, cudaMemcpyDeviceToHost));
+    if (opts && opts->counters) {
+        unsigned long long h[kCounters];
+        CK(cudaMemcpy(h, c->ctr.p, sizeof(h), cudaMemcpyDeviceToHost));
+        h[CTR_CHAIN_LAUNCHES] = r.chain_launches_;
+        h[CTR_BANK_LAUNCHES] = r.bank_launches_;
+        h[CTR_LAUNCHES] = r.launches_;
+        for (int k = 0; k < kCounters && k < INDIALIGN_COUNTERS; k++) opts->counters[k] = (long long)h[k];
+    }
+    if (r.timing) {
+        // stage boundaries: 0 start, 100 seeds done, s+1 after trace stage s
+        float ms = 0;
+        cudaEvent_t prev = nullptr;
+        double stage[INDIALIGN_STAGES] = {0};
+        for (auto &x : r.stage_ev) {
+            if (prev) {
+                CK(cudaEventElapsedTime(&ms, prev, x.second));
+                int slot = x.first == 100 ? 0 : x.first;  // seeds -> 0, trace stage s -> s+1
+                if (slot >= 0 && slot < INDIALIGN_STAGES - 1) stage[slot] += ms;
+            }
+            prev = x.second;
+        }
+        if (!r.stage_ev.empty()) {
+            CK(cudaEventElapsedTime(&ms, r.stage_ev.front().second, r.stage_ev.back().second));
+            stage[INDIALIGN_STAGES - 1] = ms;
+        }
+        if (opts->stage_ms)
+            for (int k = 0; k < INDIALIGN_STAGES; k++) opts->stage_ms[k] = stage[k];
+        if (opts->kernel_ms) {
+            double ch = 0, bk = 0;
+            for (auto &x : r.chain_ev) { CK(cudaEventElapsedTime(&ms, x.first, x.second)); ch += ms; }
+            for (auto &x : r.bank_ev) { CK(cudaEventElapsedTime(&ms, x.first, x.second)); bk += ms; }
+            opts->kernel_ms[0] = ch;
+            opts->kernel_ms[1] = bk;
+            opts->kernel_ms[2] = (double)r.chain_ev.size();
+            opts->kernel_ms[3] = (double)r.bank_ev.size();
+        }
+        r.recycle();
+    }
     if (d_out) {
         launch_export(b, d_out, st);
         CK(cudaGetLastError());
