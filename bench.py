@@ -305,7 +305,8 @@ def main():
             r = cpu_baseline(pairs, args.cpu_sample)
             if r:
                 cpu, sample, ref_s = r
-                idx = [pairs.index(p) for p in sample]
+                pos = {id(p): k for k, p in enumerate(pairs)}
+                idx = [pos[id(p)] for p in sample]
                 d = scores[idx] - ref_s
                 cpu["parity_on_sample"] = {"min_dTM": float(d.min()), "max_abs_dTM": float(np.abs(d).max()),
                                            "pairs_below_ref_minus_1e-6": int(np.sum(d < -1e-6))}

@@ -61,73 +61,129 @@ struct NWParams {
     const uint8_t *Lp, *Ln;  // SS labels (compact order)
 };
 
+// One score-matrix entry (indialign_c/align.h:86-98; ss.h:69-72, 118-131).
+IA_DEV double smat_entry(const NWParams &pr, double mx, double my, double mz, uint8_t lp,
+                         const double *q, int jn) {
+    if (pr.smode == SMAT_SS2) return (lp == pr.Ln[jn]) ? 1.0 : 0.0;
+    const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (pr.smode == SMAT_DP) return d2 <= pr.cut2 ? 1.0 / (1.0 + d2 * pr.inv_d0sq) : 0.0;
+    double sc = 1.0 / (1.0 + d2 * pr.inv_d0sq);
+    if (lp == pr.Ln[jn]) sc += 0.5;
+    return sc;
+}
+
+// One NW cell from its diagonal source (value), up and left (encoded), with
+// the reference's gap rule and tie order (indialign_c/nw.h:20-35).
+IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc, double gap,
+                      uint32_t &dir) {
+    const double diag = diag_src + sc;
+    const double up = fabs(up_enc) + (signbit(up_enc) ? gap : 0.0);
+    const double left = fabs(left_enc) + (signbit(left_enc) ? gap : 0.0);
+    double nh;
+    if (diag >= up && diag >= left) { nh = diag; dir = 0; }
+    else if (left >= up) { nh = left; dir = 2; }
+    else { nh = up; dir = 1; }
+    return dir == 0 ? -nh : nh;
+}
+
 // Fill the trace of the NW DP for (R,t) and return the aligned pair count;
 // the pairs are written (reversed) to al.
+//
+// Each lane owns two consecutive rows of a 64-row stripe; row r of lane l
+// computes column j at step k*P + 2l + r + j - 1 for stripe k, with period
+// P = max(nlen+1, 64).  Row 1 trails row 0 by one step inside the lane, lane
+// l trails lane l-1 by two steps, and a lane moves on to its rows of the
+// next stripe as soon as it finishes the current one (the top row of stripe
+// k+1 reads the boundary row that lane 31 wrote for stripe k at least one
+// step earlier, since P >= 64).  Per step a lane computes two independent
+// cells with one shuffle and one shared-memory column load.
 IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
                     double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
     if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
     const int wpr = (nlen + 15) >> 4;
+    const int P = max(nlen + 1, 64);
+    const int S = (plen + 63) >> 6;  // stripes
+    const double gap = pr.gap;
     for (int j = lane; j <= nlen; j += 32) bH[j] = 0.0;
     __syncwarp();
-    for (int s0 = 0; s0 < plen; s0 += 32) {
-        const int i = s0 + lane + 1;
-        const bool row_ok = i <= plen;
-        double mx = 0, my = 0, mz = 0;
-        uint8_t lp = 0;
-        if (row_ok) {
-            const double *p = x.P + 3 * (i - 1);
-            if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], mx, my, mz);
-            if (pr.smode != SMAT_DP) lp = pr.Lp[i - 1];
+    int k = 0, j0 = 1 - 2 * lane;  // stripe and row-0 column of this lane
+    int i0 = 2 * lane + 1;         // 1-based row of row 0
+    double m0x = 0, m0y = 0, m0z = 0, m1x = 0, m1y = 0, m1z = 0;
+    uint8_t l0 = 0, l1 = 0;
+    double h0 = 0.0, h1 = 0.0, h0prev = 0.0, up0prev = 0.0;
+    double q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
+    uint32_t acc0 = 0, acc1 = 0;
+    // the last stripe ends when the lane holding row plen finishes column nlen
+    const int last_lane = ((plen - 1) & 63) >> 1;
+    const int total_steps = (S - 1) * P + 2 * last_lane + 1 + nlen + 1;
+    for (int step = 0; step < total_steps; step++) {
+        // up value for row 0: lane l-1's row 1 (same column), or the boundary
+        double up0 = __shfl_up_sync(kFull, h1, 1);
+        if (j0 > P) {  // next stripe
+            j0 -= P;
+            k++;
+            i0 += 64;
         }
-        const bool last = s0 + 32 >= plen;
-        double h_enc = 0.0, up_prev = 0.0;
-        uint32_t acc = 0;
-        uint32_t *trow = trace + (size_t)(i - 1) * wpr;
-        const int nsteps = nlen + 31;
-        for (int step = 0; step < nsteps; step++) {
-            const int j = step - lane + 1;
-            double up_enc = __shfl_up_sync(kFull, h_enc, 1);
-            const bool jok = j >= 1 && j <= nlen;
-            if (lane == 0) up_enc = jok ? bH[j] : 0.0;
-            if (row_ok && jok) {
-                double sc;
-                if (pr.smode == SMAT_SS2) {
-                    sc = (lp == pr.Ln[j - 1]) ? 1.0 : 0.0;
-                } else {
-                    const double *q = x.Q + 3 * (j - 1);
-                    const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
-                    const double d2 = dx * dx + dy * dy + dz * dz;
-                    if (pr.smode == SMAT_DP) {
-                        sc = d2 <= pr.cut2 ? 1.0 / (1.0 + d2 * pr.inv_d0sq) : 0.0;
-                    } else {
-                        sc = 1.0 / (1.0 + d2 * pr.inv_d0sq);
-                        if (lp == pr.Ln[j - 1]) sc += 0.5;
-                    }
-                }
-                const double up_v = fabs(up_enc), hl_v = fabs(h_enc);
-                const double diag = up_prev + sc;
-                const double up = up_v + (signbit(up_enc) ? pr.gap : 0.0);
-                const double left = hl_v + (signbit(h_enc) ? pr.gap : 0.0);
-                double nh;
-                uint32_t dir;
-                if (diag >= up && diag >= left) { nh = diag; dir = 0; }
-                else if (left >= up) { nh = left; dir = 2; }
-                else { nh = up; dir = 1; }
-                h_enc = dir == 0 ? -nh : nh;
-                up_prev = up_v;
-                const int jj = j - 1;
-                acc |= dir << (2 * (jj & 15));
-                if ((jj & 15) == 15 || j == nlen) {
-                    trow[jj >> 4] = acc;
-                    acc = 0;
-                }
-                if (lane == 31 && !last) bH[j] = h_enc;
+        const bool in_stripe = k < S;
+        if (j0 == 1 && in_stripe) {  // entering the stripe: load the two rows
+            h0 = h1 = h0prev = up0prev = 0.0;
+            acc0 = acc1 = 0;
+            if (i0 <= plen) {
+                const double *p = x.P + 3 * (i0 - 1);
+                if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], m0x, m0y, m0z);
+                if (pr.smode != SMAT_DP) l0 = pr.Lp[i0 - 1];
+            }
+            if (i0 + 1 <= plen) {
+                const double *p = x.P + 3 * i0;
+                if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], m1x, m1y, m1z);
+                if (pr.smode != SMAT_DP) l1 = pr.Lp[i0];
             }
         }
-        __syncwarp();
+        const bool c0 = in_stripe && j0 >= 1 && j0 <= nlen;      // row 0 column valid
+        const bool c1 = in_stripe && j0 >= 2 && j0 <= nlen + 1;  // row 1 column j0-1 valid
+        if (lane == 0) up0 = (c0 && k > 0) ? bH[j0] : 0.0;
+        double q0x = 0, q0y = 0, q0z = 0;
+        if (c0 && pr.smode != SMAT_SS2) {
+            const double *q = x.Q + 3 * (j0 - 1);
+            q0x = q[0]; q0y = q[1]; q0z = q[2];
+        }
+        double n0 = h0, n1 = h1;
+        if (c1 && i0 + 1 <= plen) {  // row 1, column j0-1
+            const int jn = j0 - 2;
+            const double q[3] = {q1x, q1y, q1z};
+            const double sc = smat_entry(pr, m1x, m1y, m1z, l1, q, jn);
+            uint32_t dir;
+            n1 = nw_cell(h0prev, sc, h0, h1, gap, dir);
+            acc1 |= dir << (2 * (jn & 15));
+            if ((jn & 15) == 15 || jn == nlen - 1) {
+                trace[(size_t)i0 * wpr + (jn >> 4)] = acc1;
+                acc1 = 0;
+            }
+            if (lane == 31 && k + 1 < S) bH[jn + 1] = n1;
+        }
+        if (c0 && i0 <= plen) {  // row 0, column j0
+            const int jn = j0 - 1;
+            const double q[3] = {q0x, q0y, q0z};
+            const double sc = smat_entry(pr, m0x, m0y, m0z, l0, q, jn);
+            uint32_t dir;
+            n0 = nw_cell(up0prev, sc, up0, h0, gap, dir);
+            acc0 |= dir << (2 * (jn & 15));
+            if ((jn & 15) == 15 || jn == nlen - 1) {
+                trace[(size_t)(i0 - 1) * wpr + (jn >> 4)] = acc0;
+                acc0 = 0;
+            }
+        }
+        h0prev = fabs(h0);
+        up0prev = fabs(up0);
+        h0 = n0;
+        h1 = n1;
+        q1x = q0x; q1y = q0y; q1z = q0z;
+        j0++;
     }
+    __syncwarp();
     // traceback from (plen, nlen): diag emits a pair, up steps i, else j
     int i = plen, j = nlen, cnt = 0, rb = -1, cw = -1;
     uint32_t word = 0;
@@ -259,10 +315,10 @@ IA_DEV double lite_detailed(const Pts &x, const uint32_t *al, int na, const doub
 
 // ---- the chain kernel ----------------------------------------------------
 struct ChainCtl {
-    int chunk, task;
+    int chunk, task, next;
 };
 
-__global__ void __launch_bounds__(32 * kChainWarps)
+__global__ void __launch_bounds__(32 * kChainWarps, 3)
 k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         int ntasks, const ScanOut *__restrict__ scan, int *counter, uint32_t *gtrace,
         size_t trace_words, double *gbh, uint32_t *gal, int pmax, int nmax, int flags) {
@@ -307,6 +363,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             }
             ctl.chunk = c;
             ctl.task = t;
+            ctl.next = 0;
         }
         __syncthreads();
         const int c = ctl.chunk, ti = ctl.task;
@@ -335,8 +392,14 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             }
             staged = T.pair;
         }
-        const int chain = (c - chunk_begin[ti]) * kChainWarps + warp;
-        if (chain < T.n_chains) {
+        // warps of the CTA pull the chunk's chains one at a time, so a long
+        // chain does not hold the other warps at a barrier
+        for (;;) {
+            int idx = 0;
+            if (lane == 0) idx = atomicAdd(&ctl.next, 1);
+            idx = __shfl_sync(kFull, idx, 0);
+            const int chain = (c - chunk_begin[ti]) * kChainChunk + idx;
+            if (idx >= kChainChunk || chain >= T.n_chains) break;
             if (lane == 0) atomicAdd(b.ctr + CTR_CHAINS, 1ull);
             const int gaps = T.gaps;
             const int si = chain / gaps, g = chain % gaps;

@@ -218,7 +218,7 @@ __global__ void k_plan_chain(DevBatch b, PlanCtx c) {
     if (on && T.n_chains == 0 && (c.kind == CH_LOCAL || c.kind == CH_THREAD || c.kind == CH_SINGLE))
         rec_ident(S.rec[REC_STAGE], kScoreInit);
     c.ctasks[s] = T;
-    c.counts[s] = (T.n_chains + kChainWarps - 1) / kChainWarps;
+    c.counts[s] = (T.n_chains + kChainChunk - 1) / kChainChunk;
 }
 
 // ---- chain reductions (warp per pair) ---------------------------------------
