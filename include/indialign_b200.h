@@ -138,6 +138,10 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
  * denominator for the search kernels, which are FP64 SIMT work). */
 int indialign_fp64_peak(int device, double *tflops);
 
+/* Diagnostic: y[i] = the search kernels' Newton-Raphson reciprocal of x[i],
+ * computed on the device (host arrays of n doubles). */
+int indialign_selftest_rcp(int n, const double *x, double *y);
+
 /* Text of the last error on this thread ("" if none). */
 const char *indialign_last_error(void);
 

@@ -102,10 +102,68 @@ IA_DEV void jacobi_rot(double (&A)[4][4], double (&V)[4][4]) {
     }
 }
 
-// Horn's 4x4 from the 3x3 covariance H, 8 cyclic Jacobi sweeps, dominant
-// eigenvector (first index on ties) -> rotation (indialign_c/core.h:64-90).
-IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
-    double A[4][4], V[4][4];
+// Reciprocal by Newton-Raphson (y <- y + y(1 - xy), quadratic convergence)
+// from the hardware single-precision approximation: two steps take the
+// ~2^-22 seed error below double rounding, so the result is within 1 ulp of
+// 1/x.  Valid for |x| in the normal float range.
+IA_DEV double rcp_nr(double x) {
+    float yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(__double2float_rn(x)));
+    double y = (double)yf;
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+// Rotation (c, s, t) annihilating A[p][q] (the formulas of
+// indialign_c/core.h:42-45), with the divides and square roots done by
+// rcp_nr / rsqrt (<= 1-2 ulp each instead of correctly rounded).
+IA_DEV void rot_fast(double app, double aqq, double apq, double &c, double &s, double &t) {
+    const double tau = (aqq - app) * rcp_nr(2.0 * apq);
+    const double u = fma(tau, tau, 1.0);
+    const double sq = u * rsqrt(u);
+    const double r = rcp_nr(fabs(tau) + sq);
+    t = tau >= 0 ? r : -r;
+    c = rsqrt(fma(t, t, 1.0));
+    s = t * c;
+}
+
+template <int p, int q>
+IA_DEV void rot_apply(double (&A)[4][4], double (&V)[4][4], double c, double s, double t) {
+    const double apq = A[p][q];
+    A[p][p] -= t * apq;
+    A[q][q] += t * apq;
+    A[p][q] = A[q][p] = 0.0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        if (r == p || r == q) continue;
+        const double rp = A[r][p], rq = A[r][q];
+        A[r][p] = A[p][r] = c * rp - s * rq;
+        A[r][q] = A[q][r] = s * rp + c * rq;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        const double vp = V[r][p], vq = V[r][q];
+        V[r][p] = c * vp - s * vq;
+        V[r][q] = s * vp + c * vq;
+    }
+}
+
+// One round of two rotations on disjoint index pairs (p1,q1), (p2,q2): both
+// parameter sets come from the same A (the (p2,q2) block is untouched by
+// the first rotation), so the two long div/sqrt chains run side by side.
+template <int p1, int q1, int p2, int q2>
+IA_DEV void jacobi_round(double (&A)[4][4], double (&V)[4][4]) {
+    double c1 = 1, s1 = 0, t1 = 0, c2 = 1, s2 = 0, t2 = 0;
+    const bool d1 = fabs(A[p1][q1]) >= 1e-15, d2 = fabs(A[p2][q2]) >= 1e-15;
+    if (d1) rot_fast(A[p1][p1], A[q1][q1], A[p1][q1], c1, s1, t1);
+    if (d2) rot_fast(A[p2][p2], A[q2][q2], A[p2][q2], c2, s2, t2);
+    if (d1) rot_apply<p1, q1>(A, V, c1, s1, t1);
+    if (d2) rot_apply<p2, q2>(A, V, c2, s2, t2);
+}
+
+IA_DEV void horn_matrix(const double (&H)[3][3], double (&A)[4][4]) {
     A[0][0] = H[0][0] + H[1][1] + H[2][2];
     A[0][1] = A[1][0] = H[1][2] - H[2][1];
     A[0][2] = A[2][0] = H[2][0] - H[0][2];
@@ -116,35 +174,24 @@ IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
     A[2][2] = -H[0][0] + H[1][1] - H[2][2];
     A[2][3] = A[3][2] = H[1][2] + H[2][1];
     A[3][3] = -H[0][0] - H[1][1] + H[2][2];
+}
+
+IA_DEV void set_eye4(double (&V)[4][4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) V[i][j] = (i == j) ? 1.0 : 0.0;
-    // The reference always runs 8 sweeps; once every off-diagonal entry is
-    // below 1e-15 of the largest diagonal entry the remaining rotations only
-    // move A and V at the level of rounding (their angles are ~1e-16), so
-    // the sweeps stop there.  Checked against the reference build: final
-    // TM-scores agree to ~1e-16 (typically 4 sweeps run).
-#pragma unroll 1
-    for (int sweep = 0; sweep < 8; sweep++) {
-        const double off = fmax(fmax(fmax(fabs(A[0][1]), fabs(A[0][2])), fmax(fabs(A[0][3]), fabs(A[1][2]))),
-                                fmax(fabs(A[1][3]), fabs(A[2][3])));
-        const double dg = fmax(fmax(fabs(A[0][0]), fabs(A[1][1])), fmax(fabs(A[2][2]), fabs(A[3][3])));
-        if (off <= 1e-15 * dg) break;
-        jacobi_rot<0, 1>(A, V);
-        jacobi_rot<0, 2>(A, V);
-        jacobi_rot<0, 3>(A, V);
-        jacobi_rot<1, 2>(A, V);
-        jacobi_rot<1, 3>(A, V);
-        jacobi_rot<2, 3>(A, V);
-    }
+}
+
+// Dominant eigenvector (first index among equal diagonal maxima) -> unit
+// quaternion -> rotation (indialign_c/core.h:76-89).
+IA_DEV void quat_to_rotation(const double (&A)[4][4], const double (&V)[4][4], double *R) {
     int best = 0;
     double bv = A[0][0];
     if (A[1][1] > bv) { best = 1; bv = A[1][1]; }
     if (A[2][2] > bv) { best = 2; bv = A[2][2]; }
     if (A[3][3] > bv) { best = 3; bv = A[3][3]; }
     double q0, q1, q2, q3;
-    // select the column without dynamic register indexing
     q0 = best == 0 ? V[0][0] : best == 1 ? V[0][1] : best == 2 ? V[0][2] : V[0][3];
     q1 = best == 0 ? V[1][0] : best == 1 ? V[1][1] : best == 2 ? V[1][2] : V[1][3];
     q2 = best == 0 ? V[2][0] : best == 1 ? V[2][1] : best == 2 ? V[2][2] : V[2][3];
@@ -164,6 +211,59 @@ IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
     R[6] = 2 * (q1 * q3 + q0 * q2);
     R[7] = 2 * (q2 * q3 - q0 * q1);
     R[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+}
+
+// The reference eigen-solve exactly: 8 cyclic sweeps in its pair order with
+// correctly rounded divides and square roots (indialign_c/core.h:29-60).
+IA_DEV void jacobi_reference(double (&A)[4][4], double (&V)[4][4]) {
+    set_eye4(V);
+#pragma unroll 1
+    for (int sweep = 0; sweep < 8; sweep++) {
+        jacobi_rot<0, 1>(A, V);
+        jacobi_rot<0, 2>(A, V);
+        jacobi_rot<0, 3>(A, V);
+        jacobi_rot<1, 2>(A, V);
+        jacobi_rot<1, 3>(A, V);
+        jacobi_rot<2, 3>(A, V);
+    }
+}
+
+// Horn's 4x4 from the 3x3 covariance H -> dominant eigenvector -> rotation
+// (indialign_c/core.h:64-90).
+//
+// Fast path: Jacobi sweeps in the round order (0,1)(2,3) | (0,2)(1,3) |
+// (0,3)(1,2) with rot_fast, stopping once every off-diagonal entry is below
+// 1e-15 of the largest diagonal entry.  A converged Jacobi returns the
+// dominant eigenvector to rounding whatever the rotation order, as long as
+// the top eigenvalue is separated; when the two largest eigenvalues are
+// within 1e-4 of the spectrum's scale (about 1 solve in 3000 in this search,
+// mostly exact degeneracies) the eigenvector inside the degenerate subspace
+// depends on the rotation sequence, and the reference's own sequence is rerun.
+IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
+    double A[4][4], V[4][4];
+    horn_matrix(H, A);
+    set_eye4(V);
+#pragma unroll 1
+    for (int sweep = 0; sweep < 8; sweep++) {
+        const double off = fmax(fmax(fmax(fabs(A[0][1]), fabs(A[0][2])), fmax(fabs(A[0][3]), fabs(A[1][2]))),
+                                fmax(fabs(A[1][3]), fabs(A[2][3])));
+        const double dg = fmax(fmax(fabs(A[0][0]), fabs(A[1][1])), fmax(fabs(A[2][2]), fabs(A[3][3])));
+        if (off <= 1e-15 * dg) break;
+        jacobi_round<0, 1, 2, 3>(A, V);
+        jacobi_round<0, 2, 1, 3>(A, V);
+        jacobi_round<0, 3, 1, 2>(A, V);
+    }
+    // gap between the two largest diagonal entries
+    const double d0 = A[0][0], d1 = A[1][1], d2 = A[2][2], d3 = A[3][3];
+    const double hi01 = fmax(d0, d1), lo01 = fmin(d0, d1), hi23 = fmax(d2, d3), lo23 = fmin(d2, d3);
+    const double top = fmax(hi01, hi23);
+    const double second = fmax(fmin(hi01, hi23), fmax(lo01, lo23));
+    const double scale = fmax(fmax(fabs(d0), fabs(d1)), fmax(fabs(d2), fabs(d3)));
+    if (!(top - second >= 1e-4 * scale) || scale == 0.0) {
+        horn_matrix(H, A);
+        jacobi_reference(A, V);
+    }
+    quat_to_rotation(A, V, R);
 }
 
 // Raw first and second moments of a selected point set.

@@ -67,8 +67,10 @@ IA_DEV double smat_entry(const NWParams &pr, double mx, double my, double mz, ui
     if (pr.smode == SMAT_SS2) return (lp == pr.Ln[jn]) ? 1.0 : 0.0;
     const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
     const double d2 = dx * dx + dy * dy + dz * dz;
-    if (pr.smode == SMAT_DP) return d2 <= pr.cut2 ? 1.0 / (1.0 + d2 * pr.inv_d0sq) : 0.0;
-    double sc = 1.0 / (1.0 + d2 * pr.inv_d0sq);
+    // 1/(1 + d2/d0^2) with the Newton reciprocal (<= 1 ulp); arguments past
+    // the float range (d > ~1e19 d0) contribute nothing representable to H.
+    if (pr.smode == SMAT_DP) return d2 <= pr.cut2 ? rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30)) : 0.0;
+    double sc = rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30));
     if (lp == pr.Ln[jn]) sc += 0.5;
     return sc;
 }
@@ -184,18 +186,28 @@ IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const dou
         j0++;
     }
     __syncwarp();
-    // traceback from (plen, nlen): diag emits a pair, up steps i, else j
-    int i = plen, j = nlen, cnt = 0, rb = -1, cw = -1;
-    uint32_t word = 0;
+    // traceback from (plen, nlen): diag emits a pair, up steps i, else j.
+    // The walk only moves up and left; a tile is 32 rows x 64 columns, lane
+    // l holding row rb-l's 4 trace words w0..w0+3 (one load each, issued
+    // together), so a path crosses few tiles.
+    int i = plen, j = nlen, cnt = 0, rb = -1, w0 = 0x7fffffff;
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
     while (i > 0 && j > 0) {
         const int w = (j - 1) >> 4;
-        if (w != cw || i > rb || i <= rb - 32) {
+        if (w < w0 || i > rb || i <= rb - 32) {
             rb = i;
-            cw = w;
+            w0 = w >= 3 ? w - 3 : 0;
             const int r = rb - lane;
-            word = r >= 1 ? trace[(size_t)(r - 1) * wpr + w] : 0u;
+            const uint32_t *row = trace + (size_t)(r - 1) * wpr + w0;
+            const bool ok = r >= 1;
+            t0 = ok ? row[0] : 0u;
+            t1 = ok && w0 + 1 < wpr ? row[1] : 0u;
+            t2 = ok && w0 + 2 < wpr ? row[2] : 0u;
+            t3 = ok && w0 + 3 < wpr ? row[3] : 0u;
         }
-        const uint32_t rw = __shfl_sync(kFull, word, rb - i);
+        const int wk = w - w0;
+        const uint32_t mine = wk == 0 ? t0 : wk == 1 ? t1 : wk == 2 ? t2 : t3;
+        const uint32_t rw = __shfl_sync(kFull, mine, rb - i);
         const uint32_t dir = (rw >> (2 * ((j - 1) & 15))) & 3u;
         if (dir == 0) {
             if (lane == 0) al[cnt] = ((uint32_t)(i - 1) << 16) | (uint32_t)(j - 1);

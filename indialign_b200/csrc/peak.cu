@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/indialign_b200.h"
+#include "dmath.cuh"
 
 namespace ia {
 
@@ -52,4 +53,24 @@ extern "C" int indialign_fp64_peak(int device, double *tflops) {
     if (e != cudaSuccess) return INDIALIGN_E_CUDA;
     *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3) / 1e12;
     return INDIALIGN_OK;
+}
+
+namespace ia {
+__global__ void k_rcp_check(const double *x, double *y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = rcp_nr(x[i]);
+}
+}  // namespace ia
+
+// Diagnostic: the search's Newton-Raphson reciprocal on the device for n
+// host values (tests compare it with the correctly rounded 1/x).
+extern "C" int indialign_selftest_rcp(int n, const double *x, double *y) {
+    if (n <= 0 || !x || !y) return INDIALIGN_E_INPUT;
+    double *d = nullptr;
+    if (cudaMalloc(&d, 2 * sizeof(double) * (size_t)n) != cudaSuccess) return INDIALIGN_E_CUDA;
+    cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    ia::k_rcp_check<<<(n + 255) / 256, 256>>>(d, d + n, n);
+    cudaError_t e = cudaMemcpy(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? INDIALIGN_OK : INDIALIGN_E_CUDA;
 }

@@ -135,3 +135,20 @@ def test_injected_failure_leaves_context_usable():
         ia.search(W.single(0))
     s, _, _ = ia.search(W.single(0))
     assert s[0] > 0.3
+
+
+def test_newton_reciprocal_within_one_ulp():
+    """rcp_nr (float seed + 2 Newton steps) against the correctly rounded 1/x
+    over the ranges the search feeds it (1 + d2/d0^2 and Jacobi pivots)."""
+    rng = np.random.default_rng(0)
+    x = np.concatenate([1.0 + rng.exponential(50.0, 20000), 10 ** rng.uniform(-14, 25, 20000),
+                        -(10 ** rng.uniform(-14, 25, 5000))])
+    y = np.zeros_like(x)
+    lib = ia.load()
+    lib.indialign_selftest_rcp.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double)]
+    assert lib.indialign_selftest_rcp(len(x), x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      y.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 0
+    exact = 1.0 / x
+    ulp = np.abs(y - exact) / np.spacing(np.abs(exact))
+    assert ulp.max() <= 1.0, ulp.max()
