@@ -206,7 +206,7 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
     kern = np.zeros(4)
-    ctr = np.zeros(8, np.int64)
+    ctr = np.zeros(12, np.int64)
     opts = ia.BatchOptions()
     opts.device = local
     opts.stream = ctypes.c_void_p(stream.cuda_stream)
@@ -230,7 +230,7 @@ def main():
         flush.zero_()
         step()
     torch.cuda.synchronize()
-    times, kms, cells, visits, launches = [], [], [], [], []
+    times, kms, cells, visits, launches, cyc = [], [], [], [], [], []
     with Clocks(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -247,6 +247,7 @@ def main():
             cells.append(ctr[0])
             visits.append(ctr[1])
             launches.append(int(ctr[7]) + 2)  # + repack and export
+            cyc.append(ctr[8:12].copy())
     clocks = clk.summary()
     ms = float(np.mean(times))
     t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -299,7 +300,9 @@ def main():
                     "peak_source": "measured FP64 FMA rate (indialign_fp64_peak) in this run",
                     "kernel_ms_per_step": k_ms, "kernel_share": k_ms / ms,
                     "nw_cells_per_step": int(np.mean(cells)),
-                    "refine_visits_per_step": int(np.mean(visits))}
+                    "refine_visits_per_step": int(np.mean(visits)),
+                    "warp_cycle_split": dict(zip(["nw_fill", "traceback", "detailed", "kabsch"],
+                                                 [float(x) for x in np.mean(cyc, 0) / max(1.0, np.mean(cyc, 0).sum())]))}
         cpu = None
         if not args.no_cpu_baseline:
             r = cpu_baseline(pairs, args.cpu_sample)

@@ -101,7 +101,9 @@ typedef struct {
     long long *counters;     /* optional [INDIALIGN_COUNTERS] work counters: NW cells,
                                 chain residue visits, bank residue visits, bank
                                 items, chains, NW-chain kernel launches, bank
-                                kernel launches, all kernel launches */
+                                kernel launches, all kernel launches, then SM
+                                cycles summed over warps in NW fill, traceback,
+                                detailed refinement, alignment Kabsch */
     double *kernel_ms;       /* optional [4]: summed device ms of the NW-chain
                                 kernel and of the bank kernel, their launch counts */
     double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
@@ -114,7 +116,7 @@ typedef struct {
 #define INDIALIGN_TRACE_STAGES 10
 
 #define INDIALIGN_STAGES 12
-#define INDIALIGN_COUNTERS 8
+#define INDIALIGN_COUNTERS 12
 
 /* Batched search with per-call options.  Same inputs and outputs as
  * indialign_tmscore_search_batch. */

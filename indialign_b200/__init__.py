@@ -22,7 +22,7 @@ from .abi import NativeConfig, NativePairInput, NativePairResult
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("INDIALIGN_B200_LIB", os.path.join(HERE, "libindialign.so"))
 STAGES = 12
-COUNTERS = 8
+COUNTERS = 12
 TRACE_STAGES = 10
 
 _lib = None

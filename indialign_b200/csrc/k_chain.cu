@@ -62,31 +62,32 @@ struct NWParams {
 };
 
 // One score-matrix entry (indialign_c/align.h:86-98; ss.h:69-72, 118-131).
+// 1/(1 + d2/d0^2) uses the Newton reciprocal (<= 1 ulp); arguments past the
+// float range (d > ~1e19 d0) contribute nothing representable to H.
+template <int SMODE>
 IA_DEV double smat_entry(const NWParams &pr, double mx, double my, double mz, uint8_t lp,
-                         const double *q, int jn) {
-    if (pr.smode == SMAT_SS2) return (lp == pr.Ln[jn]) ? 1.0 : 0.0;
-    const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+                         double qx, double qy, double qz, uint8_t ln) {
+    if (SMODE == SMAT_SS2) return (lp == ln) ? 1.0 : 0.0;
+    const double dx = mx - qx, dy = my - qy, dz = mz - qz;
     const double d2 = dx * dx + dy * dy + dz * dz;
-    // 1/(1 + d2/d0^2) with the Newton reciprocal (<= 1 ulp); arguments past
-    // the float range (d > ~1e19 d0) contribute nothing representable to H.
-    if (pr.smode == SMAT_DP) return d2 <= pr.cut2 ? rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30)) : 0.0;
-    double sc = rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30));
-    if (lp == pr.Ln[jn]) sc += 0.5;
-    return sc;
+    const double r = rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30));
+    if (SMODE == SMAT_DP) return d2 <= pr.cut2 ? r : 0.0;
+    return (lp == ln) ? r + 0.5 : r;
 }
 
 // One NW cell from its diagonal source (value), up and left (encoded), with
-// the reference's gap rule and tie order (indialign_c/nw.h:20-35).
+// the reference's gap rule and tie order (indialign_c/nw.h:20-35), written
+// with selects so that a step is a single basic block.
 IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc, double gap,
                       uint32_t &dir) {
     const double diag = diag_src + sc;
     const double up = fabs(up_enc) + (signbit(up_enc) ? gap : 0.0);
     const double left = fabs(left_enc) + (signbit(left_enc) ? gap : 0.0);
-    double nh;
-    if (diag >= up && diag >= left) { nh = diag; dir = 0; }
-    else if (left >= up) { nh = left; dir = 2; }
-    else { nh = up; dir = 1; }
-    return dir == 0 ? -nh : nh;
+    const bool is_diag = diag >= up && diag >= left;
+    const bool l_ge_u = left >= up;
+    dir = is_diag ? 0u : (l_ge_u ? 2u : 1u);
+    const double nh = is_diag ? diag : (l_ge_u ? left : up);
+    return is_diag ? -nh : nh;
 }
 
 // Fill the trace of the NW DP for (R,t) and return the aligned pair count;
@@ -99,12 +100,16 @@ IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc
 // next stripe as soon as it finishes the current one (the top row of stripe
 // k+1 reads the boundary row that lane 31 wrote for stripe k at least one
 // step earlier, since P >= 64).  Per step a lane computes two independent
-// cells with one shuffle and one shared-memory column load.
-IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
-                    double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
+// cells with one shuffle and one shared-memory column load; out-of-range
+// cells are computed on clamped indices and discarded, so the two cells'
+// score and DP chains interleave in one basic block.
+template <int SMODE>
+IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
+                      double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
     if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
+    const long long clk0 = clock64();
     const int wpr = (nlen + 15) >> 4;
     const int P = max(nlen + 1, 64);
     const int S = (plen + 63) >> 6;  // stripes
@@ -114,78 +119,76 @@ IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const dou
     int k = 0, j0 = 1 - 2 * lane;  // stripe and row-0 column of this lane
     int i0 = 2 * lane + 1;         // 1-based row of row 0
     double m0x = 0, m0y = 0, m0z = 0, m1x = 0, m1y = 0, m1z = 0;
-    uint8_t l0 = 0, l1 = 0;
+    uint8_t l0 = 0, l1 = 0, ln1 = 0;
     double h0 = 0.0, h1 = 0.0, h0prev = 0.0, up0prev = 0.0;
     double q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
     uint32_t acc0 = 0, acc1 = 0;
-    // the last stripe ends when the lane holding row plen finishes column nlen
+    bool r0ok = false, r1ok = false;
     const int last_lane = ((plen - 1) & 63) >> 1;
     const int total_steps = (S - 1) * P + 2 * last_lane + 1 + nlen + 1;
     for (int step = 0; step < total_steps; step++) {
-        // up value for row 0: lane l-1's row 1 (same column), or the boundary
         double up0 = __shfl_up_sync(kFull, h1, 1);
-        if (j0 > P) {  // next stripe
+        if (j0 > P) {  // next stripe (rare)
             j0 -= P;
             k++;
             i0 += 64;
         }
-        const bool in_stripe = k < S;
-        if (j0 == 1 && in_stripe) {  // entering the stripe: load the two rows
+        if (j0 == 1) {  // entering a stripe (rare): load its two rows
             h0 = h1 = h0prev = up0prev = 0.0;
             acc0 = acc1 = 0;
-            if (i0 <= plen) {
-                const double *p = x.P + 3 * (i0 - 1);
-                if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], m0x, m0y, m0z);
-                if (pr.smode != SMAT_DP) l0 = pr.Lp[i0 - 1];
+            r0ok = k < S && i0 <= plen;
+            r1ok = k < S && i0 + 1 <= plen;
+            const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
+            const double *p0 = x.P + 3 * a0, *p1 = x.P + 3 * a1;
+            if (SMODE != SMAT_SS2) {
+                xform(R, t, p0[0], p0[1], p0[2], m0x, m0y, m0z);
+                xform(R, t, p1[0], p1[1], p1[2], m1x, m1y, m1z);
             }
-            if (i0 + 1 <= plen) {
-                const double *p = x.P + 3 * i0;
-                if (pr.smode != SMAT_SS2) xform(R, t, p[0], p[1], p[2], m1x, m1y, m1z);
-                if (pr.smode != SMAT_DP) l1 = pr.Lp[i0];
+            if (SMODE != SMAT_DP) {
+                l0 = pr.Lp[a0];
+                l1 = pr.Lp[a1];
             }
         }
-        const bool c0 = in_stripe && j0 >= 1 && j0 <= nlen;      // row 0 column valid
-        const bool c1 = in_stripe && j0 >= 2 && j0 <= nlen + 1;  // row 1 column j0-1 valid
-        if (lane == 0) up0 = (c0 && k > 0) ? bH[j0] : 0.0;
-        double q0x = 0, q0y = 0, q0z = 0;
-        if (c0 && pr.smode != SMAT_SS2) {
-            const double *q = x.Q + 3 * (j0 - 1);
-            q0x = q[0]; q0y = q[1]; q0z = q[2];
-        }
-        double n0 = h0, n1 = h1;
-        if (c1 && i0 + 1 <= plen) {  // row 1, column j0-1
-            const int jn = j0 - 2;
-            const double q[3] = {q1x, q1y, q1z};
-            const double sc = smat_entry(pr, m1x, m1y, m1z, l1, q, jn);
-            uint32_t dir;
-            n1 = nw_cell(h0prev, sc, h0, h1, gap, dir);
-            acc1 |= dir << (2 * (jn & 15));
-            if ((jn & 15) == 15 || jn == nlen - 1) {
-                trace[(size_t)i0 * wpr + (jn >> 4)] = acc1;
+        const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;      // row 0, column j0
+        const bool v1 = r1ok && j0 >= 2 && j0 <= nlen + 1;  // row 1, column j0-1
+        const int jc = min(max(j0, 1), nlen) - 1;            // clamped 0-based column
+        const double *q = x.Q + 3 * jc;
+        const double q0x = q[0], q0y = q[1], q0z = q[2];
+        const uint8_t ln0 = SMODE != SMAT_DP ? pr.Ln[jc] : (uint8_t)0;
+        double bh = 0.0;
+        if (lane == 0 && k > 0 && v0) bh = bH[j0];
+        if (lane == 0) up0 = bh;
+        uint32_t d0, d1;
+        const double sc1 = smat_entry<SMODE>(pr, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
+        const double sc0 = smat_entry<SMODE>(pr, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
+        const double n1 = nw_cell(h0prev, sc1, h0, h1, gap, d1);
+        const double n0 = nw_cell(up0prev, sc0, up0, h0, gap, d0);
+        const int jn1 = j0 - 2, jn0 = j0 - 1;
+        if (v1) {
+            acc1 |= d1 << (2 * (jn1 & 15));
+            if ((jn1 & 15) == 15 || jn1 == nlen - 1) {
+                trace[(size_t)i0 * wpr + (jn1 >> 4)] = acc1;
                 acc1 = 0;
             }
-            if (lane == 31 && k + 1 < S) bH[jn + 1] = n1;
+            if (lane == 31 && k + 1 < S) bH[jn1 + 1] = n1;
         }
-        if (c0 && i0 <= plen) {  // row 0, column j0
-            const int jn = j0 - 1;
-            const double q[3] = {q0x, q0y, q0z};
-            const double sc = smat_entry(pr, m0x, m0y, m0z, l0, q, jn);
-            uint32_t dir;
-            n0 = nw_cell(up0prev, sc, up0, h0, gap, dir);
-            acc0 |= dir << (2 * (jn & 15));
-            if ((jn & 15) == 15 || jn == nlen - 1) {
-                trace[(size_t)(i0 - 1) * wpr + (jn >> 4)] = acc0;
+        if (v0) {
+            acc0 |= d0 << (2 * (jn0 & 15));
+            if ((jn0 & 15) == 15 || jn0 == nlen - 1) {
+                trace[(size_t)(i0 - 1) * wpr + (jn0 >> 4)] = acc0;
                 acc0 = 0;
             }
         }
         h0prev = fabs(h0);
         up0prev = fabs(up0);
-        h0 = n0;
-        h1 = n1;
+        h1 = v1 ? n1 : h1;
+        h0 = v0 ? n0 : h0;
         q1x = q0x; q1y = q0y; q1z = q0z;
+        ln1 = ln0;
         j0++;
     }
     __syncwarp();
+    const long long clk1 = clock64();
     // traceback from (plen, nlen): diag emits a pair, up steps i, else j.
     // The walk only moves up and left; a tile is 32 rows x 64 columns, lane
     // l holding row rb-l's 4 trace words w0..w0+3 (one load each, issued
@@ -221,7 +224,19 @@ IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const dou
         }
     }
     __syncwarp();
+    if (lane == 0) {
+        const long long clk2 = clock64();
+        atomicAdd(ctr + CTR_CYC_NW, (unsigned long long)(clk1 - clk0));
+        atomicAdd(ctr + CTR_CYC_TRACE, (unsigned long long)(clk2 - clk1));
+    }
     return cnt;
+}
+
+IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
+                    double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
+    if (pr.smode == SMAT_DP) return nw_align_t<SMAT_DP>(x, pr, R, t, bH, trace, al, ctr);
+    if (pr.smode == SMAT_SS4) return nw_align_t<SMAT_SS4>(x, pr, R, t, bH, trace, al, ctr);
+    return nw_align_t<SMAT_SS2>(x, pr, R, t, bH, trace, al, ctr);
 }
 
 // Kabsch on the aligned pairs + their compact TM (no d8)
@@ -451,7 +466,9 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 // EMIT: one alignment; aligned coordinates, count and (for
                 // SMAT_DP) the Kabsch on it with its compact score.
                 int na = 0;
-                if (live) na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
+                // ss_nw_align / dp_refine_chunk need >= 3 valid on each side
+                // (indialign_c/ss.h:58, align.h:141)
+                if (live && plen >= 3 && nlen >= 3) na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
                 if (lane == 0) T.na_out[si] = na;
                 double *aP = T.alP + (size_t)si * T.al_cap * 3;
                 double *aQ = T.alQ + (size_t)si * T.al_cap * 3;
@@ -475,12 +492,21 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 // d0_search_lite): best starts at score 0 / identity.
                 double bs = 0.0, bR[9], bt[3];
                 set_identity(bR, bt);
-                for (int it = 0; live && it < T.max_iter; it++) {
+                // dp_refine_chunk returns 0 / identity unless both sides have
+                // >= 3 valid residues (indialign_c/align.h:141)
+                const bool sized = plen >= 3 && nlen >= 3;
+                for (int it = 0; live && sized && it < T.max_iter; it++) {
                     const int na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
                     if (na < 3) break;  // same transform -> same alignment next time
                     double nR[9], nt[3], dR[9], dt[3];
+                    const long long ck0 = clock64();
                     double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt, b.ctr);
+                    const long long ck1 = clock64();
                     double ds = lite_detailed(x, al, na, nR, nt, I.dcut, I.d0, T.sd8, I.lnorm, dR, dt, b.ctr);
+                    if (lane == 0) {
+                        atomicAdd(b.ctr + CTR_CYC_KABSCH, (unsigned long long)(ck1 - ck0));
+                        atomicAdd(b.ctr + CTR_CYC_DETAIL, (unsigned long long)(clock64() - ck1));
+                    }
                     if (ds > s) {
                         s = ds;
 #pragma unroll

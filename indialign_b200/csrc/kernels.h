@@ -46,6 +46,10 @@ enum Counter {
     CTR_CHAIN_LAUNCHES,   // k_chain launches (host-counted)
     CTR_BANK_LAUNCHES,    // k_bank launches (host-counted)
     CTR_LAUNCHES,         // all kernel launches (host-counted)
+    CTR_CYC_NW,           // SM cycles (summed over warps) in NW fill
+    CTR_CYC_TRACE,        // ... in traceback
+    CTR_CYC_DETAIL,       // ... in the lite detailed search
+    CTR_CYC_KABSCH,       // ... in window / alignment Kabsch + compact score
     kCounters
 };
 
