@@ -75,19 +75,42 @@ IA_DEV double smat_entry(const NWParams &pr, double mx, double my, double mz, ui
     return (lp == ln) ? r + 0.5 : r;
 }
 
-// One NW cell from its diagonal source (value), up and left (encoded), with
-// the reference's gap rule and tie order (indialign_c/nw.h:20-35), written
-// with selects so that a step is a single basic block.
+// One NW cell (indialign_c/nw.h:20-35).  With a gap penalty the "reached
+// diagonally" bit of a cell travels in the sign of its H (H >= 0; -0.0 is a
+// diagonal zero) and a gap move out of a diagonal cell pays the penalty;
+// without one the bit is irrelevant and H is kept plain.  Ties prefer diag,
+// then left, then up.  Selects only, so a step is one basic block.
+template <bool GAPZ>
 IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc, double gap,
                       uint32_t &dir) {
     const double diag = diag_src + sc;
-    const double up = fabs(up_enc) + (signbit(up_enc) ? gap : 0.0);
-    const double left = fabs(left_enc) + (signbit(left_enc) ? gap : 0.0);
+    double up, left;
+    if (GAPZ) {
+        up = up_enc;
+        left = left_enc;
+    } else {
+        up = fabs(up_enc) + (signbit(up_enc) ? gap : 0.0);
+        left = fabs(left_enc) + (signbit(left_enc) ? gap : 0.0);
+    }
     const bool is_diag = diag >= up && diag >= left;
     const bool l_ge_u = left >= up;
     dir = is_diag ? 0u : (l_ge_u ? 2u : 1u);
     const double nh = is_diag ? diag : (l_ge_u ? left : up);
-    return is_diag ? -nh : nh;
+    return (GAPZ || !is_diag) ? nh : -nh;
+}
+
+// Plain value of an encoded H.
+template <bool GAPZ>
+IA_DEV double hval(double h) { return GAPZ ? h : fabs(h); }
+
+// Trace layout: cell (i, j) of stripe k = (i-1)/64, lane l = ((i-1)%64)/2,
+// row r = (i-1)%2 is computed at step t = base(i) + j - 1 with
+// base(i) = k*P + 2l + r.  Its 2 direction bits sit at bit 2*(t%16) of word
+// t/16 - base(i)/16 of row i's block of `wpr` words, so every lane fills and
+// stores its words on the same steps.
+IA_DEV int trace_base(int i, int P) {
+    const int rem = (i - 1) & 63;
+    return ((i - 1) >> 6) * P + (rem & ~1) + (rem & 1);
 }
 
 // Fill the trace of the NW DP for (R,t) and return the aligned pair count;
@@ -100,17 +123,18 @@ IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc
 // next stripe as soon as it finishes the current one (the top row of stripe
 // k+1 reads the boundary row that lane 31 wrote for stripe k at least one
 // step earlier, since P >= 64).  Per step a lane computes two independent
-// cells with one shuffle and one shared-memory column load; out-of-range
-// cells are computed on clamped indices and discarded, so the two cells'
-// score and DP chains interleave in one basic block.
-template <int SMODE>
+// cells with one shuffle and one shared-memory column load.  Cells outside
+// the matrix are computed on clamped indices and never read by a valid one
+// (a row's state is reset when it enters a stripe, and its neighbours only
+// read its in-range cells), so the step has no per-cell branches.
+template <int SMODE, bool GAPZ>
 IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
                       double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
     if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
     const long long clk0 = clock64();
-    const int wpr = (nlen + 15) >> 4;
+    const int wpr = (nlen + 15) / 16 + 1;
     const int P = max(nlen + 1, 64);
     const int S = (plen + 63) >> 6;  // stripes
     const double gap = pr.gap;
@@ -124,21 +148,32 @@ IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const d
     double q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
     uint32_t acc0 = 0, acc1 = 0;
     bool r0ok = false, r1ok = false;
+    uint32_t *row0 = trace, *row1 = trace;  // this lane's two trace rows
+    int wb0 = 0, wb1 = 0;                   // their first word index (base/16)
     const int last_lane = ((plen - 1) & 63) >> 1;
     const int total_steps = (S - 1) * P + 2 * last_lane + 1 + nlen + 1;
     for (int step = 0; step < total_steps; step++) {
         double up0 = __shfl_up_sync(kFull, h1, 1);
-        if (j0 > P) {  // next stripe (rare)
+        if (j0 > P) {  // next stripe (rare): flush the finished rows' last words
+            const int w = (step - 1) >> 4;
+            if (((step - 1) & 15) != 15) {  // else stored (and cleared) last step
+                if (r0ok && w - wb0 < wpr) row0[w - wb0] = acc0;
+                if (r1ok && w - wb1 < wpr) row1[w - wb1] = acc1;
+            }
             j0 -= P;
             k++;
             i0 += 64;
         }
-        if (j0 == 1) {  // entering a stripe (rare): load its two rows
+        if (j0 == 1) {  // entering a stripe (rare): set up its two rows
             h0 = h1 = h0prev = up0prev = 0.0;
             acc0 = acc1 = 0;
             r0ok = k < S && i0 <= plen;
             r1ok = k < S && i0 + 1 <= plen;
             const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
+            row0 = trace + (size_t)a0 * wpr;
+            row1 = trace + (size_t)a1 * wpr;
+            wb0 = step >> 4;
+            wb1 = (step + 1) >> 4;
             const double *p0 = x.P + 3 * a0, *p1 = x.P + 3 * a1;
             if (SMODE != SMAT_SS2) {
                 xform(R, t, p0[0], p0[1], p0[2], m0x, m0y, m0z);
@@ -149,69 +184,70 @@ IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const d
                 l1 = pr.Lp[a1];
             }
         }
-        const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;      // row 0, column j0
-        const bool v1 = r1ok && j0 >= 2 && j0 <= nlen + 1;  // row 1, column j0-1
-        const int jc = min(max(j0, 1), nlen) - 1;            // clamped 0-based column
+        const int jc = min(max(j0, 1), nlen) - 1;  // clamped 0-based column
         const double *q = x.Q + 3 * jc;
         const double q0x = q[0], q0y = q[1], q0z = q[2];
         const uint8_t ln0 = SMODE != SMAT_DP ? pr.Ln[jc] : (uint8_t)0;
-        double bh = 0.0;
-        if (lane == 0 && k > 0 && v0) bh = bH[j0];
-        if (lane == 0) up0 = bh;
+        const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;
+        if (lane == 0) up0 = (k > 0 && v0) ? bH[j0] : 0.0;
         uint32_t d0, d1;
         const double sc1 = smat_entry<SMODE>(pr, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
         const double sc0 = smat_entry<SMODE>(pr, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
-        const double n1 = nw_cell(h0prev, sc1, h0, h1, gap, d1);
-        const double n0 = nw_cell(up0prev, sc0, up0, h0, gap, d0);
-        const int jn1 = j0 - 2, jn0 = j0 - 1;
-        if (v1) {
-            acc1 |= d1 << (2 * (jn1 & 15));
-            if ((jn1 & 15) == 15 || jn1 == nlen - 1) {
-                trace[(size_t)i0 * wpr + (jn1 >> 4)] = acc1;
-                acc1 = 0;
-            }
-            if (lane == 31 && k + 1 < S) bH[jn1 + 1] = n1;
+        const double n1 = nw_cell<GAPZ>(h0prev, sc1, h0, h1, gap, d1);
+        const double n0 = nw_cell<GAPZ>(up0prev, sc0, up0, h0, gap, d0);
+        const int sh = 2 * (step & 15);
+        acc0 |= d0 << sh;
+        acc1 |= d1 << sh;
+        if (lane == 31 && k + 1 < S && r1ok && j0 >= 2 && j0 <= nlen + 1) bH[j0 - 1] = n1;
+        if ((step & 15) == 15) {  // uniform: every lane stores its two words
+            const int w = step >> 4;
+            if (r0ok && w - wb0 < wpr) row0[w - wb0] = acc0;
+            if (r1ok && w - wb1 < wpr) row1[w - wb1] = acc1;
+            acc0 = acc1 = 0;
         }
-        if (v0) {
-            acc0 |= d0 << (2 * (jn0 & 15));
-            if ((jn0 & 15) == 15 || jn0 == nlen - 1) {
-                trace[(size_t)(i0 - 1) * wpr + (jn0 >> 4)] = acc0;
-                acc0 = 0;
-            }
-        }
-        h0prev = fabs(h0);
-        up0prev = fabs(up0);
-        h1 = v1 ? n1 : h1;
-        h0 = v0 ? n0 : h0;
+        h0prev = hval<GAPZ>(h0);
+        up0prev = hval<GAPZ>(up0);
+        h1 = n1;
+        h0 = n0;
         q1x = q0x; q1y = q0y; q1z = q0z;
         ln1 = ln0;
         j0++;
     }
+    if (((total_steps - 1) & 15) != 15) {  // flush the last rows' pending words
+        const int w = (total_steps - 1) >> 4;
+        if (r0ok && w - wb0 < wpr && w >= wb0) row0[w - wb0] = acc0;
+        if (r1ok && w - wb1 < wpr && w >= wb1) row1[w - wb1] = acc1;
+    }
     __syncwarp();
     const long long clk1 = clock64();
     // traceback from (plen, nlen): diag emits a pair, up steps i, else j.
-    // The walk only moves up and left; a tile is 32 rows x 64 columns, lane
-    // l holding row rb-l's 4 trace words w0..w0+3 (one load each, issued
-    // together), so a path crosses few tiles.
-    int i = plen, j = nlen, cnt = 0, rb = -1, w0 = 0x7fffffff;
+    // The walk only moves up and left.  A tile is 32 rows; lane l holds the
+    // 4 trace words of row rb-l that end at the word of column jl (the
+    // column when the tile was loaded), so a path crosses few tiles.
+    int i = plen, j = nlen, cnt = 0, rb = -1, jl = 0;
     uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
     while (i > 0 && j > 0) {
-        const int w = (j - 1) >> 4;
-        if (w < w0 || i > rb || i <= rb - 32) {
+        const int bi = trace_base(i, P);
+        const int wi = ((bi + j - 1) >> 4) - (bi >> 4);  // word of (i, j) in row i
+        const int wl = ((bi + jl - 1) >> 4) - (bi >> 4);  // last word held for row i
+        if (i > rb || i <= rb - 32 || wi < wl - 3) {
             rb = i;
-            w0 = w >= 3 ? w - 3 : 0;
+            jl = j;
             const int r = rb - lane;
-            const uint32_t *row = trace + (size_t)(r - 1) * wpr + w0;
-            const bool ok = r >= 1;
-            t0 = ok ? row[0] : 0u;
-            t1 = ok && w0 + 1 < wpr ? row[1] : 0u;
-            t2 = ok && w0 + 2 < wpr ? row[2] : 0u;
-            t3 = ok && w0 + 3 < wpr ? row[3] : 0u;
+            if (r >= 1) {
+                const int br = trace_base(r, P);
+                const int wr = ((br + j - 1) >> 4) - (br >> 4);
+                const uint32_t *rowp = trace + (size_t)(r - 1) * wpr;
+                t3 = rowp[wr];
+                t2 = wr >= 1 ? rowp[wr - 1] : 0u;
+                t1 = wr >= 2 ? rowp[wr - 2] : 0u;
+                t0 = wr >= 3 ? rowp[wr - 3] : 0u;
+            }
         }
-        const int wk = w - w0;
-        const uint32_t mine = wk == 0 ? t0 : wk == 1 ? t1 : wk == 2 ? t2 : t3;
+        const int wk = wi - (((bi + jl - 1) >> 4) - (bi >> 4)) + 3;  // 0..3 within the tile
+        const uint32_t mine = wk == 3 ? t3 : wk == 2 ? t2 : wk == 1 ? t1 : t0;
         const uint32_t rw = __shfl_sync(kFull, mine, rb - i);
-        const uint32_t dir = (rw >> (2 * ((j - 1) & 15))) & 3u;
+        const uint32_t dir = (rw >> (2 * ((bi + j - 1) & 15))) & 3u;
         if (dir == 0) {
             if (lane == 0) al[cnt] = ((uint32_t)(i - 1) << 16) | (uint32_t)(j - 1);
             cnt++;
@@ -234,9 +270,12 @@ IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const d
 
 IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
                     double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
-    if (pr.smode == SMAT_DP) return nw_align_t<SMAT_DP>(x, pr, R, t, bH, trace, al, ctr);
-    if (pr.smode == SMAT_SS4) return nw_align_t<SMAT_SS4>(x, pr, R, t, bH, trace, al, ctr);
-    return nw_align_t<SMAT_SS2>(x, pr, R, t, bH, trace, al, ctr);
+    if (pr.smode == SMAT_DP) {
+        if (pr.gap == 0.0) return nw_align_t<SMAT_DP, true>(x, pr, R, t, bH, trace, al, ctr);
+        return nw_align_t<SMAT_DP, false>(x, pr, R, t, bH, trace, al, ctr);
+    }
+    if (pr.smode == SMAT_SS4) return nw_align_t<SMAT_SS4, false>(x, pr, R, t, bH, trace, al, ctr);
+    return nw_align_t<SMAT_SS2, false>(x, pr, R, t, bH, trace, al, ctr);
 }
 
 // Kabsch on the aligned pairs + their compact TM (no d8)

@@ -365,7 +365,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel_ptr(), 32 * kChainWarps,
                                                      smem));
     if (per_sm < 1) per_sm = 1;
-    trace_words_ = (size_t)pmax * ((nmax + 15) / 16);
+    trace_words_ = (size_t)pmax * ((nmax + 15) / 16 + 1);  // NW trace rows (k_chain.cu)
     long long warps = (long long)c_->sms * per_sm * kChainWarps;
     const size_t budget = (size_t)4 << 30;  // trace scratch budget
     long long cap = (long long)(budget / (trace_words_ * 4 + 1));
