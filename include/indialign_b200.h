@@ -136,6 +136,17 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
                                     const double *lnorm, const NativeConfig *cfg,
                                     const IndialignBatchOptions *opts, double *d_out);
 
+/* Needleman-Wunsch alignment of one explicit score matrix; replaces the
+ * reference's nw_dp + nw_traceback pair (indialign_c/nw.h:10-68): zero
+ * boundaries, a gap move out of a diagonally reached cell pays `gap`, ties
+ * prefer diag, then left, then up; the traceback starts at (np, nn).
+ * d_smat: np*nn doubles, row-major, device memory.  Writes the aligned
+ * (pred, native) index pairs in ascending order to d_ap/d_an (device,
+ * min(np,nn) ints each) and their count to *d_na (device int).  Synchronous
+ * on `stream` (NULL: the library's stream).  1 <= np, nn <= 65535. */
+int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_ap, int *d_an,
+                       int *d_na, void *stream);
+
 /* Measured FP64 FMA throughput of the device in TFLOP/s (the roofline
  * denominator for the search kernels, which are FP64 SIMT work). */
 int indialign_fp64_peak(int device, double *tflops);

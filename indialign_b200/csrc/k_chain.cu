@@ -59,6 +59,7 @@ struct NWParams {
     double inv_d0sq;  // 1/d0^2 of the score matrix
     double cut2;      // SMAT_DP: score only if d2 <= cut2
     const uint8_t *Lp, *Ln;  // SS labels (compact order)
+    const double *smat;      // SMAT_EXPLICIT: plen x nlen row-major
 };
 
 // One score-matrix entry (indialign_c/align.h:86-98; ss.h:69-72, 118-131).
@@ -175,24 +176,35 @@ IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const d
             wb0 = step >> 4;
             wb1 = (step + 1) >> 4;
             const double *p0 = x.P + 3 * a0, *p1 = x.P + 3 * a1;
-            if (SMODE != SMAT_SS2) {
+            if (SMODE != SMAT_SS2 && SMODE != SMAT_EXPLICIT) {
                 xform(R, t, p0[0], p0[1], p0[2], m0x, m0y, m0z);
                 xform(R, t, p1[0], p1[1], p1[2], m1x, m1y, m1z);
             }
-            if (SMODE != SMAT_DP) {
+            if (SMODE == SMAT_SS2 || SMODE == SMAT_SS4) {
                 l0 = pr.Lp[a0];
                 l1 = pr.Lp[a1];
             }
         }
         const int jc = min(max(j0, 1), nlen) - 1;  // clamped 0-based column
-        const double *q = x.Q + 3 * jc;
-        const double q0x = q[0], q0y = q[1], q0z = q[2];
-        const uint8_t ln0 = SMODE != SMAT_DP ? pr.Ln[jc] : (uint8_t)0;
+        double q0x = 0, q0y = 0, q0z = 0;
+        if (SMODE != SMAT_EXPLICIT) {
+            const double *q = x.Q + 3 * jc;
+            q0x = q[0]; q0y = q[1]; q0z = q[2];
+        }
+        const uint8_t ln0 = (SMODE == SMAT_SS2 || SMODE == SMAT_SS4) ? pr.Ln[jc] : (uint8_t)0;
         const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;
         if (lane == 0) up0 = (k > 0 && v0) ? bH[j0] : 0.0;
         uint32_t d0, d1;
-        const double sc1 = smat_entry<SMODE>(pr, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
-        const double sc0 = smat_entry<SMODE>(pr, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
+        double sc0, sc1;
+        if (SMODE == SMAT_EXPLICIT) {
+            const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
+            const int jc1 = min(max(j0 - 1, 1), nlen) - 1;
+            sc0 = pr.smat[(size_t)a0 * nlen + jc];
+            sc1 = pr.smat[(size_t)a1 * nlen + jc1];
+        } else {
+            sc1 = smat_entry<SMODE>(pr, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
+            sc0 = smat_entry<SMODE>(pr, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
+        }
         const double n1 = nw_cell<GAPZ>(h0prev, sc1, h0, h1, gap, d1);
         const double n0 = nw_cell<GAPZ>(up0prev, sc0, up0, h0, gap, d0);
         const int sh = 2 * (step & 15);
@@ -572,6 +584,45 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
         }
         __syncthreads();
     }
+}
+
+// ---- NW on an explicit score matrix (one warp per problem) ---------------
+// nw_dp + nw_traceback (indialign_c/nw.h:10-68) on a caller-given FP64 score
+// matrix: the same fill and traceback as the chains, so that the DP can be
+// checked bit for bit against the reference on identical inputs.
+__global__ void k_nw_explicit(const double *__restrict__ smat, int np, int nn, double gap,
+                              uint32_t *trace, double *bH, uint32_t *al, int *ap, int *an,
+                              int *na_out, unsigned long long *ctr) {
+    NWParams pr;
+    pr.plen = np;
+    pr.nlen = nn;
+    pr.smode = SMAT_EXPLICIT;
+    pr.gap = gap;
+    pr.inv_d0sq = 0.0;
+    pr.cut2 = 0.0;
+    pr.Lp = pr.Ln = nullptr;
+    pr.smat = smat;
+    Pts x = {nullptr, nullptr};
+    const double I[12] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0};
+    int na = 0;
+    if (np >= 1 && nn >= 1) {
+        if (gap == 0.0) na = nw_align_t<SMAT_EXPLICIT, true>(x, pr, I, I + 9, bH, trace, al, ctr);
+        else na = nw_align_t<SMAT_EXPLICIT, false>(x, pr, I, I + 9, bH, trace, al, ctr);
+    }
+    for (int k = threadIdx.x; k < na; k += 32) {
+        const uint32_t e = al[na - 1 - k];
+        ap[k] = (int)(e >> 16);
+        an[k] = (int)(e & 0xffffu);
+    }
+    if (threadIdx.x == 0) *na_out = na;
+}
+
+size_t nw_trace_words(int np, int nn) { return (size_t)np * ((nn + 15) / 16 + 1); }
+
+void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t *trace,
+                        double *bH, uint32_t *al, int *ap, int *an, int *na,
+                        unsigned long long *ctr, cudaStream_t st) {
+    k_nw_explicit<<<1, 32, 0, st>>>(smat, np, nn, gap, trace, bH, al, ap, an, na, ctr);
 }
 
 size_t chain_smem_bytes(int pmax, int nmax, int flags) {

@@ -89,6 +89,10 @@ void launch_chain(const DevBatch &b, const ChainTask *tasks, const int *chunk_be
                   cudaStream_t st);
 cudaError_t chain_set_attributes();
 const void *chain_kernel_ptr();
+size_t nw_trace_words(int np, int nn);
+void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t *trace,
+                        double *bH, uint32_t *al, int *ap, int *an, int *na,
+                        unsigned long long *ctr, cudaStream_t st);
 
 // k_plan.cu
 void launch_plan_bank(const DevBatch &b, const PlanCtx &c, cudaStream_t st);

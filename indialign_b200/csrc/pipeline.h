@@ -95,7 +95,7 @@ struct BankTask {
 // ---- NW chains ---------------------------------------------------------
 enum ChainStart { START_WINDOW = 0, START_RT = 1 };
 enum ChainMode { CHAIN_LITE = 0, CHAIN_EMIT = 1 };
-enum ScoreMode { SMAT_DP = 0, SMAT_SS2 = 1, SMAT_SS4 = 2 };
+enum ScoreMode { SMAT_DP = 0, SMAT_SS2 = 1, SMAT_SS4 = 2, SMAT_EXPLICIT = 3 };
 
 // One task = all chains of one pair in one stage (windows x 2 gaps, or
 // RT starts x 2 gaps, or single EMIT NW alignments).

@@ -970,6 +970,40 @@ int indialign_cuda_available(void) {
     return major == 10 ? 1 : 0;
 }
 
+int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_ap, int *d_an,
+                       int *d_na, void *stream) {
+    ia::g_last_error.clear();
+    if (!d_smat || !d_ap || !d_an || !d_na || np < 1 || nn < 1 || np > 65535 || nn > 65535) {
+        ia::g_last_error = "nw_align: null pointer or size outside 1..65535";
+        return INDIALIGN_E_INPUT;
+    }
+    ia::Ctx *c = nullptr;
+    int rc = ia::acquire(-1, &c);
+    if (rc) return rc;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    rc = INDIALIGN_OK;
+    do {
+        const size_t words = ia::nw_trace_words(np, nn);
+        if (c->gtrace.ensure(words) != cudaSuccess || c->gbh.ensure((size_t)nn + 1) != cudaSuccess ||
+            c->gal.ensure((size_t)(np < nn ? np : nn)) != cudaSuccess ||
+            c->ctr.ensure(ia::kCounters) != cudaSuccess) {
+            ia::g_last_error = "nw_align: workspace allocation failed";
+            rc = INDIALIGN_E_CUDA;
+            break;
+        }
+        ia::launch_nw_explicit(d_smat, np, nn, gap, c->gtrace.p, c->gbh.p, c->gal.p, d_ap, d_an, d_na,
+                               c->ctr.p, st);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            ia::set_error("nw_align", e);
+            rc = INDIALIGN_E_CUDA;
+        }
+    } while (0);
+    ia::release(c);
+    return rc;
+}
+
 int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d_pred,
                                     const double *d_nat, const uint8_t *d_v,
                                     const uint8_t *d_pv, const uint8_t *d_nv,

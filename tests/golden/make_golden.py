@@ -104,6 +104,47 @@ def main():
         np.savez_compressed(os.path.join(OUT, f"golden_{name}.npz"), score=s, R=R, t=t,
                             trace=trace, sigma=np.array([p.sigma for p in pairs]), **pack(pairs))
         print(name, len(pairs), np.round(s, 4))
+    # NW on explicit score matrices (nw_dp + nw_traceback), tie-heavy cases
+    st = ctypes.CDLL(STAGES)
+    st.ref_nw_align.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                ctypes.c_double, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    rng = np.random.default_rng(9)
+    nw = {}
+    # matrices are stored as uint16 grids q with score = q / 4096 (exact in
+    # FP64); the large shapes only for the tie-heavy kinds, which compress
+    shapes = [(1, 1), (1, 5), (5, 1), (3, 3), (7, 40), (64, 64), (65, 130), (130, 65),
+              (200, 151), (300, 287)]
+    kinds = ["uniform", "binary", "ss4", "cutoff"]
+    case = 0
+    for (np_, nn_) in shapes:
+        for kind in kinds:
+            if np_ * nn_ > 20000 and kind in ("uniform", "ss4"):
+                continue
+            gaps = (-0.6, 0.0, -1.0) if np_ * nn_ <= 20000 else ((-0.6,) if kind == "binary" else (0.0,))
+            for gap in gaps:
+                if kind == "uniform":
+                    q = rng.integers(0, 4096, (np_, nn_))
+                elif kind == "binary":
+                    q = 4096 * (rng.uniform(size=(np_, nn_)) < 0.4)
+                elif kind == "ss4":
+                    q = rng.integers(0, 200, (np_, nn_)) + 2048 * (rng.uniform(size=(np_, nn_)) < 0.5)
+                else:
+                    d = rng.integers(0, 4096, (np_, nn_))
+                    q = np.where(rng.uniform(size=(np_, nn_)) < 0.35, d, 0)
+                q = q.astype(np.uint16)
+                m = np.ascontiguousarray(q.astype(np.float64) / 4096.0)
+                ap = np.zeros(min(np_, nn_), np.int32)
+                an = np.zeros(min(np_, nn_), np.int32)
+                na = st.ref_nw_align(m.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), np_, nn_, gap,
+                                     ap.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                     an.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+                nw[f"q{case}"] = q
+                nw[f"g{case}"] = np.array([gap])
+                nw[f"ap{case}"] = ap[:na].copy()
+                nw[f"an{case}"] = an[:na].copy()
+                case += 1
+    np.savez_compressed(os.path.join(OUT, "golden_nw.npz"), **nw)
+    print("nw cases", case)
     # std::sort tie order of the anchor candidates (count-only comparator)
     st = ctypes.CDLL(STAGES)
     rng = np.random.default_rng(5)

@@ -74,3 +74,30 @@ def test_oracle_length_zero(oracle):
     out.score = 7.0
     assert oracle.ora_tmscore_search(ctypes.byref(inp), ctypes.byref(cfg), ctypes.byref(out)) == -1
     assert out.score == 7.0
+
+
+def _nw_cases():
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_nw.npz"))
+    k = 0
+    while f"q{k}" in z:
+        yield z[f"q{k}"].astype(np.float64) / 4096.0, float(z[f"g{k}"][0]), z[f"ap{k}"], z[f"an{k}"]
+        k += 1
+
+
+def test_oracle_nw_matches_golden(oracle):
+    oracle.ora_nw_align.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_double, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_int)]
+    n = 0
+    for m, gap, ap, an in _nw_cases():
+        m = np.ascontiguousarray(m)
+        a = np.zeros(min(m.shape), np.int32)
+        b = np.zeros(min(m.shape), np.int32)
+        na = oracle.ora_nw_align(m.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), m.shape[0], m.shape[1],
+                                 gap, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                 b.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+        np.testing.assert_array_equal(a[:na], ap)
+        np.testing.assert_array_equal(b[:na], an)
+        n += 1
+    assert n >= 90

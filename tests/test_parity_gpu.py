@@ -152,3 +152,30 @@ def test_newton_reciprocal_within_one_ulp():
     exact = 1.0 / x
     ulp = np.abs(y - exact) / np.spacing(np.abs(exact))
     assert ulp.max() <= 1.0, ulp.max()
+
+
+def test_nw_explicit_bit_exact_vs_reference():
+    """Given an identical FP64 score matrix, the device NW (fill + traceback)
+    returns exactly the reference's alignment, ties included."""
+    import os
+    torch = pytest.importorskip("torch")
+    lib = ia.load()
+    lib.indialign_nw_align.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.indialign_nw_align.restype = ctypes.c_int
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_nw.npz"))
+    k = 0
+    while f"q{k}" in z:
+        m = torch.from_numpy(np.ascontiguousarray(z[f"q{k}"].astype(np.float64) / 4096.0)).cuda()
+        npr, nn = m.shape
+        ap = torch.zeros(min(npr, nn), dtype=torch.int32, device="cuda")
+        an = torch.zeros_like(ap)
+        na = torch.zeros(1, dtype=torch.int32, device="cuda")
+        rc = lib.indialign_nw_align(m.data_ptr(), npr, nn, float(z[f"g{k}"][0]), ap.data_ptr(),
+                                    an.data_ptr(), na.data_ptr(), None)
+        assert rc == 0, ia.last_error()
+        n = int(na.item())
+        np.testing.assert_array_equal(ap[:n].cpu().numpy(), z[f"ap{k}"], err_msg=f"case {k}")
+        np.testing.assert_array_equal(an[:n].cpu().numpy(), z[f"an{k}"], err_msg=f"case {k}")
+        k += 1
+    assert k >= 90
