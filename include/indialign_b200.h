@@ -147,6 +147,20 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
 int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_ap, int *d_an,
                        int *d_na, void *stream);
 
+/* indialign_nw_align without any device allocation (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc when they align: code
+ * running under another component's CUDA graph capture, or hosts whose device
+ * memory belongs to a framework's pool.  Same arguments, kernel and outputs
+ * as indialign_nw_align; the caller passes device inputs and outputs, the
+ * scratch lives in a fixed device array of about 1.1 MB that every GPU using
+ * the library keeps until exit.  Limit: 1 <= np, nn <= 2048, else
+ * INDIALIGN_E_INPUT.  The first call on a device looks the array up with
+ * cudaGetSymbolAddress (make it before any stream capture).  All calls share
+ * the array: calls whose work overlaps on the GPU race.  stream NULL is the
+ * legacy default stream; the call returns after the stream synchronizes. */
+int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap, int *d_ap,
+                               int *d_an, int *d_na, void *stream);
+
 /* Measured FP64 FMA throughput of the device in TFLOP/s (the roofline
  * denominator for the search kernels, which are FP64 SIMT work). */
 int indialign_fp64_peak(int device, double *tflops);

@@ -53,6 +53,9 @@ enum Counter {
     kCounters
 };
 
+// search.cu: text returned by indialign_last_error on this thread
+void set_last_error_text(const char *msg);
+
 // k_misc.cu
 void launch_prep(const DevBatch &b, int use_frag, cudaStream_t st);
 void launch_anchor(const DevBatch &b, cudaStream_t st);

@@ -28,6 +28,8 @@ static void set_error(const char *what, cudaError_t e) {
     g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
 }
 
+void set_last_error_text(const char *msg) { g_last_error = msg; }
+
 #define CK(x)                                 \
     do {                                      \
         cudaError_t e_ = (x);                 \
