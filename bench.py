@@ -207,11 +207,13 @@ def main():
     stream = torch.cuda.current_stream()
     kern = np.zeros(4)
     ctr = np.zeros(12, np.int64)
+    stage_ms = np.zeros(12)
     opts = ia.BatchOptions()
     opts.device = local
     opts.stream = ctypes.c_void_p(stream.cuda_stream)
     opts.kernel_ms = kern.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     opts.counters = ctr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    opts.stage_ms = stage_ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
     def step():
         rc = lib.indialign_tmscore_search_device(
@@ -230,7 +232,7 @@ def main():
         flush.zero_()
         step()
     torch.cuda.synchronize()
-    times, kms, cells, visits, launches, cyc = [], [], [], [], [], []
+    times, kms, cells, visits, launches, cyc, stg = [], [], [], [], [], [], []
     with Clocks(local) as clk:
         for _ in range(args.steps):
             flush.zero_()
@@ -248,6 +250,7 @@ def main():
             visits.append(ctr[1])
             launches.append(int(ctr[7]) + 2)  # + repack and export
             cyc.append(ctr[8:12].copy())
+            stg.append(stage_ms.copy())
     clocks = clk.summary()
     ms = float(np.mean(times))
     t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -322,6 +325,10 @@ def main():
                            "parallelism": f"independent pairs per GPU x{world}"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(np.mean(launches)), "clocks": clocks,
+                "stage_ms": dict(zip(["seeds", "seed_bank", "ss", "gapless", "local_fragment",
+                                      "threading_dp", "dense_local_fragment", "topk", "dp_refine",
+                                      "offset_dp", "weighted", "total"],
+                                     [round(float(x), 2) for x in np.mean(stg, 0)])),
                 "mean_tm": float(scores.mean())}
         print(json.dumps(line))
     if dist:

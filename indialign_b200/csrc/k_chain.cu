@@ -27,6 +27,18 @@ namespace ia {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// build-time tuning knobs: minimum resident CTAs per SM for k_chain (caps
+// registers; 4 -> 128 registers measured best) and the NW step-loop unroll
+// factor (1 measured best: the rare stripe branches make unrolled copies
+// larger without shortening the dependency chain)
+#ifndef IA_CHAIN_MINB
+#define IA_CHAIN_MINB 4
+#endif
+#ifndef IA_NW_UNROLL
+#define IA_NW_UNROLL 1
+#endif
+constexpr int kNwUnroll = IA_NW_UNROLL;
+
 // ---- warp helpers ----------------------------------------------------------
 struct Pts {
     const double *P;  // pred compact xyz
@@ -128,9 +140,12 @@ IA_DEV int trace_base(int i, int P) {
 // the matrix are computed on clamped indices and never read by a valid one
 // (a row's state is reset when it enters a stripe, and its neighbours only
 // read its in-range cells), so the step has no per-cell branches.
+// inlined: measured faster than out-of-line calls (the call frame costs more
+// than the registers it frees)
+#define IA_NW_ATTR IA_DEV
 template <int SMODE, bool GAPZ>
-IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
-                      double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
+IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
+                          double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
     if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
@@ -153,6 +168,7 @@ IA_DEV int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const d
     int wb0 = 0, wb1 = 0;                   // their first word index (base/16)
     const int last_lane = ((plen - 1) & 63) >> 1;
     const int total_steps = (S - 1) * P + 2 * last_lane + 1 + nlen + 1;
+#pragma unroll kNwUnroll
     for (int step = 0; step < total_steps; step++) {
         double up0 = __shfl_up_sync(kFull, h1, 1);
         if (j0 > P) {  // next stripe (rare): flush the finished rows' last words
@@ -322,7 +338,7 @@ IA_DEV double aligned_kabsch(const Pts &x, const uint32_t *al, int na, double d0
 // d8-filtered score.  The all-pairs seed's Kabsch is the (R0,t0) just
 // computed by aligned_kabsch.  Lane groups of 4 run the 6 cutoffs side by
 // side; the first maximum in cutoff order wins.
-IA_DEV double lite_detailed(const Pts &x, const uint32_t *al, int na, const double *R0,
+IA_NW_ATTR double lite_detailed(const Pts &x, const uint32_t *al, int na, const double *R0,
                             const double *t0, const double *dcut, double d0, double sd8,
                             double lnorm, double *Ro, double *to, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31, g = lane >> 2, sub = lane & 3;
@@ -396,7 +412,7 @@ struct ChainCtl {
     int chunk, task, next;
 };
 
-__global__ void __launch_bounds__(32 * kChainWarps, 3)
+__global__ void __launch_bounds__(32 * kChainWarps, IA_CHAIN_MINB)
 k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         int ntasks, const ScanOut *__restrict__ scan, int *counter, uint32_t *gtrace,
         size_t trace_words, double *gbh, uint32_t *gal, int pmax, int nmax, int flags) {
