@@ -412,6 +412,10 @@ struct ChainCtl {
     int chunk, task, next;
 };
 
+// EMIT = false: LITE dp_refine chains only (the hot rescue kernel, DP score
+// mode only); EMIT = true: single NW alignments for SS seeds / full dp_refine.
+// Two instantiations keep the hot kernel's code small.
+template <bool EMIT>
 __global__ void __launch_bounds__(32 * kChainWarps, IA_CHAIN_MINB)
 k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         int ntasks, const ScanOut *__restrict__ scan, int *counter, uint32_t *gtrace,
@@ -529,7 +533,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 pr.cut2 = T.sd8 * T.sd8;
             }
             if (T.live && !T.live[si]) live = false;
-            if (T.na_out) {
+            if (EMIT) {
                 // EMIT: one alignment; aligned coordinates, count and (for
                 // SMAT_DP) the Kabsch on it with its compact score.
                 int na = 0;
@@ -563,7 +567,8 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 // >= 3 valid residues (indialign_c/align.h:141)
                 const bool sized = plen >= 3 && nlen >= 3;
                 for (int it = 0; live && sized && it < T.max_iter; it++) {
-                    const int na = nw_align(x, pr, R, t, bH, trace, al, b.ctr);
+                    const int na = pr.gap == 0.0 ? nw_align_t<SMAT_DP, true>(x, pr, R, t, bH, trace, al, b.ctr)
+                                                 : nw_align_t<SMAT_DP, false>(x, pr, R, t, bH, trace, al, b.ctr);
                     if (na < 3) break;  // same transform -> same alignment next time
                     double nR[9], nt[3], dR[9], dt[3];
                     const long long ck0 = clock64();
@@ -654,18 +659,26 @@ size_t chain_smem_bytes(int pmax, int nmax, int flags) {
 
 void launch_chain(const DevBatch &b, const ChainTask *tasks, const int *chunk_begin, int ntasks,
                   const ScanOut *scan, int *counter, uint32_t *gtrace, size_t trace_words,
-                  double *gbh, uint32_t *gal, int pmax, int nmax, int flags, int grid,
+                  double *gbh, uint32_t *gal, int pmax, int nmax, int flags, int grid, bool emit,
                   cudaStream_t st) {
     size_t sm = chain_smem_bytes(pmax, nmax, flags);
-    k_chain<<<grid, 32 * kChainWarps, sm, st>>>(b, tasks, chunk_begin, ntasks, scan, counter,
-                                                gtrace, trace_words, gbh, gal, pmax, nmax, flags);
+    if (emit)
+        k_chain<true><<<grid, 32 * kChainWarps, sm, st>>>(b, tasks, chunk_begin, ntasks, scan, counter,
+                                                          gtrace, trace_words, gbh, gal, pmax, nmax, flags);
+    else
+        k_chain<false><<<grid, 32 * kChainWarps, sm, st>>>(b, tasks, chunk_begin, ntasks, scan, counter,
+                                                           gtrace, trace_words, gbh, gal, pmax, nmax, flags);
 }
 
-const void *chain_kernel_ptr() { return (const void *)k_chain; }
+const void *chain_kernel_ptr() { return (const void *)k_chain<false>; }
 
 cudaError_t chain_set_attributes() {
-    return cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kChainSmemMax);
+    cudaError_t e = cudaFuncSetAttribute(k_chain<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kChainSmemMax);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_chain<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kChainSmemMax);
+    return e;
 }
 
 }  // namespace ia

@@ -88,7 +88,7 @@ const void *bank_kernel_ptr(bool smem);
 size_t chain_smem_bytes(int pmax, int nmax, int flags);
 void launch_chain(const DevBatch &b, const ChainTask *tasks, const int *chunk_begin, int ntasks,
                   const ScanOut *scan, int *counter, uint32_t *gtrace, size_t trace_words,
-                  double *gbh, uint32_t *gal, int pmax, int nmax, int flags, int grid,
+                  double *gbh, uint32_t *gal, int pmax, int nmax, int flags, int grid, bool emit,
                   cudaStream_t st);
 cudaError_t chain_set_attributes();
 const void *chain_kernel_ptr();

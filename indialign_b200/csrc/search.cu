@@ -449,8 +449,9 @@ int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, b
         e1 = new_event();
         cudaEventRecord(e0, c_->stream);
     }
+    const bool emit = kind == CH_SS2 || kind == CH_SS4 || kind == CH_DP_EMIT;
     launch_chain(b, c_->ctasks.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->gtrace.p,
-                 trace_words_, c_->gbh.p, c_->gal.p, pmax, nmax, chain_flags_, chain_grid_,
+                 trace_words_, c_->gbh.p, c_->gal.p, pmax, nmax, chain_flags_, chain_grid_, emit,
                  c_->stream);
     if (timing) {
         cudaEventRecord(e1, c_->stream);
