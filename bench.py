@@ -205,7 +205,7 @@ def main():
     d_out = torch.zeros(n * 13, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    kern = np.zeros(4)
+    kern = np.zeros(6)
     ctr = np.zeros(12, np.int64)
     stage_ms = np.zeros(12)
     opts = ia.BatchOptions()

@@ -104,11 +104,41 @@ typedef struct {
                                 kernel launches, all kernel launches, then SM
                                 cycles summed over warps in NW fill, traceback,
                                 detailed refinement, alignment Kabsch */
-    double *kernel_ms;       /* optional [4]: summed device ms of the NW-chain
-                                kernel and of the bank kernel, their launch counts */
+    double *kernel_ms;       /* optional [6]: summed device ms of the NW-chain
+                                kernel and of the bank kernel, their launch counts,
+                                then ms and launches of the window-ranker kernel */
     double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
                                 best {score,R,t} after each search stage */
+    /* ---- learned window ranker (dense local-fragment rescue) ---- */
+    int mode;                /* INDIALIGN_MODE_PLAIN (0), _LEARNED or _COLLECT */
+    const float *ranker;     /* LEARNED: host FP32 parameter blob of
+                                INDIALIGN_RANKER_FLOATS floats */
+    int top_k;               /* LEARNED: windows refined per pair (1..32; 0: 8) */
+    double margin;           /* LEARNED: refine all windows when the predicted
+                                top-1 minus top-k score is below this */
+    double audit_rate;       /* LEARNED: fraction of pairs refined on all windows */
+    unsigned long long seed; /* LEARNED: audit draw */
+    long long *rank_stats;   /* LEARNED: optional [INDIALIGN_RANK_STATS] out: pairs
+                                ranked, margin fallbacks, audits, pruned pairs,
+                                windows, windows refined, audit misses, pairs with
+                                at most top_k windows */
+    float *win_feat;         /* COLLECT: out [windows][16] raw window features */
+    float *win_label;        /* COLLECT: out [windows] refined window score, NaN
+                                where the pair did not reach the dense rescue */
+    long long win_cap;       /* COLLECT, or LEARNED with win_score: capacity of the
+                                per-window outputs in windows */
+    float *win_score;        /* optional out [windows] (LEARNED, or COLLECT with a
+                                ranker): predicted score of every window */
+    int *win_select;         /* optional out [n_pairs][33] (LEARNED): windows refined
+                                (-1: all, margin fallback or at most top_k windows;
+                                -2: all, audit), then the top_k windows ascending */
 } IndialignBatchOptions;
+
+#define INDIALIGN_MODE_PLAIN 0   /* the reference's search, every window refined */
+#define INDIALIGN_MODE_LEARNED 1 /* dense rescue refines the ranker's top-k windows */
+#define INDIALIGN_MODE_COLLECT 2 /* plain search + per-window features and labels */
+#define INDIALIGN_RANKER_FLOATS 18849
+#define INDIALIGN_RANK_STATS 8
 
 /* Stages recorded in stage_best, in search order: seed bank, SS seeds,
  * gapless threading, local fragment DP, threading DP, dense local fragment
@@ -160,6 +190,40 @@ int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_
  * legacy default stream; the call returns after the stream synchronizes. */
 int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap, int *d_ap,
                                int *d_an, int *d_na, void *stream);
+
+/* Dense-rescue windows of a pair with plen / nlen valid pred / native
+ * residues (rescue.h:12-46 schedule).  In COLLECT mode pair p's windows sit
+ * at the running sum of this count over the pairs before it, every pair
+ * counted, in the batch's order. */
+int indialign_window_count(int plen, int nlen, int dense);
+
+/* ---- ranker training on caller-owned device buffers (no counterpart in the
+ * reference, which has no learned component).  The parameter blob is FP32:
+ * mean[16] std[16] W1[16][128] b1[128] W2[128][128] b2[128] w3[128] b3, weights
+ * [in][out]; mean/std standardise the raw features and are not trained.  The
+ * network runs on BF16 tensor cores with FP32 accumulation.  All calls are
+ * asynchronous on `stream` (NULL: legacy default stream). */
+size_t indialign_mlp_packed_bytes(void);
+/* BF16 / layout copy of a device blob, read by the forward and backward. */
+int indialign_mlp_pack(const float *d_blob, void *d_packed, void *stream);
+size_t indialign_mlp_save_bytes(int n);
+/* y[n] = MLP(x[n][16]); with d_save (indialign_mlp_save_bytes(n) bytes) the
+ * activations the backward needs are kept. */
+int indialign_mlp_forward(const void *d_packed, const float *d_x, int n, float *d_y,
+                          void *d_save, void *stream);
+/* Loss = mean squared error + lambda * mean logistic ranking loss over the
+ * row pairs (2i, 2i+1); writes d_dy[n] = dLoss/dy and d_loss[0]. */
+int indialign_mlp_loss(const float *d_y, const float *d_t, int n, float lambda, float *d_dy,
+                       float *d_loss, void *stream);
+size_t indialign_mlp_work_bytes(int n);
+/* Gradients of sum_i dy[i] y[i] w.r.t. the blob, written to d_grad
+ * (INDIALIGN_RANKER_FLOATS floats; the mean/std entries are zeroed).  d_save
+ * from the forward on the same rows; d_work of indialign_mlp_work_bytes(n). */
+int indialign_mlp_backward(const void *d_packed, const float *d_dy, int n, const void *d_save,
+                           float *d_grad, void *d_work, void *stream);
+/* One Adam step (bias-corrected, step >= 1) on the trained blob entries. */
+int indialign_mlp_adam(float *d_blob, const float *d_grad, float *d_m, float *d_v, int step,
+                       float lr, float beta1, float beta2, float eps, void *stream);
 
 /* Measured FP64 FMA throughput of the device in TFLOP/s (the roofline
  * denominator for the search kernels, which are FP64 SIMT work). */

@@ -24,6 +24,13 @@ LIB_PATH = os.environ.get("INDIALIGN_B200_LIB", os.path.join(HERE, "libindialign
 STAGES = 12
 COUNTERS = 12
 TRACE_STAGES = 10
+KERNEL_MS = 6
+MODE_PLAIN, MODE_LEARNED, MODE_COLLECT = 0, 1, 2
+RANKER_FLOATS = 18849
+RANK_STATS = 8
+RANK_STAT_NAMES = ("gated", "fallback", "audit", "pruned", "windows", "refined",
+                   "audit_miss", "small")
+FEATURES = 16
 
 _lib = None
 
@@ -38,7 +45,19 @@ class BatchOptions(ctypes.Structure):
                 ("stage_ms", ctypes.POINTER(ctypes.c_double)),
                 ("counters", ctypes.POINTER(ctypes.c_longlong)),
                 ("kernel_ms", ctypes.POINTER(ctypes.c_double)),
-                ("stage_best", ctypes.POINTER(ctypes.c_double))]
+                ("stage_best", ctypes.POINTER(ctypes.c_double)),
+                ("mode", ctypes.c_int),
+                ("ranker", ctypes.POINTER(ctypes.c_float)),
+                ("top_k", ctypes.c_int),
+                ("margin", ctypes.c_double),
+                ("audit_rate", ctypes.c_double),
+                ("seed", ctypes.c_ulonglong),
+                ("rank_stats", ctypes.POINTER(ctypes.c_longlong)),
+                ("win_feat", ctypes.POINTER(ctypes.c_float)),
+                ("win_label", ctypes.POINTER(ctypes.c_float)),
+                ("win_cap", ctypes.c_longlong),
+                ("win_score", ctypes.POINTER(ctypes.c_float)),
+                ("win_select", ctypes.POINTER(ctypes.c_int))]
 
 
 def build():
@@ -75,6 +94,22 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.indialign_tmscore_search_device.restype = ctypes.c_int
     lib.indialign_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.indialign_fp64_peak.restype = ctypes.c_int
+    lib.indialign_window_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.indialign_window_count.restype = ctypes.c_int
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    for name, args, res in (
+            ("indialign_mlp_packed_bytes", [], sz),
+            ("indialign_mlp_save_bytes", [ctypes.c_int], sz),
+            ("indialign_mlp_work_bytes", [ctypes.c_int], sz),
+            ("indialign_mlp_pack", [vp, vp, vp], ctypes.c_int),
+            ("indialign_mlp_forward", [vp, vp, ctypes.c_int, vp, vp, vp], ctypes.c_int),
+            ("indialign_mlp_loss", [vp, vp, ctypes.c_int, ctypes.c_float, vp, vp, vp], ctypes.c_int),
+            ("indialign_mlp_backward", [vp, vp, ctypes.c_int, vp, vp, vp, vp], ctypes.c_int),
+            ("indialign_mlp_adam", [vp, vp, vp, vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, ctypes.c_float, vp], ctypes.c_int)):
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
     if path is None:
         _lib = lib
     return lib
@@ -88,14 +123,46 @@ def last_error() -> str:
     return load().indialign_last_error().decode()
 
 
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, margin: float = 0.02,
+                    audit_rate: float = 0.02, seed: int = 0,
+                    rank_stats: np.ndarray | None = None) -> BatchOptions:
+    """Fill the learned-mode fields of `opts` (keeps `ranker` referenced by
+    the caller, which must outlive the call)."""
+    assert ranker.dtype == np.float32 and ranker.size == RANKER_FLOATS and ranker.flags.c_contiguous
+    opts.mode = MODE_LEARNED
+    opts.ranker = _fptr(ranker)
+    opts.top_k = int(top_k)
+    opts.margin = float(margin)
+    opts.audit_rate = float(audit_rate)
+    opts.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    if rank_stats is not None:
+        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS
+        opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+    return opts
+
+
+def window_count(plen: int, nlen: int, dense: bool = True) -> int:
+    """Dense-rescue windows of a pair with plen / nlen valid residues."""
+    return int(load().indialign_window_count(int(plen), int(nlen), int(dense)))
+
+
 def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = False,
            stage_ms: np.ndarray | None = None, counters: np.ndarray | None = None,
            stage_best: np.ndarray | None = None, kernel_ms: np.ndarray | None = None,
-           stream: int | None = None):
+           stream: int | None = None, ranker: np.ndarray | None = None, top_k: int = 8,
+           margin: float = 0.02, audit_rate: float = 0.02, seed: int = 0,
+           rank_stats: np.ndarray | None = None):
     """Run the batched search on the GPU.
 
     pairs: objects with .pred/.native (L,3) float64, .valid/.pred_valid/
     .native_valid (L,) uint8 and .lnorm.  Returns (score[n], R[n,9], t[n,3]).
+    With `ranker` (FP32 parameter blob) the dense local-fragment rescue runs
+    in learned mode: top_k windows per pair, all windows when the predicted
+    top-1 / top-k margin is below `margin` or on an audit draw.
     """
     lib = load()
     cfg = cfg or default_config()
@@ -104,6 +171,8 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     opts = BatchOptions()
     opts.device = -1
     opts.profile = int(profile)
+    if ranker is not None:
+        learned_options(opts, ranker, top_k, margin, audit_rate, seed, rank_stats)
     if stage_ms is not None:
         assert stage_ms.dtype == np.float64 and stage_ms.size >= STAGES
         opts.stage_ms = stage_ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
@@ -111,7 +180,7 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
         assert counters.dtype == np.int64 and counters.size >= COUNTERS
         opts.counters = counters.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
     if kernel_ms is not None:
-        assert kernel_ms.dtype == np.float64 and kernel_ms.size >= 4
+        assert kernel_ms.dtype == np.float64 and kernel_ms.size >= KERNEL_MS
         opts.kernel_ms = kernel_ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     if stream is not None:
         opts.stream = ctypes.c_void_p(stream)
@@ -123,6 +192,34 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     if rc != 0:
         raise IndialignError(f"indialign_tmscore_search_batch_ex rc={rc}: {last_error()}")
     return abi.results_to_numpy(res, pk.n)
+
+
+def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None):
+    """Plain search in COLLECT mode: every dense-rescue window's 16 raw
+    features and refined score.  Returns (results, feat[W,16] f32, label[W]
+    f32 (NaN where the pair did not reach the dense rescue), woff[n+1]) with
+    pair p's windows at woff[p]:woff[p+1]."""
+    lib = load()
+    cfg = cfg or default_config()
+    pk = abi.PackedInputs(pairs)
+    counts = [window_count(int(np.count_nonzero(p.pred_valid)), int(np.count_nonzero(p.native_valid)))
+              for p in pairs]
+    woff = np.zeros(len(pairs) + 1, np.int64)
+    woff[1:] = np.cumsum(counts)
+    W = int(woff[-1])
+    feat = np.zeros((max(W, 1), FEATURES), np.float32)
+    label = np.zeros(max(W, 1), np.float32)
+    res = (NativePairResult * max(1, pk.n))()
+    opts = BatchOptions()
+    opts.device = -1
+    opts.mode = MODE_COLLECT
+    opts.win_feat = _fptr(feat)
+    opts.win_label = _fptr(label)
+    opts.win_cap = W
+    rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
+    if rc != 0:
+        raise IndialignError(f"indialign_tmscore_search_batch_ex(collect) rc={rc}: {last_error()}")
+    return abi.results_to_numpy(res, pk.n), feat[:W], label[:W], woff
 
 
 def fp64_peak_tflops(device: int = 0) -> float:

@@ -347,4 +347,23 @@ IA_DEV int warp_sum_int(int v) {
     return v;
 }
 
+// Compact coordinate views of one pair (pred / native restricted to their
+// valid residues), as used by the chain and ranker kernels.
+struct Pts {
+    const double *P;  // pred compact xyz
+    const double *Q;  // native compact xyz
+};
+
+// Kabsch over pairs (P[a+i], Q[b+i]), i < cnt (a window), by the warp.
+IA_DEV void warp_kabsch_window(const Pts &x, int a, int b, int cnt, double *R, double *t) {
+    Moments m;
+    m.clear();
+    for (int i = threadIdx.x & 31; i < cnt; i += 32) {
+        const double *p = x.P + 3 * (a + i), *q = x.Q + 3 * (b + i);
+        m.add(p[0], p[1], p[2], q[0], q[1], q[2]);
+    }
+    m.group_sum(32);
+    kabsch_from_moments(m, 3.0, R, t);
+}
+
 }  // namespace ia

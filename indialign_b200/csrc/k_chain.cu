@@ -39,24 +39,6 @@ constexpr unsigned kFull = 0xffffffffu;
 #endif
 constexpr int kNwUnroll = IA_NW_UNROLL;
 
-// ---- warp helpers ----------------------------------------------------------
-struct Pts {
-    const double *P;  // pred compact xyz
-    const double *Q;  // native compact xyz
-};
-
-// Kabsch over pairs (P[a+i], Q[b+i]), i < cnt (a window), by the warp.
-IA_DEV void warp_kabsch_window(const Pts &x, int a, int b, int cnt, double *R, double *t) {
-    Moments m;
-    m.clear();
-    for (int i = threadIdx.x & 31; i < cnt; i += 32) {
-        const double *p = x.P + 3 * (a + i), *q = x.Q + 3 * (b + i);
-        m.add(p[0], p[1], p[2], q[0], q[1], q[2]);
-    }
-    m.group_sum(32);
-    kabsch_from_moments(m, 3.0, R, t);
-}
-
 // Aligned pair k (forward order) from the reversed traceback list.
 IA_DEV void al_get(const uint32_t *al, int na, int k, int &pi, int &ni) {
     uint32_t e = al[na - 1 - k];
@@ -506,7 +488,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             bool live = true;
             if (T.start == START_WINDOW) {
                 int flen, ps, ns;
-                window_at(plen, nlen, T.dense, si, flen, ps, ns);
+                window_at(plen, nlen, T.dense, T.wlist ? T.wlist[si] : si, flen, ps, ns);
                 warp_kabsch_window(x, ps, ns, flen, R, t);
             } else {
                 const double *r = T.rt + (size_t)si * kRec;

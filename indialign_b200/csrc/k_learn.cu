@@ -1,0 +1,771 @@
+// Learned window ranker for the dense local-fragment rescue
+// (evaluate_local_fragment_dp, indialign_c/rescue.h:50-117).
+//
+// The dense rescue refines every (fragment length, pred start, native start)
+// window of a weak pair with a 2-iteration dp_refine chain, thousands of NW
+// chains per pair.  The ranker predicts each window's refined dp_refine score
+// from 16 cheap features, and the search refines only the top-k windows of a
+// pair, falling back to all windows when the predicted top-1 / top-k margin
+// is small and on a random audit of pairs.
+//
+//   k_rank    persistent CTAs over 64-window chunks: per window the warp
+//             computes the features (window Kabsch + diagonal TM sums, FP64),
+//             then the 16 -> 128 -> 128 -> 1 GELU MLP runs on BF16 tensor
+//             cores (mma.sync m16n8k16, FP32 accumulation) over the warp's
+//             16-window tile, with the weights resident in shared memory.
+//   k_select  warp per pair: top-k by (predicted score desc, window asc),
+//             margin fallback, audit draw, window list in ascending order (so
+//             the chain reduction keeps the reference's first-max rule).
+//   k_audit   audited pairs: did the top-k windows contain the best score?
+//   training  forward with saved activations, MSE + pairwise ranking loss,
+//             backward through BF16 tensor-core GEMMs (split-K, fixed-order
+//             sums), Adam on FP32 master weights.
+#include <cuda_bf16.h>
+
+#include "dmath.cuh"
+#include "pipeline.h"
+#include "kernels.h"
+#include "sched.cuh"
+
+namespace ia {
+
+namespace {
+
+constexpr unsigned kAllLanes = 0xffffffffu;
+constexpr int kW1Words = 12;  // bf16 row of W1T (16) padded to 24 -> conflict-free fragments
+constexpr int kW2Words = 68;  // bf16 row of W2T (128) padded to 136
+
+struct MlpSmem {
+    uint32_t w1t[kHidden][kW1Words];
+    uint32_t w2t[kHidden][kW2Words];
+    float b1[kHidden], b2[kHidden], w3[kHidden];
+    float mean[kFeatures], inv_std[kFeatures];
+    float b3, pad_[3];
+};
+
+IA_DEV uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+
+// D += A B for one m16n8k16 BF16 tile (row-major A, column-major B).
+IA_DEV void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
+constexpr float kGeluC = 0.7978845608028654f;
+constexpr float kGeluA = 0.044715f;
+IA_DEV float gelu(float x) {
+    const float u = kGeluC * (x + kGeluA * x * x * x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+IA_DEV float gelu_grad(float x) {
+    const float u = kGeluC * (x + kGeluA * x * x * x);
+    const float th = tanhf(u);
+    return 0.5f * (1.0f + th) + 0.5f * x * (1.0f - th * th) * kGeluC * (1.0f + 3.0f * kGeluA * x * x);
+}
+
+// Copy the packed parameters into the fragment-friendly shared layout (all
+// threads of the CTA; caller synchronises).
+IA_DEV void load_mlp_smem(const MlpPacked *g, MlpSmem *s) {
+    const uint32_t *w1 = reinterpret_cast<const uint32_t *>(g->W1T);
+    const uint32_t *w2 = reinterpret_cast<const uint32_t *>(g->W2T);
+    for (int i = threadIdx.x; i < kHidden * (kFeatures / 2); i += blockDim.x)
+        s->w1t[i / (kFeatures / 2)][i % (kFeatures / 2)] = w1[i];
+    for (int i = threadIdx.x; i < kHidden * (kHidden / 2); i += blockDim.x)
+        s->w2t[i / (kHidden / 2)][i % (kHidden / 2)] = w2[i];
+    for (int i = threadIdx.x; i < kHidden; i += blockDim.x) {
+        s->b1[i] = g->b1[i];
+        s->b2[i] = g->b2[i];
+        s->w3[i] = g->w3[i];
+    }
+    for (int i = threadIdx.x; i < kFeatures; i += blockDim.x) {
+        s->mean[i] = g->mean[i];
+        s->inv_std[i] = g->inv_std[i];
+    }
+    if (threadIdx.x == 0) s->b3 = g->b3;
+}
+
+// The MLP on one 16-row tile by one warp.  xt: [16][16] standardised inputs
+// (FP32, shared).  Lane (g = lane/4, c = lane%4) returns the outputs of rows
+// g and g+8 (valid on every lane of the quad).  With `sv`, rows < nvalid of
+// the tile's activations are stored at rows row0.. of the save arrays.
+IA_DEV void mlp_tile(const MlpSmem &S, const float *xt, float &y_g, float &y_g8, const MlpSave *sv,
+                     long long row0, int nvalid) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, c = lane & 3;
+    const bool st_g = sv && g < nvalid, st_g8 = sv && g + 8 < nvalid;
+    const long long rg = row0 + g, rg8 = row0 + g + 8;
+    uint32_t a[4];
+    a[0] = pack_bf16(xt[g * 16 + 2 * c], xt[g * 16 + 2 * c + 1]);
+    a[1] = pack_bf16(xt[(g + 8) * 16 + 2 * c], xt[(g + 8) * 16 + 2 * c + 1]);
+    a[2] = pack_bf16(xt[g * 16 + 2 * c + 8], xt[g * 16 + 2 * c + 9]);
+    a[3] = pack_bf16(xt[(g + 8) * 16 + 2 * c + 8], xt[(g + 8) * 16 + 2 * c + 9]);
+    if (st_g) {
+        uint32_t *x = reinterpret_cast<uint32_t *>(sv->xn + rg * kFeatures);
+        x[c] = a[0];
+        x[4 + c] = a[2];
+    }
+    if (st_g8) {
+        uint32_t *x = reinterpret_cast<uint32_t *>(sv->xn + rg8 * kFeatures);
+        x[c] = a[1];
+        x[4 + c] = a[3];
+    }
+    // layer 1: [16 x 16] x [16 x 128]
+    uint32_t h[8][4];
+#pragma unroll
+    for (int kk = 0; kk < 8; kk++) {
+        float d[2][4];
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            const int nt = 2 * kk + half, col = 8 * nt + 2 * c;
+            d[half][0] = d[half][2] = S.b1[col];
+            d[half][1] = d[half][3] = S.b1[col + 1];
+            mma_bf16(d[half], a, S.w1t[8 * nt + g][c], S.w1t[8 * nt + g][c + 4]);
+            if (st_g) *reinterpret_cast<float2 *>(sv->z1 + rg * kHidden + col) = make_float2(d[half][0], d[half][1]);
+            if (st_g8) *reinterpret_cast<float2 *>(sv->z1 + rg8 * kHidden + col) = make_float2(d[half][2], d[half][3]);
+        }
+        // accumulator tiles 2kk, 2kk+1 are the A fragment of k-chunk kk
+        h[kk][0] = pack_bf16(gelu(d[0][0]), gelu(d[0][1]));
+        h[kk][1] = pack_bf16(gelu(d[0][2]), gelu(d[0][3]));
+        h[kk][2] = pack_bf16(gelu(d[1][0]), gelu(d[1][1]));
+        h[kk][3] = pack_bf16(gelu(d[1][2]), gelu(d[1][3]));
+        if (st_g) {
+            uint32_t *o = reinterpret_cast<uint32_t *>(sv->h1 + rg * kHidden + 16 * kk);
+            o[c] = h[kk][0];
+            o[4 + c] = h[kk][2];
+        }
+        if (st_g8) {
+            uint32_t *o = reinterpret_cast<uint32_t *>(sv->h1 + rg8 * kHidden + 16 * kk);
+            o[c] = h[kk][1];
+            o[4 + c] = h[kk][3];
+        }
+    }
+    // layer 2: [16 x 128] x [128 x 128], then the w3 head
+    float y0 = 0.f, y8 = 0.f;
+#pragma unroll 4
+    for (int nt = 0; nt < 16; nt++) {
+        const int col = 8 * nt + 2 * c;
+        float d[4] = {S.b2[col], S.b2[col + 1], S.b2[col], S.b2[col + 1]};
+        const uint32_t *wr = S.w2t[8 * nt + g];
+#pragma unroll
+        for (int kk = 0; kk < 8; kk++) mma_bf16(d, h[kk], wr[8 * kk + c], wr[8 * kk + c + 4]);
+        if (st_g) *reinterpret_cast<float2 *>(sv->z2 + rg * kHidden + col) = make_float2(d[0], d[1]);
+        if (st_g8) *reinterpret_cast<float2 *>(sv->z2 + rg8 * kHidden + col) = make_float2(d[2], d[3]);
+        y0 += gelu(d[0]) * S.w3[col] + gelu(d[1]) * S.w3[col + 1];
+        y8 += gelu(d[2]) * S.w3[col] + gelu(d[3]) * S.w3[col + 1];
+    }
+    y0 += __shfl_xor_sync(kAllLanes, y0, 1);
+    y0 += __shfl_xor_sync(kAllLanes, y0, 2);
+    y8 += __shfl_xor_sync(kAllLanes, y8, 1);
+    y8 += __shfl_xor_sync(kAllLanes, y8, 2);
+    y_g = y0 + S.b3;
+    y_g8 = y8 + S.b3;
+}
+
+// The 16 features of window w of a pair (raw, before standardisation),
+// computed by the whole warp; every lane returns all 16.
+//   0 fragment length / ml        1 pred start / (plen-1)   2 native start / (nlen-1)
+//   3 start shift / ml            4 window RMSD / 10        5 TM along the window's
+//   diagonal under its Kabsch     6, 7 fraction of that diagonal within d0, 2 d0
+//   8 window-local TM             9, 10 stem fraction of the pred / native window
+//   11 log(ml) / 7                12 running best score     13 d0 / 10
+//   14 min(RMSD / d0, 10) / 10    15 TM along the same-index diagonal
+// (ml = min(plen, nlen); indices are compact valid-residue positions.)
+IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, const PairInfo &I,
+                            double best, int dense, int w, float (&f)[kFeatures]) {
+    const int lane = threadIdx.x & 31;
+    const int plen = I.plen, nlen = I.nlen, ml = plen < nlen ? plen : nlen;
+    int flen, ps, ns;
+    window_at(plen, nlen, dense, w, flen, ps, ns);
+    double R[9], t[3];
+    warp_kabsch_window(x, ps, ns, flen, R, t);
+    const double d0sq = I.d0 * I.d0, inv = 1.0 / d0sq;
+    double sd2 = 0.0, stm = 0.0, sp = 0.0, sn = 0.0;
+    for (int i = lane; i < flen; i += 32) {
+        const double *p = x.P + 3 * (ps + i), *q = x.Q + 3 * (ns + i);
+        const double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
+        sd2 += d2;
+        stm += 1.0 / (1.0 + d2 * inv);
+        sp += Lp[ps + i] != 'L' ? 1.0 : 0.0;
+        sn += Ln[ns + i] != 'L' ? 1.0 : 0.0;
+    }
+    const int s = ns - ps;
+    const int lo = s < 0 ? -s : 0, hi = plen < nlen - s ? plen : nlen - s;
+    double dtm = 0.0, c1 = 0.0, c2 = 0.0, tm0 = 0.0;
+    for (int i = lo + lane; i < hi; i += 32) {
+        const double *p = x.P + 3 * i, *q = x.Q + 3 * (i + s);
+        const double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
+        dtm += 1.0 / (1.0 + d2 * inv);
+        c1 += d2 < d0sq ? 1.0 : 0.0;
+        c2 += d2 < 4.0 * d0sq ? 1.0 : 0.0;
+    }
+    for (int i = lane; i < ml; i += 32) {
+        const double *p = x.P + 3 * i, *q = x.Q + 3 * i;
+        tm0 += 1.0 / (1.0 + dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]) * inv);
+    }
+    sd2 = warp_sum(sd2);
+    stm = warp_sum(stm);
+    sp = warp_sum(sp);
+    sn = warp_sum(sn);
+    dtm = warp_sum(dtm);
+    c1 = warp_sum(c1);
+    c2 = warp_sum(c2);
+    tm0 = warp_sum(tm0);
+    const double mld = (double)ml, rmsd = sqrt(sd2 / flen);
+    f[0] = (float)(flen / mld);
+    f[1] = (float)(ps / (double)(plen > 1 ? plen - 1 : 1));
+    f[2] = (float)(ns / (double)(nlen > 1 ? nlen - 1 : 1));
+    f[3] = (float)(s / mld);
+    f[4] = (float)(rmsd / 10.0);
+    f[5] = (float)(dtm / I.lnorm);
+    f[6] = (float)(c1 / mld);
+    f[7] = (float)(c2 / mld);
+    f[8] = (float)(stm / flen);
+    f[9] = (float)(sp / flen);
+    f[10] = (float)(sn / flen);
+    f[11] = (float)(log(mld) / 7.0);
+    f[12] = (float)best;
+    f[13] = (float)(I.d0 / 10.0);
+    f[14] = (float)(fmin(rmsd / I.d0, 10.0) / 10.0);
+    f[15] = (float)(tm0 / I.lnorm);
+}
+
+}  // namespace
+
+// ---- ranking: features + MLP over the windows of gated pairs ------------------
+__global__ void k_plan_rank(DevBatch b, int dense, int *counts) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= b.n) return;
+    const PairInfo &I = b.info[p];
+    const int W = window_count(I.plen, I.nlen, dense);
+    const bool on = I.status == 0 && b.state[p].flag && W > 0;
+    counts[p] = on ? (W + kRankChunk - 1) / kRankChunk : 0;
+}
+
+__global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int *__restrict__ chunk_begin,
+                                              const ScanOut *__restrict__ scan, int *counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(smem_raw);
+    float *xt = reinterpret_cast<float *>(smem_raw + sizeof(MlpSmem)) + (threadIdx.x >> 5) * 256;
+    __shared__ int s_chunk, s_pair;
+    if (a.mlp) load_mlp_smem(a.mlp, &S);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = scan->total_chunks;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int c = atomicAdd(counter, 1);
+            int t = -1;
+            if (c < total) {
+                int lo = 0, hi = b.n;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (chunk_begin[mid] <= c) lo = mid + 1; else hi = mid;
+                }
+                t = lo - 1;
+            }
+            s_chunk = c;
+            s_pair = t;
+        }
+        __syncthreads();
+        const int c = s_chunk, p = s_pair;
+        if (c >= total || p < 0) break;
+        const PairInfo &I = b.info[p];
+        const int W = window_count(I.plen, I.nlen, a.dense);
+        const int w0 = (c - chunk_begin[p]) * kRankChunk + warp * 16;
+        if (w0 < W) {
+            const Pts x = {b.predc + 3 * (size_t)I.off, b.natc + 3 * (size_t)I.off};
+            const uint8_t *Lp = reinterpret_cast<const uint8_t *>(b.sspc + I.off);
+            const uint8_t *Ln = reinterpret_cast<const uint8_t *>(b.ssnc + I.off);
+            const double best = b.state[p].rec[REC_BEST][0];
+            const long long wb = a.wbase[p];
+            for (int r = 0; r < 16; r++) {
+                const int w = w0 + r;
+                float mine = 0.f;
+                if (w < W) {
+                    float f[kFeatures];
+                    window_features(x, Lp, Ln, I, best, a.dense, w, f);
+#pragma unroll
+                    for (int j = 0; j < kFeatures; j++)
+                        if (lane == j) mine = f[j];
+                    if (a.feat && lane < kFeatures) a.feat[(wb + w) * kFeatures + lane] = mine;
+                }
+                if (lane < kFeatures)
+                    xt[r * 16 + lane] = (w < W && a.mlp) ? (mine - S.mean[lane]) * S.inv_std[lane] : 0.f;
+            }
+            __syncwarp();
+            if (a.mlp) {
+                float y0, y8;
+                mlp_tile(S, xt, y0, y8, nullptr, 0, 0);
+                const int g = lane >> 2;
+                if ((lane & 3) == 0) {
+                    if (w0 + g < W) a.score[wb + w0 + g] = y0;
+                    if (w0 + g + 8 < W) a.score[wb + w0 + g + 8] = y8;
+                }
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+// ---- top-k selection ------------------------------------------------------------
+IA_DEV unsigned long long mix64(unsigned long long z) {  // splitmix64 finaliser
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_select(DevBatch b, SelectArgs a) {
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (p >= b.n) return;
+    const PairInfo &I = b.info[p];
+    int *list = a.wlist + (size_t)p * kMaxTopK;
+    if (I.status != 0 || !b.state[p].flag) {
+        if (lane == 0) a.wcount[p] = -1;
+        list[lane] = -1;
+        return;
+    }
+    const int W = window_count(I.plen, I.nlen, a.dense);
+    const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
+    if (lane == 0) {
+        atomicAdd(a.stats + RS_GATED, 1ull);
+        atomicAdd(a.stats + RS_WINDOWS, (unsigned long long)W);
+    }
+    if (W <= k) {
+        list[lane] = -1;
+        if (lane == 0) {
+            a.wcount[p] = -1;
+            atomicAdd(a.stats + RS_SMALL, 1ull);
+            atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
+        }
+        return;
+    }
+    const float *sc = a.score + a.wbase[p];
+    // k rounds of "next in (score desc, window asc) order"
+    float prev_s = INFINITY, top1 = 0.f;
+    int prev_i = -1;
+    for (int r = 0; r < k; r++) {
+        float bs = -INFINITY;
+        int bi = 0x7fffffff;
+        for (int w = lane; w < W; w += 32) {
+            float v = sc[w];
+            if (!(v == v)) v = -INFINITY;
+            const bool after = v < prev_s || (v == prev_s && w > prev_i);
+            if (after && (v > bs || (v == bs && w < bi))) {
+                bs = v;
+                bi = w;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float s2 = __shfl_xor_sync(kAllLanes, bs, o);
+            const int i2 = __shfl_xor_sync(kAllLanes, bi, o);
+            if (s2 > bs || (s2 == bs && i2 < bi)) {
+                bs = s2;
+                bi = i2;
+            }
+        }
+        if (r == 0) top1 = bs;
+        prev_s = bs;
+        prev_i = bi;
+        if (lane == 0) list[r] = bi;
+    }
+    if (lane == 0) {
+        for (int i = 1; i < k; i++)  // ascending window order
+            for (int j = i; j > 0 && list[j] < list[j - 1]; j--) {
+                const int t = list[j]; list[j] = list[j - 1]; list[j - 1] = t;
+            }
+        const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)p + 0x9e3779b97f4a7c15ull)) >> 11) *
+                         (1.0 / 9007199254740992.0);
+        if (u < a.audit_rate) {
+            a.wcount[p] = -2;
+            atomicAdd(a.stats + RS_AUDIT, 1ull);
+            atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
+        } else if (top1 - prev_s < a.margin) {
+            a.wcount[p] = -1;
+            atomicAdd(a.stats + RS_FALLBACK, 1ull);
+            atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
+        } else {
+            a.wcount[p] = k;
+            atomicAdd(a.stats + RS_PRUNED, 1ull);
+            atomicAdd(a.stats + RS_REFINED, (unsigned long long)k);
+        }
+    }
+}
+
+// A window's refined score: the dp_refine result over its two gap chains
+// (later chain only if strictly better, indialign_c/align.h:131-145).
+IA_DEV double window_score(const double *res, int w) {
+    const double s0 = res[(size_t)(2 * w) * kRec], s1 = res[(size_t)(2 * w + 1) * kRec];
+    return s1 > s0 ? s1 : s0;
+}
+
+// Audited pairs ran every window: count those whose selected windows miss the
+// best window score.
+__global__ void k_audit(DevBatch b, SelectArgs a, const double *chain_res, const long long *chain_base) {
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (p >= b.n || a.wcount[p] != -2) return;
+    const PairInfo &I = b.info[p];
+    const int W = window_count(I.plen, I.nlen, a.dense);
+    const double *res = chain_res + (size_t)chain_base[p] * kRec;
+    const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
+    double full = -INFINITY, sel = -INFINITY;
+    for (int w = lane; w < W; w += 32) full = fmax(full, window_score(res, w));
+    for (int r = lane; r < k; r += 32) sel = fmax(sel, window_score(res, a.wlist[(size_t)p * kMaxTopK + r]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        full = fmax(full, __shfl_xor_sync(kAllLanes, full, o));
+        sel = fmax(sel, __shfl_xor_sync(kAllLanes, sel, o));
+    }
+    if (lane == 0 && sel < full) atomicAdd(a.stats + RS_AUDIT_MISS, 1ull);
+}
+
+// Training labels: every window's refined score for pairs that ran the stage
+// on all windows, NaN elsewhere.
+__global__ void k_collect_labels(DevBatch b, const long long *wbase, const double *chain_res,
+                                 const long long *chain_base, int dense, float *label) {
+    const int p = blockIdx.x;
+    const PairInfo &I = b.info[p];
+    const int W = window_count(I.plen, I.nlen, dense);
+    const bool on = I.status == 0 && b.state[p].flag;
+    const double *res = chain_res + (size_t)(on ? chain_base[p] : 0) * kRec;
+    float *out = label + wbase[p];
+    for (int w = threadIdx.x; w < W; w += blockDim.x) out[w] = on ? (float)window_score(res, w) : NAN;
+}
+
+// ---- training ---------------------------------------------------------------------
+__global__ void k_mlp_pack(const float *__restrict__ blob, MlpPacked *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kHidden * kFeatures) {  // W1T[o][k] = W1[k][o]
+        const int o = i / kFeatures, k = i % kFeatures;
+        out->W1T[i] = __bfloat16_as_ushort(__float2bfloat16_rn(blob[kBlobW1 + k * kHidden + o]));
+    }
+    if (i < kHidden * kHidden) {
+        const int o = i / kHidden, k = i % kHidden;
+        out->W2T[i] = __bfloat16_as_ushort(__float2bfloat16_rn(blob[kBlobW2 + k * kHidden + o]));
+        out->W2[i] = __bfloat16_as_ushort(__float2bfloat16_rn(blob[kBlobW2 + i]));
+    }
+    if (i < kHidden) {
+        out->b1[i] = blob[kBlobB1 + i];
+        out->b2[i] = blob[kBlobB2 + i];
+        out->w3[i] = blob[kBlobW3 + i];
+    }
+    if (i < kFeatures) {
+        out->mean[i] = blob[kBlobMean + i];
+        const float sd = blob[kBlobStd + i];
+        out->inv_std[i] = sd > 0.f ? 1.0f / sd : 1.0f;
+    }
+    if (i == 0) out->b3 = blob[kBlobB3];
+}
+
+// Forward over n raw feature rows (row-major [n][16]); 4 warps x 16 rows per CTA.
+__global__ void __launch_bounds__(128) k_mlp_forward(const MlpPacked *mlp, const float *__restrict__ x, int n,
+                                                     float *y, MlpSave sv, int save) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MlpSmem &S = *reinterpret_cast<MlpSmem *>(smem_raw);
+    float *xt = reinterpret_cast<float *>(smem_raw + sizeof(MlpSmem)) + (threadIdx.x >> 5) * 256;
+    load_mlp_smem(mlp, &S);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const long long row0 = (long long)blockIdx.x * 64 + (threadIdx.x >> 5) * 16;
+    if (row0 >= n) return;
+    const int nvalid = n - row0 < 16 ? (int)(n - row0) : 16;
+    for (int e = lane; e < 256; e += 32) {
+        const int r = e >> 4, j = e & 15;
+        xt[e] = r < nvalid ? (x[(row0 + r) * kFeatures + j] - S.mean[j]) * S.inv_std[j] : 0.f;
+    }
+    __syncwarp();
+    float y0, y8;
+    mlp_tile(S, xt, y0, y8, save ? &sv : nullptr, row0, nvalid);
+    const int g = lane >> 2;
+    if ((lane & 3) == 0) {
+        if (g < nvalid) y[row0 + g] = y0;
+        if (g + 8 < nvalid) y[row0 + g + 8] = y8;
+    }
+}
+
+// Loss over n = 2m predictions: mean squared error plus lambda x a pairwise
+// logistic ranking term on the rows (2i, 2i+1), which the caller draws from
+// the same pair.  One CTA; fixed-order reduction.
+__global__ void __launch_bounds__(1024) k_mlp_loss(const float *__restrict__ y, const float *__restrict__ t,
+                                                   int n, float lambda, float *dy, float *loss) {
+    __shared__ float red[32];
+    const int m = n / 2;
+    float acc = 0.f;
+    const float inv_n = 1.0f / (float)(n > 0 ? n : 1), inv_m = 1.0f / (float)(m > 0 ? m : 1);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int ia = 2 * i, ib = 2 * i + 1;
+        const float ea = y[ia] - t[ia], eb = y[ib] - t[ib];
+        float ga = 2.f * ea * inv_n, gb = 2.f * eb * inv_n;
+        acc += (ea * ea + eb * eb) * inv_n;
+        const float dt = t[ia] - t[ib];
+        if (fabsf(dt) > 1e-6f) {
+            const float sgn = dt > 0.f ? 1.f : -1.f;
+            const float z = -sgn * (y[ia] - y[ib]);
+            const float sp = z > 20.f ? z : log1pf(expf(z));
+            const float sig = 1.f / (1.f + expf(-z));
+            acc += lambda * sp * inv_m;
+            ga += -lambda * sgn * sig * inv_m;
+            gb += lambda * sgn * sig * inv_m;
+        }
+        dy[ia] = ga;
+        dy[ib] = gb;
+    }
+    if ((n & 1) && threadIdx.x == 0) {  // odd tail: MSE only
+        const float e = y[n - 1] - t[n - 1];
+        acc += e * e * inv_n;
+        dy[n - 1] = 2.f * e * inv_n;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kAllLanes, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+        *loss = s;
+    }
+}
+
+// Head backward: dz2 = dy w3 gelu'(z2) (bf16), db2 = colsum(dz2),
+// dw3 = sum_b dy gelu(z2), db3 = sum dy.  Block = 32 columns x 8 row groups.
+__global__ void __launch_bounds__(256) k_mlp_head_bwd(const MlpPacked *mlp, const float *__restrict__ dy,
+                                                      const float *__restrict__ z2, int n, uint16_t *dz2,
+                                                      float *grad) {
+    __shared__ float r_b2[8][33], r_w3[8][33];
+    const int col = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;
+    const float w3 = mlp->w3[col];
+    float sb = 0.f, sw = 0.f;
+    for (int r = rg; r < n; r += 8) {
+        const float z = z2[(size_t)r * kHidden + col], d = dy[r];
+        const float dz = d * w3 * gelu_grad(z);
+        dz2[(size_t)r * kHidden + col] = __bfloat16_as_ushort(__float2bfloat16_rn(dz));
+        sb += dz;
+        sw += d * gelu(z);
+    }
+    r_b2[rg][threadIdx.x & 31] = sb;
+    r_w3[rg][threadIdx.x & 31] = sw;
+    __syncthreads();
+    if (rg == 0) {
+        float b2 = 0.f, w = 0.f;
+        for (int k = 0; k < 8; k++) {
+            b2 += r_b2[k][threadIdx.x];
+            w += r_w3[k][threadIdx.x];
+        }
+        grad[kBlobB2 + col] = b2;
+        grad[kBlobW3 + col] = w;
+    }
+    if (blockIdx.x == 0 && rg == 1) {
+        float s = 0.f;
+        for (int r = threadIdx.x & 31; r < n; r += 32) s += dy[r];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kAllLanes, s, o);
+        if ((threadIdx.x & 31) == 0) grad[kBlobB3] = s;
+    }
+}
+
+// dz = dh gelu'(z) (bf16) and its column sums.
+__global__ void __launch_bounds__(256) k_mlp_act_bwd(const float *__restrict__ dh, const float *__restrict__ z,
+                                                     int n, uint16_t *dz, float *dbias) {
+    __shared__ float red[8][33];
+    const int col = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;
+    float s = 0.f;
+    for (int r = rg; r < n; r += 8) {
+        const size_t i = (size_t)r * kHidden + col;
+        const float v = dh[i] * gelu_grad(z[i]);
+        dz[i] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+        s += v;
+    }
+    red[rg][threadIdx.x & 31] = s;
+    __syncthreads();
+    if (rg == 0) {
+        float t = 0.f;
+        for (int k = 0; k < 8; k++) t += red[k][threadIdx.x];
+        dbias[col] = t;
+    }
+}
+
+// BF16 GEMM tile kernel: 64 x 64 output tile per CTA (2 x 2 warps of 32 x 32),
+// K in steps of 32 staged through shared memory; gridDim.z splits K.
+constexpr int kGBM = 64, kGBN = 64, kGBK = 32, kGStride = kGBK + 8;
+__global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t *__restrict__ A, int ta,
+                                                   const uint16_t *__restrict__ B, int tb, int M, int N, int K,
+                                                   int kper, float *out) {
+    __shared__ __align__(16) uint16_t As[kGBM][kGStride];
+    __shared__ __align__(16) uint16_t Bs[kGBN][kGStride];
+    const int m0 = blockIdx.y * kGBM, n0 = blockIdx.x * kGBN;
+    const int kbeg = blockIdx.z * kper, kend = min(K, kbeg + kper);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32, g = lane >> 2, c = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
+    for (int k0 = kbeg; k0 < kend; k0 += kGBK) {
+        for (int e = tid; e < kGBM * kGBK; e += 128) {
+            int m, k;
+            if (ta) { k = e / kGBM; m = e % kGBM; } else { m = e / kGBK; k = e % kGBK; }
+            const int gm = m0 + m, gk = k0 + k;
+            uint16_t v = 0;
+            if (gm < M && gk < kend) v = ta ? A[(size_t)gk * M + gm] : A[(size_t)gm * K + gk];
+            As[m][k] = v;
+        }
+        for (int e = tid; e < kGBN * kGBK; e += 128) {
+            int nn, k;
+            if (tb) { nn = e / kGBK; k = e % kGBK; } else { k = e / kGBN; nn = e % kGBN; }
+            const int gn = n0 + nn, gk = k0 + k;
+            uint16_t v = 0;
+            if (gn < N && gk < kend) v = tb ? B[(size_t)gn * K + gk] : B[(size_t)gk * N + gn];
+            Bs[nn][k] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kGBK; kk += 16) {
+            uint32_t a[2][4];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = wm + 16 * i + g;
+                a[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * c]);
+                a[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * c]);
+                a[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * c + 8]);
+                a[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * c + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int cn = wn + 8 * j + g;
+                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&Bs[cn][kk + 2 * c]);
+                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&Bs[cn][kk + 2 * c + 8]);
+#pragma unroll
+                for (int i = 0; i < 2; i++) mma_bf16(acc[i][j], a[i], b0, b1);
+            }
+        }
+        __syncthreads();
+    }
+    float *o = out + (size_t)blockIdx.z * M * N;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = m0 + wm + 16 * i + g, cc = n0 + wn + 8 * j + 2 * c;
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int rr = r + (e >> 1) * 8, col = cc + (e & 1);
+                if (rr < M && col < N) o[(size_t)rr * N + col] = acc[i][j][e];
+            }
+        }
+}
+
+__global__ void k_splitk_sum(const float *__restrict__ part, int splits, int mn, float *C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mn) return;
+    float s = 0.f;
+    for (int z = 0; z < splits; z++) s += part[(size_t)z * mn + i];
+    C[i] = s;
+}
+
+// Adam with bias correction factors bc1 = 1 - b1^t, bc2 = 1 - b2^t.
+__global__ void k_adam(float *w, const float *__restrict__ g, float *m, float *v, int n, int first,
+                       float lr, float b1, float b2, float eps, float bc1, float bc2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + first;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+}
+
+// ---- launch wrappers ------------------------------------------------------------
+size_t rank_smem_bytes() { return sizeof(MlpSmem) + 4 * 256 * sizeof(float); }
+
+const void *rank_kernel_ptr() { return (const void *)k_rank; }
+
+cudaError_t rank_set_attributes() {
+    cudaError_t e = cudaFuncSetAttribute(k_rank, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)rank_smem_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)rank_smem_bytes());
+    return e;
+}
+
+void launch_plan_rank(const DevBatch &b, int dense, int *counts, cudaStream_t st) {
+    if (b.n > 0) k_plan_rank<<<(b.n + 127) / 128, 128, 0, st>>>(b, dense, counts);
+}
+
+void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
+                 int *counter, int grid, cudaStream_t st) {
+    if (b.n > 0) k_rank<<<grid, 128, rank_smem_bytes(), st>>>(b, a, chunk_begin, scan, counter);
+}
+
+void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st) {
+    if (b.n > 0) k_select<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a);
+}
+
+void launch_audit(const DevBatch &b, const SelectArgs &a, const double *chain_res,
+                  const long long *chain_base, cudaStream_t st) {
+    if (b.n > 0) k_audit<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a, chain_res, chain_base);
+}
+
+void launch_collect_labels(const DevBatch &b, const long long *wbase, const double *chain_res,
+                           const long long *chain_base, int dense, float *label, cudaStream_t st) {
+    if (b.n > 0) k_collect_labels<<<b.n, 256, 0, st>>>(b, wbase, chain_res, chain_base, dense, label);
+}
+
+void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st) {
+    k_mlp_pack<<<(kHidden * kHidden + 255) / 256, 256, 0, st>>>(blob, out);
+}
+
+void launch_mlp_forward(const MlpPacked *mlp, const float *x, int n, float *y, const MlpSave *save,
+                        cudaStream_t st) {
+    if (n <= 0) return;
+    MlpSave sv = save ? *save : MlpSave{nullptr, nullptr, nullptr, nullptr};
+    k_mlp_forward<<<(n + 63) / 64, 128, rank_smem_bytes(), st>>>(mlp, x, n, y, sv, save ? 1 : 0);
+}
+
+void launch_mlp_loss(const float *y, const float *t, int n, float lambda, float *dy, float *loss,
+                     cudaStream_t st) {
+    k_mlp_loss<<<1, 1024, 0, st>>>(y, t, n, lambda, dy, loss);
+}
+
+void launch_mlp_head_bwd(const MlpPacked *mlp, const float *dy, const float *z2, int n, uint16_t *dz2,
+                         float *grad, cudaStream_t st) {
+    k_mlp_head_bwd<<<kHidden / 32, 256, 0, st>>>(mlp, dy, z2, n, dz2, grad);
+}
+
+void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *dbias,
+                        cudaStream_t st) {
+    k_mlp_act_bwd<<<kHidden / 32, 256, 0, st>>>(dh, z, n, dz, dbias);
+}
+
+void launch_gemm_bf16(const uint16_t *A, int ta, const uint16_t *B, int tb, int M, int N, int K,
+                      float *C, float *partial, int splits, cudaStream_t st) {
+    if (splits < 1) splits = 1;
+    int kper = (K + splits - 1) / splits;
+    kper = (kper + kGBK - 1) / kGBK * kGBK;
+    splits = (K + kper - 1) / kper;
+    if (splits < 1) splits = 1;
+    dim3 grid((N + kGBN - 1) / kGBN, (M + kGBM - 1) / kGBM, splits);
+    if (splits == 1) {
+        k_gemm_bf16<<<grid, 128, 0, st>>>(A, ta, B, tb, M, N, K, kper, C);
+        return;
+    }
+    k_gemm_bf16<<<grid, 128, 0, st>>>(A, ta, B, tb, M, N, K, kper, partial);
+    k_splitk_sum<<<(M * N + 255) / 256, 256, 0, st>>>(partial, splits, M * N, C);
+}
+
+void launch_adam(float *w, const float *g, float *m, float *v, int n, int first, float lr, float b1,
+                 float b2, float eps, float bc1, float bc2, cudaStream_t st) {
+    if (n > first)
+        k_adam<<<(n - first + 255) / 256, 256, 0, st>>>(w, g, m, v, n, first, lr, b1, b2, eps, bc1, bc2);
+}
+
+}  // namespace ia

@@ -156,6 +156,7 @@ __global__ void k_plan_chain(DevBatch b, PlanCtx c) {
     T.res = c.base ? c.chain_res + (size_t)c.base[s] * kRec : nullptr;
     T.na_out = nullptr;
     T.live = nullptr;
+    T.wlist = nullptr;
     T.alP = T.alQ = nullptr;
     T.al_cap = I.N;
     bool on = I.status == 0;
@@ -190,6 +191,10 @@ __global__ void k_plan_chain(DevBatch b, PlanCtx c) {
         T.start = START_WINDOW;
         T.dense = c.iters;  // 0 normal, 1 dense
         T.n_starts = window_count(I.plen, I.nlen, T.dense);
+        if (c.wcount && c.wcount[p] >= 0) {  // ranked: the selected windows only
+            T.n_starts = c.wcount[p];
+            T.wlist = c.wlist + (size_t)p * kMaxTopK;
+        }
         T.max_iter = 2;
         T.sd8 = 100.0;
         on = on && S.flag;

@@ -97,6 +97,79 @@ void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t
                         double *bH, uint32_t *al, int *ap, int *an, int *na,
                         unsigned long long *ctr, cudaStream_t st);
 
+// k_learn.cu -------------------------------------------------------------------
+// Ranker parameters on device: FP32 biases / standardisation and BF16 weight
+// copies in the layouts the tensor-core fragments read (built from a blob by
+// launch_mlp_pack).
+struct MlpPacked {
+    float mean[kFeatures], inv_std[kFeatures];
+    float b1[kHidden], b2[kHidden], w3[kHidden];
+    float b3, pad_[3];
+    uint16_t W1T[kHidden * kFeatures];  // bf16 [out][in]
+    uint16_t W2T[kHidden * kHidden];    // bf16 [out][in]
+    uint16_t W2[kHidden * kHidden];     // bf16 [in][out]
+};
+
+// Per-sample activations kept by a training forward pass.
+struct MlpSave {
+    uint16_t *xn;  // bf16 [n][16] standardised inputs
+    float *z1;     // [n][128] layer-1 pre-activations
+    uint16_t *h1;  // bf16 [n][128] gelu(z1)
+    float *z2;     // [n][128] layer-2 pre-activations
+};
+
+struct RankArgs {
+    const MlpPacked *mlp;      // nullptr: features only
+    const long long *wbase;    // [n] first window of a pair in the window arrays
+    float *score;              // [windows] predicted refined score
+    float *feat;               // optional [windows][16] raw features
+    int dense;
+};
+
+struct SelectArgs {
+    const long long *wbase;
+    const float *score;
+    int *wcount;               // [n] selected windows, -1 = all
+    int *wlist;                // [n][kMaxTopK]
+    int top_k;
+    float margin;
+    double audit_rate;
+    unsigned long long seed;
+    int dense;
+    unsigned long long *stats;  // [kRankStats]
+};
+
+void launch_plan_rank(const DevBatch &b, int dense, int *counts, cudaStream_t st);
+void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
+                 int *counter, int grid, cudaStream_t st);
+cudaError_t rank_set_attributes();
+size_t rank_smem_bytes();
+const void *rank_kernel_ptr();
+void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st);
+void launch_audit(const DevBatch &b, const SelectArgs &a, const double *chain_res,
+                  const long long *chain_base, cudaStream_t st);
+void launch_collect_labels(const DevBatch &b, const long long *wbase, const double *chain_res,
+                           const long long *chain_base, int dense, float *label, cudaStream_t st);
+void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st);
+void launch_mlp_forward(const MlpPacked *mlp, const float *x, int n, float *y, const MlpSave *save,
+                        cudaStream_t st);
+void launch_mlp_loss(const float *y, const float *t, int n, float lambda, float *dy, float *loss,
+                     cudaStream_t st);
+// dZ = dH (or dy x w3) * gelu'(Z) as bf16, with column sums (bias gradients)
+// and, for the head, the w3 / b3 gradients.
+void launch_mlp_head_bwd(const MlpPacked *mlp, const float *dy, const float *z2, int n,
+                         uint16_t *dz2, float *grad, cudaStream_t st);
+void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *dbias,
+                        cudaStream_t st);
+// C[M][N] = op(A)[M][K] op(B)[K][N] on BF16 tensor cores, FP32 out; A is
+// [M][K] (ta = 0) or [K][M] (ta = 1) row-major, B is [K][N] (tb = 0) or
+// [N][K] (tb = 1).  K is split over `splits` partial products summed in a
+// fixed order into C.
+void launch_gemm_bf16(const uint16_t *A, int ta, const uint16_t *B, int tb, int M, int N, int K,
+                      float *C, float *partial, int splits, cudaStream_t st);
+void launch_adam(float *w, const float *g, float *m, float *v, int n, int first, float lr, float b1,
+                 float b2, float eps, float bc1, float bc2, cudaStream_t st);
+
 // k_plan.cu
 void launch_plan_bank(const DevBatch &b, const PlanCtx &c, cudaStream_t st);
 void launch_plan_chain(const DevBatch &b, const PlanCtx &c, cudaStream_t st);

@@ -113,6 +113,7 @@ struct ChainTask {
     double *res;         // LITE: n_starts*gaps records; EMIT: see below
     int *na_out;         // EMIT: aligned pair count per start
     const int *live;     // optional per-start on/off flags
+    const int *wlist;    // START_WINDOW: window index of start si (nullptr: si)
     double *alP, *alQ;   // EMIT: aligned coordinates (contiguous)
     int al_cap;          // capacity per EMIT start
     int n_chains;        // n_starts*gaps (0 = inactive)
@@ -141,6 +142,8 @@ struct PlanCtx {
     double *alP, *alQ;      // aligned sets (2 per pair)
     double *chain_res;      // LITE chain results
     double *recs, *recs2;   // stage record arrays (threading det, offset starts/results)
+    const int *wcount;      // CH_LOCAL: per pair selected windows (-1: all), or nullptr
+    const int *wlist;       // CH_LOCAL: per pair kMaxTopK selected windows, ascending
     int max_iter, iters;
     double early_term;
 };
@@ -156,6 +159,41 @@ struct GlueArgs {
 struct ScanOut {
     int total_chunks;
     int error;           // device-side error flags (bounded waits, caps)
+};
+
+// ---- learned window ranker ---------------------------------------------------
+// A 16 -> 128 -> 128 -> 1 GELU MLP predicts each rescue window's refined
+// dp_refine score from cheap features; the search refines only the top-k
+// windows of a pair (k_learn.cu).
+constexpr int kFeatures = 16;
+constexpr int kHidden = 128;
+constexpr int kMaxTopK = 32;
+constexpr int kRankChunk = 64;  // windows per CTA chunk of the ranker (4 warps x 16)
+
+// FP32 parameter blob: mean[16] std[16] W1[16][128] b1[128] W2[128][128]
+// b2[128] w3[128] b3, weights stored [in][out] row-major.  mean/std
+// standardise the raw features and are not trained.
+constexpr int kBlobMean = 0;
+constexpr int kBlobStd = kBlobMean + kFeatures;
+constexpr int kBlobW1 = kBlobStd + kFeatures;
+constexpr int kBlobB1 = kBlobW1 + kFeatures * kHidden;
+constexpr int kBlobW2 = kBlobB1 + kHidden;
+constexpr int kBlobB2 = kBlobW2 + kHidden * kHidden;
+constexpr int kBlobW3 = kBlobB2 + kHidden;
+constexpr int kBlobB3 = kBlobW3 + kHidden;
+constexpr int kBlobSize = kBlobB3 + 1;
+
+// Ranker statistics of one batch (IndialignBatchOptions.rank_stats).
+enum RankStat {
+    RS_GATED = 0,      // pairs that reached the ranked stage
+    RS_FALLBACK,       // ... refined on all windows: predicted margin below threshold
+    RS_AUDIT,          // ... refined on all windows: random audit
+    RS_PRUNED,         // ... refined on the top-k windows only
+    RS_WINDOWS,        // windows of the gated pairs
+    RS_REFINED,        // windows refined
+    RS_AUDIT_MISS,     // audited pairs whose top-k windows miss the best window score
+    RS_SMALL,          // gated pairs with at most k windows (all refined)
+    kRankStats
 };
 
 // Error bits reported through ScanOut.error / the batch status word.

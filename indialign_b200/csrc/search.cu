@@ -89,6 +89,11 @@ struct Ctx {
     DBuf<int> lay_i;
     DBuf<long long> lay_l;
     DBuf<unsigned long long> ctr;
+    // learned window ranker
+    DBuf<float> blob, wscore, wfeat, wlabel;
+    DBuf<MlpPacked> mlp;
+    DBuf<int> wcount, wlist;
+    DBuf<unsigned long long> rstats;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<double> h_pred, h_nat, h_lnorm;
     std::vector<uint8_t> h_v, h_pv, h_nv;
@@ -121,6 +126,7 @@ static int acquire(int device, Ctx **out) {
     std::call_once(g_attr_once[device & 63], [&]() {
         attr_err = bank_set_attributes();
         if (attr_err == cudaSuccess) attr_err = chain_set_attributes();
+        if (attr_err == cudaSuccess) attr_err = rank_set_attributes();
     });
     CK(attr_err);
     *out = c;
@@ -153,6 +159,10 @@ constexpr int kTrace = INDIALIGN_TRACE_STAGES;
 struct Cfg {
     int use_frag, max_iter, dp_iter;
     double r1, r2, early;
+    // dense-rescue mode (INDIALIGN_MODE_*) and ranker selection parameters
+    int mode = INDIALIGN_MODE_PLAIN, top_k = 8;
+    double margin = 0.02, audit = 0.02;
+    unsigned long long seed = 0;
 };
 
 // Host view of per-pair facts after k_prep / k_anchor.
@@ -163,6 +173,8 @@ struct Plan {
 class Runner {
   public:
     Runner(Ctx *c, const Cfg &cfg, int n) : c_(c), cfg_(cfg), n_(n) {}
+    long long windows() const { return L_win.total; }
+    bool use_mlp = false;
 
     int build_layouts(const std::vector<PairInfo> &info);
     int run_stages();
@@ -176,8 +188,8 @@ class Runner {
     // timing: events at stage boundaries and around every chain / bank launch
     bool timing = false;
     std::vector<std::pair<int, cudaEvent_t>> stage_ev;     // (boundary id, event)
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chain_ev, bank_ev;
-    long long launches_ = 0, chain_launches_ = 0, bank_launches_ = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chain_ev, bank_ev, rank_ev;
+    long long launches_ = 0, chain_launches_ = 0, bank_launches_ = 0, rank_launches_ = 0;
     cudaEvent_t new_event() {
         cudaEvent_t e = nullptr;
         if (!c_->ev_pool.empty()) {
@@ -198,14 +210,16 @@ class Runner {
         for (auto &x : stage_ev) c_->ev_pool.push_back(x.second);
         for (auto &x : chain_ev) { c_->ev_pool.push_back(x.first); c_->ev_pool.push_back(x.second); }
         for (auto &x : bank_ev) { c_->ev_pool.push_back(x.first); c_->ev_pool.push_back(x.second); }
-        stage_ev.clear(); chain_ev.clear(); bank_ev.clear();
+        for (auto &x : rank_ev) { c_->ev_pool.push_back(x.first); c_->ev_pool.push_back(x.second); }
+        stage_ev.clear(); chain_ev.clear(); bank_ev.clear(); rank_ev.clear();
     }
     int pmax = 0, nmax = 0, Nmax = 0;
 
   private:
     int bank(int kind, Layout &L, double *recs = nullptr, int set_iter = -1, double early = -1);
     int chain(int kind, Layout &L, int iters, double *recs = nullptr, double *recs2 = nullptr,
-              bool reduce = true);
+              bool reduce = true, const int *wcount = nullptr, const int *wlist = nullptr);
+    int dense_stage();
     int glue(int op, double thr = 0.0, const double *recs = nullptr, const int *idx = nullptr);
     int dp_full();
 
@@ -213,9 +227,9 @@ class Runner {
     Cfg cfg_;
     int n_;
     Layout L_pair, L_main, L_detss, L_detdp, L_gapless, L_thread, L_topk, L_localn, L_locald,
-        L_threadch, L_single, L_offdp, L_offslots;
+        L_threadch, L_single, L_offdp, L_offslots, L_win;
     long long max_items_ = 0, max_chain_recs_ = 0, n_thread_ = 0, n_off_ = 0;
-    int chain_grid_ = 0, chain_flags_ = 0;
+    int chain_grid_ = 0, chain_flags_ = 0, rank_grid_ = 1;
     size_t trace_words_ = 0;
 };
 
@@ -287,6 +301,11 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     perpair(L_localn, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 0); });
     perpair(L_locald, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 1); });
     perpair(L_single, [](const PairInfo &) { return 2LL; });
+    // dense-rescue windows of every pair (degenerate ones included, so that
+    // callers can lay out per-window outputs from the valid counts alone)
+    L_win.base.resize(n);
+    for (int p = 0; p < n; p++) L_win.base[p] = window_count(info[p].plen, info[p].nlen, 1);
+    finish_layout(L_win);
     // offset DP: start slots per (pair, offset)
     L_offdp.base.resize(n);
     L_offdp.aux.resize(n);
@@ -312,7 +331,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     // upload all layouts into one int and one long long arena
     size_t ni = 0, nl = 0;
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
-                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots}) {
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots, &L_win}) {
         ni += L->pair.size() + L->aux.size();
         nl += L->base.size();
     }
@@ -323,7 +342,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     hi.reserve(ni);
     hl.reserve(nl);
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
-                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots}) {
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots, &L_win}) {
         L->d_pair = L->pair.empty() ? nullptr : c_->lay_i.p + hi.size();
         hi.insert(hi.end(), L->pair.begin(), L->pair.end());
         L->d_aux = L->aux.empty() ? nullptr : c_->lay_i.p + hi.size();
@@ -380,6 +399,20 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     CK(c_->gal.ensure((chain_flags_ & 4) ? 1 : nw * (pmax < nmax ? pmax : nmax)));
     CK(c_->alP.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
     CK(c_->alQ.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
+    if (cfg_.mode != INDIALIGN_MODE_PLAIN) {
+        const size_t nw = (size_t)(L_win.total > 0 ? L_win.total : 1);
+        CK(c_->wscore.ensure(nw));
+        CK(c_->wcount.ensure(n > 0 ? n : 1));
+        CK(c_->wlist.ensure((size_t)(n > 0 ? n : 1) * kMaxTopK));
+        CK(c_->rstats.ensure(kRankStats));
+        if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
+            CK(c_->wfeat.ensure(nw * kFeatures));
+            CK(c_->wlabel.ensure(nw));
+        }
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rank_kernel_ptr(), 128, rank_smem_bytes()));
+        rank_grid_ = c_->sms * (per_sm > 0 ? per_sm : 1);
+    }
     return INDIALIGN_OK;
 }
 
@@ -425,7 +458,8 @@ int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early) 
     return INDIALIGN_OK;
 }
 
-int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, bool reduce) {
+int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, bool reduce,
+                  const int *wcount, const int *wlist) {
     if (L.ntasks <= 0) return INDIALIGN_OK;
     PlanCtx pc = {};
     pc.kind = kind;
@@ -441,6 +475,8 @@ int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, b
     pc.recs = recs;
     pc.recs2 = recs2;
     pc.iters = iters;
+    pc.wcount = wcount;
+    pc.wlist = wlist;
     launch_plan_chain(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -488,6 +524,65 @@ int Runner::dp_full() {
         if ((rc = glue(G_DP_STEP))) return rc;
     }
     return glue(G_DP_END);
+}
+
+// Dense local-fragment rescue (indialign_c/rescue.h:50-117 with dense =
+// true).  PLAIN refines every window.  LEARNED ranks the windows of the gated
+// pairs (features + MLP), refines the top-k of each pair (all windows on a
+// small margin or an audit draw) and reduces over the refined windows with
+// the same first-max rule.  COLLECT refines every window and records each
+// window's features and refined score.
+int Runner::dense_stage() {
+    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return chain(CH_LOCAL, L_locald, 1);
+    cudaStream_t st = c_->stream;
+    const bool learned = cfg_.mode == INDIALIGN_MODE_LEARNED;
+    launch_plan_rank(b, 1, c_->counts.p, st);
+    launch_scan(c_->counts.p, c_->begins.p, n_, c_->scan.p, c_->counter.p, st);
+    RankArgs ra;
+    ra.mlp = use_mlp ? c_->mlp.p : nullptr;
+    ra.wbase = L_win.d_base;
+    ra.score = c_->wscore.p;
+    ra.feat = learned ? nullptr : c_->wfeat.p;
+    ra.dense = 1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timing) {
+        e0 = new_event();
+        e1 = new_event();
+        cudaEventRecord(e0, st);
+    }
+    launch_rank(b, ra, c_->begins.p, c_->scan.p, c_->counter.p, rank_grid_, st);
+    if (timing) {
+        cudaEventRecord(e1, st);
+        rank_ev.push_back({e0, e1});
+    }
+    launches_ += 3;
+    rank_launches_++;
+    CK(cudaGetLastError());
+    if (!learned) {
+        if (int rc = chain(CH_LOCAL, L_locald, 1)) return rc;
+        launch_collect_labels(b, L_win.d_base, c_->chain_res.p, L_locald.d_base, 1, c_->wlabel.p, st);
+        launches_++;
+        CK(cudaGetLastError());
+        return INDIALIGN_OK;
+    }
+    SelectArgs sa;
+    sa.wbase = L_win.d_base;
+    sa.score = c_->wscore.p;
+    sa.wcount = c_->wcount.p;
+    sa.wlist = c_->wlist.p;
+    sa.top_k = cfg_.top_k;
+    sa.margin = (float)cfg_.margin;
+    sa.audit_rate = cfg_.audit;
+    sa.seed = cfg_.seed;
+    sa.dense = 1;
+    sa.stats = c_->rstats.p;
+    launch_select(b, sa, st);
+    launches_++;
+    if (int rc = chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, c_->wcount.p, c_->wlist.p)) return rc;
+    launch_audit(b, sa, c_->chain_res.p, L_locald.d_base, st);
+    launches_++;
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
 }
 
 #define RUN(x)                  \
@@ -539,7 +634,7 @@ int Runner::run_stages() {
     RUN(glue(G_STAGE_UPDATE));
     mark(4);
     RUN(glue(G_GATE, cfg_.r2));
-    RUN(chain(CH_LOCAL, L_locald, 1));
+    RUN(dense_stage());
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
@@ -771,8 +866,18 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaEventCreate(&e1));
         CK(cudaEventRecord(e0, st));
     }
+    const bool use_mlp = cfg.mode == INDIALIGN_MODE_LEARNED ||
+                         (cfg.mode == INDIALIGN_MODE_COLLECT && opts->ranker);
+    if (use_mlp) {
+        CK(c->blob.ensure(kBlobSize));
+        CK(c->mlp.ensure(1));
+        CK(cudaMemcpyAsync(c->blob.p, opts->ranker, kBlobSize * sizeof(float), cudaMemcpyHostToDevice, st));
+        launch_mlp_pack(c->blob.p, c->mlp.p, st);
+        CK(cudaGetLastError());
+    }
     Runner r(c, cfg, n);
     r.b = b;
+    r.use_mlp = use_mlp;
     r.Nmax = Nmax;
     r.timing = opts && (opts->stage_ms || opts->kernel_ms);
     r.stage_event(0);
@@ -792,6 +897,13 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     }
     int rc = r.build_layouts(info);
     if (rc) return rc;
+    const bool win_out = cfg.mode == INDIALIGN_MODE_COLLECT || (use_mlp && opts->win_score);
+    if (win_out && r.windows() > (opts->win_cap > 0 ? opts->win_cap : 0)) {
+        g_last_error = "per-window outputs: " + std::to_string(r.windows()) + " windows exceed win_cap";
+        return INDIALIGN_E_INPUT;
+    }
+    if (cfg.mode == INDIALIGN_MODE_LEARNED)
+        CK(cudaMemsetAsync(c->rstats.p, 0, kRankStats * sizeof(unsigned long long), st));
     rc = r.run_stages();
     if (rc) return rc;
     if (prof) CK(cudaEventRecord(e1, st));
@@ -816,6 +928,32 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     if (err) {
         g_last_error = "device error flag " + std::to_string(err);
         return INDIALIGN_E_DEVICE;
+    }
+    if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->rank_stats) {
+        unsigned long long h[kRankStats];
+        CK(cudaMemcpy(h, c->rstats.p, sizeof(h), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < kRankStats && k < INDIALIGN_RANK_STATS; k++) opts->rank_stats[k] = (long long)h[k];
+    }
+    if (use_mlp && opts->win_score && r.windows() > 0)
+        CK(cudaMemcpy(opts->win_score, c->wscore.p, (size_t)r.windows() * sizeof(float),
+                      cudaMemcpyDeviceToHost));
+    if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->win_select) {
+        std::vector<int> wc(n), wl((size_t)n * kMaxTopK);
+        CK(cudaMemcpy(wc.data(), c->wcount.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(wl.data(), c->wlist.p, wl.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < n; p++) {
+            int *o = opts->win_select + (size_t)p * (kMaxTopK + 1);
+            o[0] = wc[p];
+            for (int k = 0; k < kMaxTopK; k++) o[1 + k] = k < cfg.top_k ? wl[(size_t)p * kMaxTopK + k] : -1;
+        }
+    }
+    if (cfg.mode == INDIALIGN_MODE_COLLECT && r.windows() > 0) {
+        if (opts->win_feat)
+            CK(cudaMemcpy(opts->win_feat, c->wfeat.p, (size_t)r.windows() * kFeatures * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+        if (opts->win_label)
+            CK(cudaMemcpy(opts->win_label, c->wlabel.p, (size_t)r.windows() * sizeof(float),
+                          cudaMemcpyDeviceToHost));
     }
     if (opts && opts->stage_best && r.snap)
         CK(cudaMemcpy(opts->stage_best, r.snap, (size_t)n * kTrace * kRec * 8, cudaMemcpyDeviceToHost));
@@ -854,6 +992,10 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
             opts->kernel_ms[1] = bk;
             opts->kernel_ms[2] = (double)r.chain_ev.size();
             opts->kernel_ms[3] = (double)r.bank_ev.size();
+            double rk = 0;
+            for (auto &x : r.rank_ev) { CK(cudaEventElapsedTime(&ms, x.first, x.second)); rk += ms; }
+            opts->kernel_ms[4] = rk;
+            opts->kernel_ms[5] = (double)r.rank_ev.size();
         }
         r.recycle();
     }
@@ -868,7 +1010,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     return INDIALIGN_OK;
 }
 
-static Cfg make_cfg(const NativeConfig *cfg) {
+static Cfg make_cfg(const NativeConfig *cfg, const IndialignBatchOptions *opts) {
     Cfg c;
     c.use_frag = cfg->use_fragment_search != 0;
     c.max_iter = cfg->max_iter;
@@ -876,7 +1018,39 @@ static Cfg make_cfg(const NativeConfig *cfg) {
     c.r1 = cfg->rescue_score_1;
     c.r2 = cfg->rescue_score_2;
     c.early = cfg->early_term_score;
+    if (opts) {
+        c.mode = opts->mode;
+        c.top_k = opts->top_k > 0 ? opts->top_k : 8;
+        c.margin = opts->margin;
+        c.audit = opts->audit_rate;
+        c.seed = opts->seed;
+    }
     return c;
+}
+
+// Mode-specific option checks (before any device work).
+static int check_mode(const IndialignBatchOptions *opts) {
+    if (!opts || opts->mode == INDIALIGN_MODE_PLAIN) return INDIALIGN_OK;
+    if (opts->mode == INDIALIGN_MODE_LEARNED) {
+        if (!opts->ranker) {
+            g_last_error = "learned mode: ranker parameters missing";
+            return INDIALIGN_E_INPUT;
+        }
+        if (opts->top_k < 0 || opts->top_k > kMaxTopK) {
+            g_last_error = "learned mode: top_k must be in 1.." + std::to_string(kMaxTopK);
+            return INDIALIGN_E_INPUT;
+        }
+        return INDIALIGN_OK;
+    }
+    if (opts->mode == INDIALIGN_MODE_COLLECT) {
+        if (!opts->win_feat && !opts->win_label) {
+            g_last_error = "collect mode: no output buffers";
+            return INDIALIGN_E_INPUT;
+        }
+        return INDIALIGN_OK;
+    }
+    g_last_error = "unknown mode " + std::to_string(opts->mode);
+    return INDIALIGN_E_INPUT;
 }
 
 static int search_host(int n_pairs, const NativePairInput *inputs, const NativeConfig *cfg,
@@ -891,6 +1065,7 @@ static int search_host(int n_pairs, const NativePairInput *inputs, const NativeC
         g_last_error = "null argument";
         return INDIALIGN_E_INPUT;
     }
+    if (int rc = check_mode(opts)) return rc;
     Source src;
     std::vector<const NativePairInput *> &in = src.host;
     std::vector<int> ids;
@@ -916,7 +1091,7 @@ static int search_host(int n_pairs, const NativePairInput *inputs, const NativeC
     int rc = acquire(opts ? opts->device : -1, &c);
     if (rc) return rc;
     std::vector<double> res(13 * in.size());
-    rc = run_batch(c, make_cfg(cfg), src, res.data(), nullptr, opts);
+    rc = run_batch(c, make_cfg(cfg, opts), src, res.data(), nullptr, opts);
     release(c);
     if (rc) return rc;
     for (size_t k = 0; k < ids.size(); k++) {
@@ -1021,6 +1196,7 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
     if (n_pairs <= 0) return INDIALIGN_OK;
     if (!off || !d_pred || !d_nat || !d_v || !d_pv || !d_nv || !lnorm || !cfg || !d_out)
         return INDIALIGN_E_INPUT;
+    if (int rc = ia::check_mode(opts)) return rc;
     for (int p = 0; p < n_pairs; p++) {
         int L = off[p + 1] - off[p];
         if (L <= 0 || L > 65535) {
@@ -1040,9 +1216,13 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
     ia::Ctx *c = nullptr;
     int rc = ia::acquire(opts ? opts->device : -1, &c);
     if (rc) return rc;
-    rc = ia::run_batch(c, ia::make_cfg(cfg), src, nullptr, d_out, opts);
+    rc = ia::run_batch(c, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
     ia::release(c);
     return rc;
+}
+
+int indialign_window_count(int plen, int nlen, int dense) {
+    return plen < 0 || nlen < 0 ? 0 : ia::window_count(plen, nlen, dense ? 1 : 0);
 }
 
 const char *indialign_last_error(void) { return ia::g_last_error.c_str(); }

@@ -1,0 +1,169 @@
+"""Train the dense-rescue window ranker on the GPU.
+
+  python -m indialign_b200.train_ranker --pairs 200000 --heldout 20000 \
+      --out indialign_b200/ranker_weights.npy
+
+1. Synthetic training pairs (L ~ U(40, 300), sigma ~ U(0.5, 14) A, random
+   rigid transform, 5 % invalid residues per mask) and held-out pairs from a
+   different seed.
+2. Labels: the plain GPU search in COLLECT mode records every dense-rescue
+   window's 16 features and refined dp_refine score (pairs that reach the
+   dense rescue only).  Per pair at most --per-pair windows are kept: the
+   best --keep-top by label plus a random draw of the rest.
+3. Training: MSE + pairwise ranking loss, Adam (lr 1e-3, batch 8192 windows,
+   --epochs), every step on the library's BF16 tensor-core kernels.
+4. Held-out evaluation: how often the top-k predicted windows contain the
+   pair's best window score, and the margin-fallback rate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import sys
+import time
+
+import numpy as np
+
+
+def _gen(args):
+    from indialign_b200 import workloads as W
+    n, lo, hi, seed = args
+    return W.batch(n, lo, hi, seed=seed)
+
+
+def generate(n: int, lo: int, hi: int, seed: int, chunk: int = 256, procs: int = 8):
+    """n pairs in chunks generated by a spawn pool (started before any GPU
+    work); chunk c uses seed * 100003 + c."""
+    jobs = [(min(chunk, n - s), lo, hi, seed * 100003 + c) for c, s in enumerate(range(0, n, chunk))]
+    with mp.get_context("spawn").Pool(procs) as pool:
+        out = []
+        for part in pool.imap(_gen, jobs):
+            out.extend(part)
+    return out
+
+
+def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):
+    """Features / labels / group ids of the kept windows of every pair that
+    reached the dense rescue."""
+    import indialign_b200 as ia
+    rng = np.random.default_rng(seed)
+    F, Y, G = [], [], []
+    t0 = time.time()
+    for s in range(0, len(pairs), chunk):
+        part = pairs[s:s + chunk]
+        _, feat, label, woff = ia.collect_windows(part)
+        for i in range(len(part)):
+            lab = label[woff[i]:woff[i + 1]]
+            if lab.size == 0 or not np.isfinite(lab).all():
+                continue
+            idx = np.arange(lab.size)
+            if lab.size > per_pair:
+                top = np.argsort(-lab, kind="stable")[:keep_top]
+                rest = np.setdiff1d(idx, top)
+                idx = np.concatenate([top, rng.choice(rest, per_pair - keep_top, replace=False)])
+            F.append(feat[woff[i] + idx])
+            Y.append(lab[idx])
+            G.append(np.full(idx.size, s + i, np.int64))
+        log(f"collect {min(s + chunk, len(pairs))}/{len(pairs)} pairs, {sum(y.size for y in Y)} windows, "
+            f"{time.time() - t0:.0f} s")
+    if not F:
+        return np.zeros((0, 16), np.float32), np.zeros(0, np.float32), np.zeros(0, np.int64)
+    return np.concatenate(F), np.concatenate(Y).astype(np.float32), np.concatenate(G)
+
+
+def evaluate(blob, pairs, chunk: int, ks=(1, 4, 8, 16), margin: float = 0.02, log=print,
+             dump: str | None = None):
+    """Hit rates of the top-k predicted windows on held-out pairs."""
+    import torch
+
+    import indialign_b200 as ia
+    from indialign_b200 import ranker
+    tr = ranker.Trainer(blob, batch=16)
+    hits = {k: 0 for k in ks}
+    near = {k: 0 for k in ks}
+    fallback = 0
+    tot = 0
+    refined_frac = []
+    dumps = []
+    for s in range(0, len(pairs), chunk):
+        part = pairs[s:s + chunk]
+        _, feat, label, woff = ia.collect_windows(part)
+        if feat.shape[0] == 0:
+            continue
+        pred = tr.predict(torch.tensor(feat, device="cuda")).cpu().numpy()
+        for i in range(len(part)):
+            lab = label[woff[i]:woff[i + 1]]
+            if lab.size == 0 or not np.isfinite(lab).all():
+                continue
+            pr = pred[woff[i]:woff[i + 1]]
+            order = sorted(range(lab.size), key=lambda w: (-pr[w], w))
+            tot += 1
+            for k in ks:
+                sel = order[:k]
+                hits[k] += lab[sel].max() >= lab.max()
+                near[k] += lab[sel].max() >= lab.max() - 1e-3
+            k8 = order[:8]
+            fb = lab.size > 8 and pr[k8[0]] - pr[k8[-1]] < margin
+            fallback += fb
+            refined_frac.append(1.0 if (fb or lab.size <= 8) else 8.0 / lab.size)
+            if dump is not None and len(dumps) < 400:
+                dumps.append((lab.astype(np.float32), pr.astype(np.float32)))
+    res = {"pairs": tot, "fallback_rate": fallback / max(tot, 1),
+           "refined_fraction": float(np.mean(refined_frac)) if refined_frac else 0.0}
+    for k in ks:
+        res[f"hit@{k}"] = hits[k] / max(tot, 1)
+        res[f"near@{k}"] = near[k] / max(tot, 1)
+    if dump is not None and dumps:
+        np.savez_compressed(dump, **{f"lab{i}": d[0] for i, d in enumerate(dumps)},
+                            **{f"pred{i}": d[1] for i, d in enumerate(dumps)})
+    log(json.dumps(res))
+    return res
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--pairs", type=int, default=200000)
+    ap.add_argument("--heldout", type=int, default=20000)
+    ap.add_argument("--lo", type=int, default=40)
+    ap.add_argument("--hi", type=int, default=300)
+    ap.add_argument("--eval-hi", type=int, default=300)
+    ap.add_argument("--seed", type=int, default=31)
+    ap.add_argument("--eval-seed", type=int, default=32)
+    ap.add_argument("--per-pair", type=int, default=256)
+    ap.add_argument("--keep-top", type=int, default=32)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lam", type=float, default=1.0)
+    ap.add_argument("--chunk", type=int, default=1024)
+    ap.add_argument("--procs", type=int, default=8)
+    ap.add_argument("--out", default="ranker_weights.npy")
+    ap.add_argument("--dump", default=None, help="npz of held-out labels / predictions")
+    ap.add_argument("--data", default=None, help="npz cache of the collected training windows")
+    a = ap.parse_args(argv)
+
+    def log(msg):
+        print(f"[train_ranker] {msg}", file=sys.stderr, flush=True)
+
+    t0 = time.time()
+    train_pairs = generate(a.pairs, a.lo, a.hi, a.seed, procs=a.procs)
+    eval_pairs = generate(a.heldout, a.lo, a.eval_hi, a.eval_seed, procs=a.procs)
+    log(f"generated {len(train_pairs)} + {len(eval_pairs)} pairs in {time.time() - t0:.0f} s")
+    from indialign_b200 import ranker
+    F, Y, G = collect(train_pairs, a.chunk, a.per_pair, a.keep_top, a.seed, log)
+    log(f"training windows: {F.shape[0]} from {len(np.unique(G))} pairs")
+    if a.data:
+        np.savez_compressed(a.data, feat=F, label=Y, group=G)
+    t1 = time.time()
+    blob = ranker.train(F, Y, G, epochs=a.epochs, batch=a.batch, lr=a.lr, lam=a.lam, seed=a.seed, log=log)
+    log(f"trained in {time.time() - t1:.0f} s")
+    np.save(a.out, blob)
+    res = evaluate(blob, eval_pairs, a.chunk, log=log, dump=a.dump)
+    res.update({"train_windows": int(F.shape[0]), "train_pairs": int(len(np.unique(G))),
+                "epochs": a.epochs, "seconds": time.time() - t0})
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
