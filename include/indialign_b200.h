@@ -109,36 +109,46 @@ typedef struct {
                                 then ms and launches of the window-ranker kernel */
     double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
                                 best {score,R,t} after each search stage */
-    /* ---- learned window ranker (dense local-fragment rescue) ---- */
+    /* ---- learned candidate ranker of the rescue passes ----
+     * The local-fragment, threading-DP and dense local-fragment passes
+     * (rescue.h) each refine a list of candidate starts per pair (windows /
+     * offsets, INDIALIGN_CAND_*).  LEARNED mode scores them with the ranker
+     * and refines the top_k of each pair.  Per-candidate arrays below hold
+     * the three kinds back to back, each kind pair by pair, pair p with
+     * indialign_candidate_count(plen_p, nlen_p, kind) entries. */
     int mode;                /* INDIALIGN_MODE_PLAIN (0), _LEARNED or _COLLECT */
-    const float *ranker;     /* LEARNED: host FP32 parameter blob of
-                                INDIALIGN_RANKER_FLOATS floats */
-    int top_k;               /* LEARNED: windows refined per pair (1..32; 0: 8) */
-    double margin;           /* LEARNED: refine all windows when the predicted
+    const float *ranker;     /* LEARNED (or COLLECT with predictions): host FP32
+                                parameter blob of INDIALIGN_RANKER_FLOATS floats */
+    int top_k;               /* LEARNED: candidates refined per pair (1..32; 0: 8) */
+    double margin;           /* LEARNED: refine all candidates when the predicted
                                 top-1 minus top-k score is below this */
-    double audit_rate;       /* LEARNED: fraction of pairs refined on all windows */
+    double audit_rate;       /* LEARNED: fraction of pairs refined on all candidates */
     unsigned long long seed; /* LEARNED: audit draw */
-    long long *rank_stats;   /* LEARNED: optional [INDIALIGN_RANK_STATS] out: pairs
-                                ranked, margin fallbacks, audits, pruned pairs,
-                                windows, windows refined, audit misses, pairs with
-                                at most top_k windows */
-    float *win_feat;         /* COLLECT: out [windows][16] raw window features */
-    float *win_label;        /* COLLECT: out [windows] refined window score, NaN
-                                where the pair did not reach the dense rescue */
-    long long win_cap;       /* COLLECT, or LEARNED with win_score: capacity of the
-                                per-window outputs in windows */
-    float *win_score;        /* optional out [windows] (LEARNED, or COLLECT with a
-                                ranker): predicted score of every window */
-    int *win_select;         /* optional out [n_pairs][33] (LEARNED): windows refined
-                                (-1: all, margin fallback or at most top_k windows;
-                                -2: all, audit), then the top_k windows ascending */
+    long long *rank_stats;   /* LEARNED: optional [INDIALIGN_RANK_STATS] out, per kind
+                                8 counts: pairs ranked, margin fallbacks, audits,
+                                pruned pairs, candidates, candidates refined, audit
+                                misses, pairs with at most top_k candidates */
+    float *win_feat;         /* COLLECT: out [candidates][16] raw features */
+    float *win_label;        /* COLLECT: out [candidates] refined score, NaN where
+                                the pair's pass did not run */
+    long long win_cap;       /* COLLECT, or with win_score: capacity of the
+                                per-candidate outputs */
+    float *win_score;        /* optional out [candidates] (LEARNED, or COLLECT with a
+                                ranker): predicted score of every candidate */
+    int *win_select;         /* optional out [3][n_pairs][33] (LEARNED): per kind and
+                                pair the candidates refined (-1: all, margin
+                                fallback, pass not run or at most top_k; -2: all,
+                                audit), then the top_k candidates ascending */
 } IndialignBatchOptions;
 
-#define INDIALIGN_MODE_PLAIN 0   /* the reference's search, every window refined */
-#define INDIALIGN_MODE_LEARNED 1 /* dense rescue refines the ranker's top-k windows */
-#define INDIALIGN_MODE_COLLECT 2 /* plain search + per-window features and labels */
+#define INDIALIGN_MODE_PLAIN 0   /* the reference's search, every candidate refined */
+#define INDIALIGN_MODE_LEARNED 1 /* rescue passes refine the ranker's top-k candidates */
+#define INDIALIGN_MODE_COLLECT 2 /* plain search + per-candidate features and labels */
+#define INDIALIGN_CAND_LOCAL 0   /* local-fragment windows (rescue.h:50-117) */
+#define INDIALIGN_CAND_THREAD 1  /* threading-DP offsets (rescue.h:121-190) */
+#define INDIALIGN_CAND_DENSE 2   /* dense local-fragment windows */
 #define INDIALIGN_RANKER_FLOATS 18849
-#define INDIALIGN_RANK_STATS 8
+#define INDIALIGN_RANK_STATS 24
 
 /* Stages recorded in stage_best, in search order: seed bank, SS seeds,
  * gapless threading, local fragment DP, threading DP, dense local fragment
@@ -191,11 +201,9 @@ int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_
 int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap, int *d_ap,
                                int *d_an, int *d_na, void *stream);
 
-/* Dense-rescue windows of a pair with plen / nlen valid pred / native
- * residues (rescue.h:12-46 schedule).  In COLLECT mode pair p's windows sit
- * at the running sum of this count over the pairs before it, every pair
- * counted, in the batch's order. */
-int indialign_window_count(int plen, int nlen, int dense);
+/* Candidates of kind INDIALIGN_CAND_* of a pair with plen / nlen valid pred /
+ * native residues (the schedules of rescue.h:12-46 and :136-142). */
+int indialign_candidate_count(int plen, int nlen, int kind);
 
 /* ---- ranker training on caller-owned device buffers (no counterpart in the
  * reference, which has no learned component).  The parameter blob is FP32:

@@ -26,8 +26,11 @@ COUNTERS = 12
 TRACE_STAGES = 10
 KERNEL_MS = 6
 MODE_PLAIN, MODE_LEARNED, MODE_COLLECT = 0, 1, 2
+CAND_LOCAL, CAND_THREAD, CAND_DENSE = 0, 1, 2
+CAND_KINDS = 3
+CAND_NAMES = ("local", "threading", "dense")
 RANKER_FLOATS = 18849
-RANK_STATS = 8
+RANK_STATS = 24
 RANK_STAT_NAMES = ("gated", "fallback", "audit", "pruned", "windows", "refined",
                    "audit_miss", "small")
 FEATURES = 16
@@ -94,8 +97,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.indialign_tmscore_search_device.restype = ctypes.c_int
     lib.indialign_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.indialign_fp64_peak.restype = ctypes.c_int
-    lib.indialign_window_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
-    lib.indialign_window_count.restype = ctypes.c_int
+    lib.indialign_candidate_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.indialign_candidate_count.restype = ctypes.c_int
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
     for name, args, res in (
             ("indialign_mlp_packed_bytes", [], sz),
@@ -140,14 +143,32 @@ def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, marg
     opts.audit_rate = float(audit_rate)
     opts.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     if rank_stats is not None:
-        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS
+        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [3][8]
         opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
     return opts
 
 
-def window_count(plen: int, nlen: int, dense: bool = True) -> int:
-    """Dense-rescue windows of a pair with plen / nlen valid residues."""
-    return int(load().indialign_window_count(int(plen), int(nlen), int(dense)))
+def candidate_count(plen: int, nlen: int, kind: int = 2) -> int:
+    """Candidates of kind CAND_* of a pair with plen / nlen valid residues."""
+    return int(load().indialign_candidate_count(int(plen), int(nlen), int(kind)))
+
+
+def candidate_offsets(pairs: Sequence) -> np.ndarray:
+    """[3, n+1] start of each pair's candidates per kind in the per-candidate
+    arrays (kinds back to back): pair p of kind k at off[k, p]:off[k, p+1]."""
+    n = len(pairs)
+    cnt = np.zeros((CAND_KINDS, n), np.int64)
+    for i, p in enumerate(pairs):
+        pl, nl = int(np.count_nonzero(p.pred_valid)), int(np.count_nonzero(p.native_valid))
+        for k in range(CAND_KINDS):
+            cnt[k, i] = candidate_count(pl, nl, k)
+    off = np.zeros((CAND_KINDS, n + 1), np.int64)
+    base = 0
+    for k in range(CAND_KINDS):
+        off[k, 0] = base
+        off[k, 1:] = base + np.cumsum(cnt[k])
+        base = int(off[k, -1])
+    return off
 
 
 def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = False,
@@ -194,19 +215,18 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     return abi.results_to_numpy(res, pk.n)
 
 
-def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None):
-    """Plain search in COLLECT mode: every dense-rescue window's 16 raw
-    features and refined score.  Returns (results, feat[W,16] f32, label[W]
-    f32 (NaN where the pair did not reach the dense rescue), woff[n+1]) with
-    pair p's windows at woff[p]:woff[p+1]."""
+def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None,
+                    ranker: np.ndarray | None = None):
+    """Plain search in COLLECT mode: every rescue candidate's 16 raw features
+    and refined score.  Returns (results, feat[C,16] f32, label[C] f32 (NaN
+    where the pair's pass did not run), off[3, n+1]) with pair p's candidates
+    of kind k at off[k, p]:off[k, p+1].  With `ranker`, also the predicted
+    scores: (results, feat, label, off, score)."""
     lib = load()
     cfg = cfg or default_config()
     pk = abi.PackedInputs(pairs)
-    counts = [window_count(int(np.count_nonzero(p.pred_valid)), int(np.count_nonzero(p.native_valid)))
-              for p in pairs]
-    woff = np.zeros(len(pairs) + 1, np.int64)
-    woff[1:] = np.cumsum(counts)
-    W = int(woff[-1])
+    woff = candidate_offsets(pairs)
+    W = int(woff[-1, -1])
     feat = np.zeros((max(W, 1), FEATURES), np.float32)
     label = np.zeros(max(W, 1), np.float32)
     res = (NativePairResult * max(1, pk.n))()
@@ -216,10 +236,17 @@ def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None):
     opts.win_feat = _fptr(feat)
     opts.win_label = _fptr(label)
     opts.win_cap = W
+    score = None
+    if ranker is not None:
+        assert ranker.dtype == np.float32 and ranker.size == RANKER_FLOATS
+        opts.ranker = _fptr(ranker)
+        score = np.zeros(max(W, 1), np.float32)
+        opts.win_score = _fptr(score)
     rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
     if rc != 0:
         raise IndialignError(f"indialign_tmscore_search_batch_ex(collect) rc={rc}: {last_error()}")
-    return abi.results_to_numpy(res, pk.n), feat[:W], label[:W], woff
+    out = (abi.results_to_numpy(res, pk.n), feat[:W], label[:W], woff)
+    return out + (score[:W],) if ranker is not None else out
 
 
 def fp64_peak_tflops(device: int = 0) -> float:

@@ -1,22 +1,25 @@
-// Learned window ranker for the dense local-fragment rescue
-// (evaluate_local_fragment_dp, indialign_c/rescue.h:50-117).
+// Learned candidate ranker for the rescue passes of the search: the
+// local-fragment windows (evaluate_local_fragment_dp,
+// indialign_c/rescue.h:50-117, normal and dense) and the threading-DP offsets
+// (evaluate_threading_dp, rescue.h:121-190).
 //
-// The dense rescue refines every (fragment length, pred start, native start)
-// window of a weak pair with a 2-iteration dp_refine chain, thousands of NW
-// chains per pair.  The ranker predicts each window's refined dp_refine score
-// from 16 cheap features, and the search refines only the top-k windows of a
-// pair, falling back to all windows when the predicted top-1 / top-k margin
-// is small and on a random audit of pairs.
+// Each rescue pass refines every candidate start of a weak pair (a window
+// (fragment length, pred start, native start), or an offset's overlap) with
+// NW dp_refine chains, hundreds to thousands per pair.  The ranker predicts
+// each candidate's refined score from 16 cheap features, and the search
+// refines only the top-k candidates of a pair, falling back to all of them
+// when the predicted top-1 / top-k margin is small and on a random audit of
+// pairs.
 //
-//   k_rank    persistent CTAs over 64-window chunks: per window the warp
-//             computes the features (window Kabsch + diagonal TM sums, FP64),
-//             then the 16 -> 128 -> 128 -> 1 GELU MLP runs on BF16 tensor
-//             cores (mma.sync m16n8k16, FP32 accumulation) over the warp's
-//             16-window tile, with the weights resident in shared memory.
-//   k_select  warp per pair: top-k by (predicted score desc, window asc),
-//             margin fallback, audit draw, window list in ascending order (so
-//             the chain reduction keeps the reference's first-max rule).
-//   k_audit   audited pairs: did the top-k windows contain the best score?
+//   k_rank    persistent CTAs over 64-candidate chunks: per candidate the
+//             warp computes the features (segment Kabsch + diagonal TM sums,
+//             FP64), then the 16 -> 128 -> 128 -> 1 GELU MLP runs on BF16
+//             tensor cores (mma.sync m16n8k16, FP32 accumulation) over the
+//             warp's 16-candidate tile, with the weights in shared memory.
+//   k_select  warp per pair: top-k by (predicted score desc, index asc),
+//             margin fallback, audit draw, list in ascending order (so the
+//             stage's reduction keeps the reference's first-max rule).
+//   k_audit   audited pairs: did the top-k contain the best refined score?
 //   training  forward with saved activations, MSE + pairwise ranking loss,
 //             backward through BF16 tensor-core GEMMs (split-K, fixed-order
 //             sums), Adam on FP32 master weights.
@@ -28,6 +31,8 @@
 #include "sched.cuh"
 
 namespace ia {
+
+static_assert(kMaxTopK == 32, "selection lists are one entry per lane");
 
 namespace {
 
@@ -168,21 +173,21 @@ IA_DEV void mlp_tile(const MlpSmem &S, const float *xt, float &y_g, float &y_g8,
     y_g8 = y8 + S.b3;
 }
 
-// The 16 features of window w of a pair (raw, before standardisation),
+// The 16 features of candidate w of a pair (raw, before standardisation),
 // computed by the whole warp; every lane returns all 16.
-//   0 fragment length / ml        1 pred start / (plen-1)   2 native start / (nlen-1)
-//   3 start shift / ml            4 window RMSD / 10        5 TM along the window's
+//   0 segment length / ml         1 pred start / (plen-1)   2 native start / (nlen-1)
+//   3 start shift / ml            4 segment RMSD / 10       5 TM along the segment's
 //   diagonal under its Kabsch     6, 7 fraction of that diagonal within d0, 2 d0
-//   8 window-local TM             9, 10 stem fraction of the pred / native window
-//   11 log(ml) / 7                12 running best score     13 d0 / 10
+//   8 segment-local TM            9, 10 stem fraction of the pred / native segment
+//   11 log(ml) / 7                12 running best score     13 candidate kind / 2
 //   14 min(RMSD / d0, 10) / 10    15 TM along the same-index diagonal
 // (ml = min(plen, nlen); indices are compact valid-residue positions.)
 IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, const PairInfo &I,
-                            double best, int dense, int w, float (&f)[kFeatures]) {
+                            double best, int kind, int w, float (&f)[kFeatures]) {
     const int lane = threadIdx.x & 31;
     const int plen = I.plen, nlen = I.nlen, ml = plen < nlen ? plen : nlen;
     int flen, ps, ns;
-    window_at(plen, nlen, dense, w, flen, ps, ns);
+    cand_at(kind, plen, nlen, w, flen, ps, ns);
     double R[9], t[3];
     warp_kabsch_window(x, ps, ns, flen, R, t);
     const double d0sq = I.d0 * I.d0, inv = 1.0 / d0sq;
@@ -231,7 +236,7 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
     f[10] = (float)(sn / flen);
     f[11] = (float)(log(mld) / 7.0);
     f[12] = (float)best;
-    f[13] = (float)(I.d0 / 10.0);
+    f[13] = 0.5f * (float)kind;
     f[14] = (float)(fmin(rmsd / I.d0, 10.0) / 10.0);
     f[15] = (float)(tm0 / I.lnorm);
 }
@@ -239,11 +244,11 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
 }  // namespace
 
 // ---- ranking: features + MLP over the windows of gated pairs ------------------
-__global__ void k_plan_rank(DevBatch b, int dense, int *counts) {
+__global__ void k_plan_rank(DevBatch b, int kind, int *counts) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= b.n) return;
     const PairInfo &I = b.info[p];
-    const int W = window_count(I.plen, I.nlen, dense);
+    const int W = cand_count(kind, I.plen, I.nlen);
     const bool on = I.status == 0 && b.state[p].flag && W > 0;
     counts[p] = on ? (W + kRankChunk - 1) / kRankChunk : 0;
 }
@@ -276,7 +281,7 @@ __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int 
         const int c = s_chunk, p = s_pair;
         if (c >= total || p < 0) break;
         const PairInfo &I = b.info[p];
-        const int W = window_count(I.plen, I.nlen, a.dense);
+        const int W = cand_count(a.kind, I.plen, I.nlen);
         const int w0 = (c - chunk_begin[p]) * kRankChunk + warp * 16;
         if (w0 < W) {
             const Pts x = {b.predc + 3 * (size_t)I.off, b.natc + 3 * (size_t)I.off};
@@ -289,7 +294,7 @@ __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int 
                 float mine = 0.f;
                 if (w < W) {
                     float f[kFeatures];
-                    window_features(x, Lp, Ln, I, best, a.dense, w, f);
+                    window_features(x, Lp, Ln, I, best, a.kind, w, f);
 #pragma unroll
                     for (int j = 0; j < kFeatures; j++)
                         if (lane == j) mine = f[j];
@@ -331,7 +336,7 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
         list[lane] = -1;
         return;
     }
-    const int W = window_count(I.plen, I.nlen, a.dense);
+    const int W = cand_count(a.kind, I.plen, I.nlen);
     const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
     if (lane == 0) {
         atomicAdd(a.stats + RS_GATED, 1ull);
@@ -399,25 +404,33 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
     }
 }
 
-// A window's refined score: the dp_refine result over its two gap chains
-// (later chain only if strictly better, indialign_c/align.h:131-145).
-IA_DEV double window_score(const double *res, int w) {
+// A candidate's refined score: the dp_refine result over its two gap chains
+// (later chain only if strictly better, indialign_c/align.h:131-145); for a
+// threading offset the better of that and its detailed search
+// (rescue.h:163-165).  -inf for an offset that was not searched.
+IA_DEV double cand_score(const CandRes &r, int p, int w) {
+    const double *res = r.chain_res + (size_t)r.chain_base[p] * kRec;
     const double s0 = res[(size_t)(2 * w) * kRec], s1 = res[(size_t)(2 * w + 1) * kRec];
-    return s1 > s0 ? s1 : s0;
+    double s = s1 > s0 ? s1 : s0;
+    if (r.det) {
+        const double dt = r.det[((size_t)r.det_base[p] + w) * kRec];
+        if (dt <= -1e299) return -INFINITY;
+        if (!(s > dt)) s = dt;
+    }
+    return s;
 }
 
-// Audited pairs ran every window: count those whose selected windows miss the
-// best window score.
-__global__ void k_audit(DevBatch b, SelectArgs a, const double *chain_res, const long long *chain_base) {
+// Audited pairs ran every candidate: count those whose selected candidates
+// miss the best refined score.
+__global__ void k_audit(DevBatch b, SelectArgs a, CandRes r) {
     const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (p >= b.n || a.wcount[p] != -2) return;
     const PairInfo &I = b.info[p];
-    const int W = window_count(I.plen, I.nlen, a.dense);
-    const double *res = chain_res + (size_t)chain_base[p] * kRec;
+    const int W = cand_count(a.kind, I.plen, I.nlen);
     const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
     double full = -INFINITY, sel = -INFINITY;
-    for (int w = lane; w < W; w += 32) full = fmax(full, window_score(res, w));
-    for (int r = lane; r < k; r += 32) sel = fmax(sel, window_score(res, a.wlist[(size_t)p * kMaxTopK + r]));
+    for (int w = lane; w < W; w += 32) full = fmax(full, cand_score(r, p, w));
+    for (int j = lane; j < k; j += 32) sel = fmax(sel, cand_score(r, p, a.wlist[(size_t)p * kMaxTopK + j]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         full = fmax(full, __shfl_xor_sync(kAllLanes, full, o));
@@ -426,17 +439,18 @@ __global__ void k_audit(DevBatch b, SelectArgs a, const double *chain_res, const
     if (lane == 0 && sel < full) atomicAdd(a.stats + RS_AUDIT_MISS, 1ull);
 }
 
-// Training labels: every window's refined score for pairs that ran the stage
-// on all windows, NaN elsewhere.
-__global__ void k_collect_labels(DevBatch b, const long long *wbase, const double *chain_res,
-                                 const long long *chain_base, int dense, float *label) {
+// Training labels: every candidate's refined score for pairs that ran the
+// stage on all candidates, NaN elsewhere.
+__global__ void k_collect_labels(DevBatch b, const long long *wbase, CandRes r, int kind, float *label) {
     const int p = blockIdx.x;
     const PairInfo &I = b.info[p];
-    const int W = window_count(I.plen, I.nlen, dense);
+    const int W = cand_count(kind, I.plen, I.nlen);
     const bool on = I.status == 0 && b.state[p].flag;
-    const double *res = chain_res + (size_t)(on ? chain_base[p] : 0) * kRec;
     float *out = label + wbase[p];
-    for (int w = threadIdx.x; w < W; w += blockDim.x) out[w] = on ? (float)window_score(res, w) : NAN;
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
+        const double s = on ? cand_score(r, p, w) : -INFINITY;
+        out[w] = s > -1e299 ? (float)s : NAN;
+    }
 }
 
 // ---- training ---------------------------------------------------------------------
@@ -697,8 +711,8 @@ cudaError_t rank_set_attributes() {
     return e;
 }
 
-void launch_plan_rank(const DevBatch &b, int dense, int *counts, cudaStream_t st) {
-    if (b.n > 0) k_plan_rank<<<(b.n + 127) / 128, 128, 0, st>>>(b, dense, counts);
+void launch_plan_rank(const DevBatch &b, int kind, int *counts, cudaStream_t st) {
+    if (b.n > 0) k_plan_rank<<<(b.n + 127) / 128, 128, 0, st>>>(b, kind, counts);
 }
 
 void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
@@ -710,14 +724,13 @@ void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st) {
     if (b.n > 0) k_select<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a);
 }
 
-void launch_audit(const DevBatch &b, const SelectArgs &a, const double *chain_res,
-                  const long long *chain_base, cudaStream_t st) {
-    if (b.n > 0) k_audit<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a, chain_res, chain_base);
+void launch_audit(const DevBatch &b, const SelectArgs &a, const CandRes &r, cudaStream_t st) {
+    if (b.n > 0) k_audit<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a, r);
 }
 
-void launch_collect_labels(const DevBatch &b, const long long *wbase, const double *chain_res,
-                           const long long *chain_base, int dense, float *label, cudaStream_t st) {
-    if (b.n > 0) k_collect_labels<<<b.n, 256, 0, st>>>(b, wbase, chain_res, chain_base, dense, label);
+void launch_collect_labels(const DevBatch &b, const long long *wbase, const CandRes &r, int kind,
+                           float *label, cudaStream_t st) {
+    if (b.n > 0) k_collect_labels<<<b.n, 256, 0, st>>>(b, wbase, r, kind, label);
 }
 
 void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st) {

@@ -118,6 +118,12 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
         T.early_term = 1.0;
         T.out = c.recs + (size_t)s * kRec;
         on = on && S.flag && ov >= 3;
+        if (on && c.wcount && c.wcount[p] >= 0) {  // ranked: the selected offsets only
+            const int *l = c.wlist + (size_t)p * kMaxTopK;
+            bool sel = false;
+            for (int j = 0; j < c.wcount[p]; j++) sel = sel || l[j] == aux;
+            on = sel;
+        }
         if (!on) T.out[0] = kNegInf;
         break;
     }

@@ -120,10 +120,10 @@ struct MlpSave {
 
 struct RankArgs {
     const MlpPacked *mlp;      // nullptr: features only
-    const long long *wbase;    // [n] first window of a pair in the window arrays
-    float *score;              // [windows] predicted refined score
-    float *feat;               // optional [windows][16] raw features
-    int dense;
+    const long long *wbase;    // [n] first candidate of a pair in the candidate arrays
+    float *score;              // [candidates] predicted refined score
+    float *feat;               // optional [candidates][16] raw features
+    int kind;                  // CandKind
 };
 
 struct SelectArgs {
@@ -135,21 +135,30 @@ struct SelectArgs {
     float margin;
     double audit_rate;
     unsigned long long seed;
-    int dense;
-    unsigned long long *stats;  // [kRankStats]
+    int kind;                   // CandKind
+    unsigned long long *stats;  // [kRankStats] of this kind
 };
 
-void launch_plan_rank(const DevBatch &b, int dense, int *counts, cudaStream_t st);
+// Where the refined results of a stage's candidates live: two gap-chain
+// records per candidate (chain_res + chain_base[p]), and for threading
+// offsets also the detailed-search record (det + det_base[p] + offset).
+struct CandRes {
+    const double *chain_res;
+    const long long *chain_base;
+    const double *det;
+    const int *det_base;
+};
+
+void launch_plan_rank(const DevBatch &b, int kind, int *counts, cudaStream_t st);
 void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
                  int *counter, int grid, cudaStream_t st);
 cudaError_t rank_set_attributes();
 size_t rank_smem_bytes();
 const void *rank_kernel_ptr();
 void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st);
-void launch_audit(const DevBatch &b, const SelectArgs &a, const double *chain_res,
-                  const long long *chain_base, cudaStream_t st);
-void launch_collect_labels(const DevBatch &b, const long long *wbase, const double *chain_res,
-                           const long long *chain_base, int dense, float *label, cudaStream_t st);
+void launch_audit(const DevBatch &b, const SelectArgs &a, const CandRes &r, cudaStream_t st);
+void launch_collect_labels(const DevBatch &b, const long long *wbase, const CandRes &r, int kind,
+                           float *label, cudaStream_t st);
 void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st);
 void launch_mlp_forward(const MlpPacked *mlp, const float *x, int n, float *y, const MlpSave *save,
                         cudaStream_t st);

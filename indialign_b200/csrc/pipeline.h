@@ -168,7 +168,13 @@ struct ScanOut {
 constexpr int kFeatures = 16;
 constexpr int kHidden = 128;
 constexpr int kMaxTopK = 32;
-constexpr int kRankChunk = 64;  // windows per CTA chunk of the ranker (4 warps x 16)
+constexpr int kRankChunk = 64;  // candidates per CTA chunk of the ranker (4 warps x 16)
+
+// Candidate starts the ranker scores, in search order: local-fragment
+// windows (rescue.h:50-117, dense = false), threading-DP offsets
+// (rescue.h:121-190), dense local-fragment windows.  Each is a segment
+// (flen, ps, ns) of compact pred / native positions.
+enum CandKind { CAND_LOCAL = 0, CAND_THREAD = 1, CAND_DENSE = 2, kCandKinds = 3 };
 
 // FP32 parameter blob: mean[16] std[16] W1[16][128] b1[128] W2[128][128]
 // b2[128] w3[128] b3, weights stored [in][out] row-major.  mean/std
@@ -183,7 +189,7 @@ constexpr int kBlobW3 = kBlobB2 + kHidden;
 constexpr int kBlobB3 = kBlobW3 + kHidden;
 constexpr int kBlobSize = kBlobB3 + 1;
 
-// Ranker statistics of one batch (IndialignBatchOptions.rank_stats).
+// Ranker statistics of one batch per candidate kind (IndialignBatchOptions.rank_stats).
 enum RankStat {
     RS_GATED = 0,      // pairs that reached the ranked stage
     RS_FALLBACK,       // ... refined on all windows: predicted margin below threshold

@@ -179,6 +179,19 @@ IA_HD void thread_at(int plen, int nlen, int o, int &ps, int &ns, int &ov) {
     ov = imin_(plen - ps, nlen - ns);
 }
 
+// Ranked candidates of a kind (pipeline.h CandKind): windows, or threading
+// offsets as the segment of their overlap.
+IA_HD int cand_count(int kind, int plen, int nlen) {
+    return kind == 1 ? thread_count(plen, nlen) : window_count(plen, nlen, kind == 2 ? 1 : 0);
+}
+IA_HD void cand_at(int kind, int plen, int nlen, int i, int &flen, int &ps, int &ns) {
+    if (kind == 1) {
+        thread_at(plen, nlen, i, ps, ns, flen);
+    } else {
+        window_at(plen, nlen, kind == 2 ? 1 : 0, i, flen, ps, ns);
+    }
+}
+
 // Offset-DP starts: k = -N/2 .. N/2 step max(1, N/10), k != 0
 // (indialign_c/indialign.cpp:234-236).
 IA_HD int offdp_count(int N) { return offsets_count(-N / 2, N / 2, imax_(1, N / 10)); }

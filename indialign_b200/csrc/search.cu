@@ -92,7 +92,7 @@ struct Ctx {
     // learned window ranker
     DBuf<float> blob, wscore, wfeat, wlabel;
     DBuf<MlpPacked> mlp;
-    DBuf<int> wcount, wlist;
+    DBuf<int> wcount, wlist, wsel;
     DBuf<unsigned long long> rstats;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<double> h_pred, h_nat, h_lnorm;
@@ -173,7 +173,9 @@ struct Plan {
 class Runner {
   public:
     Runner(Ctx *c, const Cfg &cfg, int n) : c_(c), cfg_(cfg), n_(n) {}
-    long long windows() const { return L_win.total; }
+    long long windows() const { return koff_[kCandKinds]; }
+    int *sel_out = nullptr;  // device copy of each pass's selection (LEARNED, win_select)
+    long long cand_offset(int kind) const { return koff_[kind]; }
     bool use_mlp = false;
 
     int build_layouts(const std::vector<PairInfo> &info);
@@ -216,10 +218,15 @@ class Runner {
     int pmax = 0, nmax = 0, Nmax = 0;
 
   private:
-    int bank(int kind, Layout &L, double *recs = nullptr, int set_iter = -1, double early = -1);
+    int bank(int kind, Layout &L, double *recs = nullptr, int set_iter = -1, double early = -1,
+             const int *wcount = nullptr, const int *wlist = nullptr);
     int chain(int kind, Layout &L, int iters, double *recs = nullptr, double *recs2 = nullptr,
               bool reduce = true, const int *wcount = nullptr, const int *wlist = nullptr);
-    int dense_stage();
+    int rank_stage(int kind);
+    SelectArgs select_args(int kind);
+    int after_stage(int kind, const CandRes &r);
+    const int *sel_count() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wcount.p : nullptr; }
+    const int *sel_list() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wlist.p : nullptr; }
     int glue(int op, double thr = 0.0, const double *recs = nullptr, const int *idx = nullptr);
     int dp_full();
 
@@ -227,7 +234,8 @@ class Runner {
     Cfg cfg_;
     int n_;
     Layout L_pair, L_main, L_detss, L_detdp, L_gapless, L_thread, L_topk, L_localn, L_locald,
-        L_threadch, L_single, L_offdp, L_offslots, L_win;
+        L_threadch, L_single, L_offdp, L_offslots, L_cand[kCandKinds];
+    long long koff_[kCandKinds + 1] = {0, 0, 0, 0};
     long long max_items_ = 0, max_chain_recs_ = 0, n_thread_ = 0, n_off_ = 0;
     int chain_grid_ = 0, chain_flags_ = 0, rank_grid_ = 1;
     size_t trace_words_ = 0;
@@ -301,11 +309,15 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     perpair(L_localn, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 0); });
     perpair(L_locald, [](const PairInfo &I) { return 2LL * window_count(I.plen, I.nlen, 1); });
     perpair(L_single, [](const PairInfo &) { return 2LL; });
-    // dense-rescue windows of every pair (degenerate ones included, so that
-    // callers can lay out per-window outputs from the valid counts alone)
-    L_win.base.resize(n);
-    for (int p = 0; p < n; p++) L_win.base[p] = window_count(info[p].plen, info[p].nlen, 1);
-    finish_layout(L_win);
+    // ranked candidates of every pair (degenerate ones included, so that
+    // callers can lay out per-candidate outputs from the valid counts alone),
+    // kinds back to back
+    for (int k = 0; k < kCandKinds; k++) {
+        L_cand[k].base.resize(n);
+        for (int p = 0; p < n; p++) L_cand[k].base[p] = cand_count(k, info[p].plen, info[p].nlen);
+        finish_layout(L_cand[k]);
+        koff_[k + 1] = koff_[k] + L_cand[k].total;
+    }
     // offset DP: start slots per (pair, offset)
     L_offdp.base.resize(n);
     L_offdp.aux.resize(n);
@@ -331,7 +343,8 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     // upload all layouts into one int and one long long arena
     size_t ni = 0, nl = 0;
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
-                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots, &L_win}) {
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
+                      &L_cand[0], &L_cand[1], &L_cand[2]}) {
         ni += L->pair.size() + L->aux.size();
         nl += L->base.size();
     }
@@ -342,7 +355,8 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     hi.reserve(ni);
     hl.reserve(nl);
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
-                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots, &L_win}) {
+                      &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
+                      &L_cand[0], &L_cand[1], &L_cand[2]}) {
         L->d_pair = L->pair.empty() ? nullptr : c_->lay_i.p + hi.size();
         hi.insert(hi.end(), L->pair.begin(), L->pair.end());
         L->d_aux = L->aux.empty() ? nullptr : c_->lay_i.p + hi.size();
@@ -400,11 +414,11 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     CK(c_->alP.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
     CK(c_->alQ.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
     if (cfg_.mode != INDIALIGN_MODE_PLAIN) {
-        const size_t nw = (size_t)(L_win.total > 0 ? L_win.total : 1);
+        const size_t nw = (size_t)(windows() > 0 ? windows() : 1);
         CK(c_->wscore.ensure(nw));
-        CK(c_->wcount.ensure(n > 0 ? n : 1));
-        CK(c_->wlist.ensure((size_t)(n > 0 ? n : 1) * kMaxTopK));
-        CK(c_->rstats.ensure(kRankStats));
+        CK(c_->wcount.ensure((size_t)kCandKinds * (n > 0 ? n : 1)));
+        CK(c_->wlist.ensure((size_t)kCandKinds * (n > 0 ? n : 1) * kMaxTopK));
+        CK(c_->rstats.ensure(kCandKinds * kRankStats));
         if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
             CK(c_->wfeat.ensure(nw * kFeatures));
             CK(c_->wlabel.ensure(nw));
@@ -416,7 +430,8 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     return INDIALIGN_OK;
 }
 
-int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early) {
+int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early, const int *wcount,
+                 const int *wlist) {
     if (L.ntasks <= 0) return INDIALIGN_OK;
     PlanCtx pc = {};
     pc.kind = kind;
@@ -431,6 +446,8 @@ int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early) 
     pc.recs = recs;
     pc.max_iter = set_iter >= 0 ? set_iter : cfg_.max_iter;
     pc.early_term = early >= 0 ? early : cfg_.early;
+    pc.wcount = wcount;
+    pc.wlist = wlist;
     launch_plan_bank(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
     launches_ += 4;
@@ -526,24 +543,22 @@ int Runner::dp_full() {
     return glue(G_DP_END);
 }
 
-// Dense local-fragment rescue (indialign_c/rescue.h:50-117 with dense =
-// true).  PLAIN refines every window.  LEARNED ranks the windows of the gated
-// pairs (features + MLP), refines the top-k of each pair (all windows on a
-// small margin or an audit draw) and reduces over the refined windows with
-// the same first-max rule.  COLLECT refines every window and records each
-// window's features and refined score.
-int Runner::dense_stage() {
-    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return chain(CH_LOCAL, L_locald, 1);
+// Candidate ranking of one rescue pass (pipeline.h CandKind) for the pairs
+// its gate let in.  PLAIN: nothing.  LEARNED: features + MLP scores, then the
+// per-pair selection the pass's plan reads (wcount / wlist).  COLLECT: the
+// features of every candidate.
+int Runner::rank_stage(int kind) {
+    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return INDIALIGN_OK;
     cudaStream_t st = c_->stream;
     const bool learned = cfg_.mode == INDIALIGN_MODE_LEARNED;
-    launch_plan_rank(b, 1, c_->counts.p, st);
+    launch_plan_rank(b, kind, c_->counts.p, st);
     launch_scan(c_->counts.p, c_->begins.p, n_, c_->scan.p, c_->counter.p, st);
     RankArgs ra;
     ra.mlp = use_mlp ? c_->mlp.p : nullptr;
-    ra.wbase = L_win.d_base;
-    ra.score = c_->wscore.p;
-    ra.feat = learned ? nullptr : c_->wfeat.p;
-    ra.dense = 1;
+    ra.wbase = L_cand[kind].d_base;
+    ra.score = c_->wscore.p + koff_[kind];
+    ra.feat = learned ? nullptr : c_->wfeat.p + koff_[kind] * kFeatures;
+    ra.kind = kind;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (timing) {
         e0 = new_event();
@@ -557,29 +572,46 @@ int Runner::dense_stage() {
     }
     launches_ += 3;
     rank_launches_++;
-    CK(cudaGetLastError());
-    if (!learned) {
-        if (int rc = chain(CH_LOCAL, L_locald, 1)) return rc;
-        launch_collect_labels(b, L_win.d_base, c_->chain_res.p, L_locald.d_base, 1, c_->wlabel.p, st);
+    if (learned) {
+        launch_select(b, select_args(kind), st);
         launches_++;
-        CK(cudaGetLastError());
-        return INDIALIGN_OK;
     }
+    CK(cudaGetLastError());
+    return INDIALIGN_OK;
+}
+
+SelectArgs Runner::select_args(int kind) {
     SelectArgs sa;
-    sa.wbase = L_win.d_base;
-    sa.score = c_->wscore.p;
+    sa.wbase = L_cand[kind].d_base;
+    sa.score = c_->wscore.p + koff_[kind];
     sa.wcount = c_->wcount.p;
     sa.wlist = c_->wlist.p;
     sa.top_k = cfg_.top_k;
     sa.margin = (float)cfg_.margin;
     sa.audit_rate = cfg_.audit;
     sa.seed = cfg_.seed;
-    sa.dense = 1;
-    sa.stats = c_->rstats.p;
-    launch_select(b, sa, st);
-    launches_++;
-    if (int rc = chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, c_->wcount.p, c_->wlist.p)) return rc;
-    launch_audit(b, sa, c_->chain_res.p, L_locald.d_base, st);
+    sa.kind = kind;
+    sa.stats = c_->rstats.p + (size_t)kind * kRankStats;
+    return sa;
+}
+
+// After a ranked pass: LEARNED checks the audited pairs, COLLECT records
+// every candidate's refined score.
+int Runner::after_stage(int kind, const CandRes &r) {
+    cudaStream_t st = c_->stream;
+    if (cfg_.mode == INDIALIGN_MODE_LEARNED) {
+        launch_audit(b, select_args(kind), r, st);
+        if (sel_out) {  // keep this pass's selection for the caller
+            CK(cudaMemcpyAsync(sel_out + (size_t)kind * n_, c_->wcount.p, n_ * sizeof(int),
+                               cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(sel_out + (size_t)kCandKinds * n_ + (size_t)kind * n_ * kMaxTopK, c_->wlist.p,
+                               (size_t)n_ * kMaxTopK * sizeof(int), cudaMemcpyDeviceToDevice, st));
+        }
+    } else if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
+        launch_collect_labels(b, L_cand[kind].d_base, r, kind, c_->wlabel.p + koff_[kind], st);
+    } else {
+        return INDIALIGN_OK;
+    }
     launches_++;
     CK(cudaGetLastError());
     return INDIALIGN_OK;
@@ -621,20 +653,26 @@ int Runner::run_stages() {
     mark(2);
     // 3. rescue ladder (indialign.cpp:125-152)
     RUN(glue(G_GATE, cfg_.r1));
-    RUN(chain(CH_LOCAL, L_localn, 0));
+    RUN(rank_stage(CAND_LOCAL));
+    RUN(chain(CH_LOCAL, L_localn, 0, nullptr, nullptr, true, sel_count(), sel_list()));
+    RUN(after_stage(CAND_LOCAL, CandRes{c_->chain_res.p, L_localn.d_base, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
     mark(3);
     RUN(glue(G_GATE, cfg_.r1));
-    RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p));
+    RUN(rank_stage(CAND_THREAD));
+    RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p, -1, -1, sel_count(), sel_list()));
     RUN(chain(CH_THREAD, L_threadch, 1, c_->thread_rec.p));
+    RUN(after_stage(CAND_THREAD, CandRes{c_->chain_res.p, L_threadch.d_base, c_->thread_rec.p, L_threadch.d_aux}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
     mark(4);
     RUN(glue(G_GATE, cfg_.r2));
-    RUN(dense_stage());
+    RUN(rank_stage(CAND_DENSE));
+    RUN(chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, sel_count(), sel_list()));
+    RUN(after_stage(CAND_DENSE, CandRes{c_->chain_res.p, L_locald.d_base, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
@@ -902,8 +940,13 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         g_last_error = "per-window outputs: " + std::to_string(r.windows()) + " windows exceed win_cap";
         return INDIALIGN_E_INPUT;
     }
-    if (cfg.mode == INDIALIGN_MODE_LEARNED)
-        CK(cudaMemsetAsync(c->rstats.p, 0, kRankStats * sizeof(unsigned long long), st));
+    if (cfg.mode == INDIALIGN_MODE_LEARNED) {
+        CK(cudaMemsetAsync(c->rstats.p, 0, kCandKinds * kRankStats * sizeof(unsigned long long), st));
+        if (opts->win_select) {
+            CK(c->wsel.ensure((size_t)kCandKinds * n * (1 + kMaxTopK)));
+            r.sel_out = c->wsel.p;
+        }
+    }
     rc = r.run_stages();
     if (rc) return rc;
     if (prof) CK(cudaEventRecord(e1, st));
@@ -930,22 +973,25 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         return INDIALIGN_E_DEVICE;
     }
     if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->rank_stats) {
-        unsigned long long h[kRankStats];
+        unsigned long long h[kCandKinds * kRankStats];
         CK(cudaMemcpy(h, c->rstats.p, sizeof(h), cudaMemcpyDeviceToHost));
-        for (int k = 0; k < kRankStats && k < INDIALIGN_RANK_STATS; k++) opts->rank_stats[k] = (long long)h[k];
+        for (int k = 0; k < kCandKinds * kRankStats && k < INDIALIGN_RANK_STATS; k++)
+            opts->rank_stats[k] = (long long)h[k];
     }
     if (use_mlp && opts->win_score && r.windows() > 0)
         CK(cudaMemcpy(opts->win_score, c->wscore.p, (size_t)r.windows() * sizeof(float),
                       cudaMemcpyDeviceToHost));
     if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->win_select) {
-        std::vector<int> wc(n), wl((size_t)n * kMaxTopK);
-        CK(cudaMemcpy(wc.data(), c->wcount.p, n * sizeof(int), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(wl.data(), c->wlist.p, wl.size() * sizeof(int), cudaMemcpyDeviceToHost));
-        for (int p = 0; p < n; p++) {
-            int *o = opts->win_select + (size_t)p * (kMaxTopK + 1);
-            o[0] = wc[p];
-            for (int k = 0; k < kMaxTopK; k++) o[1 + k] = k < cfg.top_k ? wl[(size_t)p * kMaxTopK + k] : -1;
-        }
+        std::vector<int> h((size_t)kCandKinds * n * (1 + kMaxTopK));
+        CK(cudaMemcpy(h.data(), c->wsel.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        const int *wc = h.data(), *wl = h.data() + (size_t)kCandKinds * n;
+        for (int k = 0; k < kCandKinds; k++)
+            for (int p = 0; p < n; p++) {
+                int *o = opts->win_select + ((size_t)k * n + p) * (kMaxTopK + 1);
+                const int *l = wl + ((size_t)k * n + p) * kMaxTopK;
+                o[0] = wc[(size_t)k * n + p];
+                for (int j = 0; j < kMaxTopK; j++) o[1 + j] = j < cfg.top_k ? l[j] : -1;
+            }
     }
     if (cfg.mode == INDIALIGN_MODE_COLLECT && r.windows() > 0) {
         if (opts->win_feat)
@@ -1221,8 +1267,9 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
     return rc;
 }
 
-int indialign_window_count(int plen, int nlen, int dense) {
-    return plen < 0 || nlen < 0 ? 0 : ia::window_count(plen, nlen, dense ? 1 : 0);
+int indialign_candidate_count(int plen, int nlen, int kind) {
+    if (plen < 0 || nlen < 0 || kind < 0 || kind >= ia::kCandKinds) return 0;
+    return ia::cand_count(kind, plen, nlen);
 }
 
 const char *indialign_last_error(void) { return ia::g_last_error.c_str(); }

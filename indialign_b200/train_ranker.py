@@ -1,4 +1,4 @@
-"""Train the dense-rescue window ranker on the GPU.
+"""Train the rescue-candidate ranker on the GPU.
 
   python -m indialign_b200.train_ranker --pairs 200000 --heldout 20000 \
       --out indialign_b200/ranker_weights.npy
@@ -6,10 +6,11 @@
 1. Synthetic training pairs (L ~ U(40, 300), sigma ~ U(0.5, 14) A, random
    rigid transform, 5 % invalid residues per mask) and held-out pairs from a
    different seed.
-2. Labels: the plain GPU search in COLLECT mode records every dense-rescue
-   window's 16 features and refined dp_refine score (pairs that reach the
-   dense rescue only).  Per pair at most --per-pair windows are kept: the
-   best --keep-top by label plus a random draw of the rest.
+2. Labels: the plain GPU search in COLLECT mode records every rescue
+   candidate's 16 features and refined score (local-fragment windows,
+   threading-DP offsets, dense windows; pairs whose pass ran only).  Per pair
+   and kind at most --per-pair candidates are kept: the best --keep-top by
+   label plus a random draw of the rest.
 3. Training: MSE + pairwise ranking loss, Adam (lr 1e-3, batch 8192 windows,
    --epochs), every step on the library's BF16 tensor-core kernels.
 4. Held-out evaluation: how often the top-k predicted windows contain the
@@ -44,27 +45,28 @@ def generate(n: int, lo: int, hi: int, seed: int, chunk: int = 256, procs: int =
 
 
 def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):
-    """Features / labels / group ids of the kept windows of every pair that
-    reached the dense rescue."""
+    """Features / labels / group ids of the kept candidates of every pair
+    and kind whose pass ran; a group is one (pair, kind)."""
     import indialign_b200 as ia
     rng = np.random.default_rng(seed)
     F, Y, G = [], [], []
     t0 = time.time()
     for s in range(0, len(pairs), chunk):
         part = pairs[s:s + chunk]
-        _, feat, label, woff = ia.collect_windows(part)
-        for i in range(len(part)):
-            lab = label[woff[i]:woff[i + 1]]
-            if lab.size == 0 or not np.isfinite(lab).all():
-                continue
-            idx = np.arange(lab.size)
-            if lab.size > per_pair:
-                top = np.argsort(-lab, kind="stable")[:keep_top]
-                rest = np.setdiff1d(idx, top)
-                idx = np.concatenate([top, rng.choice(rest, per_pair - keep_top, replace=False)])
-            F.append(feat[woff[i] + idx])
-            Y.append(lab[idx])
-            G.append(np.full(idx.size, s + i, np.int64))
+        _, feat, label, off = ia.collect_windows(part)
+        for kind in range(ia.CAND_KINDS):
+            for i in range(len(part)):
+                lab = label[off[kind, i]:off[kind, i + 1]]
+                idx = np.flatnonzero(np.isfinite(lab))
+                if idx.size < 2:
+                    continue
+                if idx.size > per_pair:
+                    top = idx[np.argsort(-lab[idx], kind="stable")[:keep_top]]
+                    rest = np.setdiff1d(idx, top)
+                    idx = np.concatenate([top, rng.choice(rest, per_pair - keep_top, replace=False)])
+                F.append(feat[off[kind, i] + idx])
+                Y.append(lab[idx])
+                G.append(np.full(idx.size, 3 * (s + i) + kind, np.int64))
         log(f"collect {min(s + chunk, len(pairs))}/{len(pairs)} pairs, {sum(y.size for y in Y)} windows, "
             f"{time.time() - t0:.0f} s")
     if not F:
@@ -74,49 +76,46 @@ def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):
 
 def evaluate(blob, pairs, chunk: int, ks=(1, 4, 8, 16), margin: float = 0.02, log=print,
              dump: str | None = None):
-    """Hit rates of the top-k predicted windows on held-out pairs."""
-    import torch
-
+    """Per candidate kind: how often the top-k predicted candidates contain
+    the best refined score (exactly, and within 1e-3), and the fraction of
+    candidates an 8-candidate selection with the margin fallback refines."""
     import indialign_b200 as ia
-    from indialign_b200 import ranker
-    tr = ranker.Trainer(blob, batch=16)
-    hits = {k: 0 for k in ks}
-    near = {k: 0 for k in ks}
-    fallback = 0
-    tot = 0
-    refined_frac = []
+    res = {}
+    acc = [dict(tot=0, fb=0, frac=[], hits={k: 0 for k in ks}, near={k: 0 for k in ks}) for _ in range(3)]
     dumps = []
     for s in range(0, len(pairs), chunk):
         part = pairs[s:s + chunk]
-        _, feat, label, woff = ia.collect_windows(part)
-        if feat.shape[0] == 0:
-            continue
-        pred = tr.predict(torch.tensor(feat, device="cuda")).cpu().numpy()
-        for i in range(len(part)):
-            lab = label[woff[i]:woff[i + 1]]
-            if lab.size == 0 or not np.isfinite(lab).all():
-                continue
-            pr = pred[woff[i]:woff[i + 1]]
-            order = sorted(range(lab.size), key=lambda w: (-pr[w], w))
-            tot += 1
-            for k in ks:
-                sel = order[:k]
-                hits[k] += lab[sel].max() >= lab.max()
-                near[k] += lab[sel].max() >= lab.max() - 1e-3
-            k8 = order[:8]
-            fb = lab.size > 8 and pr[k8[0]] - pr[k8[-1]] < margin
-            fallback += fb
-            refined_frac.append(1.0 if (fb or lab.size <= 8) else 8.0 / lab.size)
-            if dump is not None and len(dumps) < 400:
-                dumps.append((lab.astype(np.float32), pr.astype(np.float32)))
-    res = {"pairs": tot, "fallback_rate": fallback / max(tot, 1),
-           "refined_fraction": float(np.mean(refined_frac)) if refined_frac else 0.0}
-    for k in ks:
-        res[f"hit@{k}"] = hits[k] / max(tot, 1)
-        res[f"near@{k}"] = near[k] / max(tot, 1)
+        _, feat, label, off, pred = ia.collect_windows(part, ranker=blob)
+        for kind in range(ia.CAND_KINDS):
+            a = acc[kind]
+            for i in range(len(part)):
+                lab = label[off[kind, i]:off[kind, i + 1]]
+                if lab.size == 0 or np.isnan(lab).all():
+                    continue
+                lab = np.where(np.isfinite(lab), lab, -np.inf)
+                pr = pred[off[kind, i]:off[kind, i + 1]]
+                order = np.lexsort((np.arange(lab.size), -pr))
+                a["tot"] += 1
+                for k in ks:
+                    top = lab[order[:k]].max()
+                    a["hits"][k] += top >= lab.max()
+                    a["near"][k] += top >= lab.max() - 1e-3
+                fb = lab.size > 8 and pr[order[0]] - pr[order[7]] < margin
+                a["fb"] += fb
+                a["frac"].append(1.0 if (fb or lab.size <= 8) else 8.0 / lab.size)
+                if dump is not None and len(dumps) < 600:
+                    dumps.append((kind, lab.astype(np.float32), pr.astype(np.float32)))
+    for kind, a in enumerate(acc):
+        r = {"pairs": a["tot"], "fallback_rate": a["fb"] / max(a["tot"], 1),
+             "refined_fraction": float(np.mean(a["frac"])) if a["frac"] else 0.0}
+        for k in ks:
+            r[f"hit@{k}"] = a["hits"][k] / max(a["tot"], 1)
+            r[f"near@{k}"] = a["near"][k] / max(a["tot"], 1)
+        res[ia.CAND_NAMES[kind]] = r
     if dump is not None and dumps:
-        np.savez_compressed(dump, **{f"lab{i}": d[0] for i, d in enumerate(dumps)},
-                            **{f"pred{i}": d[1] for i, d in enumerate(dumps)})
+        np.savez_compressed(dump, kind=np.array([d[0] for d in dumps]),
+                            **{f"lab{i}": d[1] for i, d in enumerate(dumps)},
+                            **{f"pred{i}": d[2] for i, d in enumerate(dumps)})
     log(json.dumps(res))
     return res
 
@@ -136,7 +135,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--lam", type=float, default=1.0)
-    ap.add_argument("--chunk", type=int, default=1024)
+    ap.add_argument("--chunk", type=int, default=512)
     ap.add_argument("--procs", type=int, default=8)
     ap.add_argument("--out", default="ranker_weights.npy")
     ap.add_argument("--dump", default=None, help="npz of held-out labels / predictions")
@@ -152,7 +151,7 @@ def main(argv=None):
     log(f"generated {len(train_pairs)} + {len(eval_pairs)} pairs in {time.time() - t0:.0f} s")
     from indialign_b200 import ranker
     F, Y, G = collect(train_pairs, a.chunk, a.per_pair, a.keep_top, a.seed, log)
-    log(f"training windows: {F.shape[0]} from {len(np.unique(G))} pairs")
+    log(f"training candidates: {F.shape[0]} from {len(np.unique(G))} (pair, kind) groups")
     if a.data:
         np.savez_compressed(a.data, feat=F, label=Y, group=G)
     t1 = time.time()
@@ -160,7 +159,7 @@ def main(argv=None):
     log(f"trained in {time.time() - t1:.0f} s")
     np.save(a.out, blob)
     res = evaluate(blob, eval_pairs, a.chunk, log=log, dump=a.dump)
-    res.update({"train_windows": int(F.shape[0]), "train_pairs": int(len(np.unique(G))),
+    res.update({"train_candidates": int(F.shape[0]), "train_groups": int(len(np.unique(G))),
                 "epochs": a.epochs, "seconds": time.time() - t0})
     print(json.dumps(res))
 

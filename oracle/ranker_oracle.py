@@ -1,10 +1,11 @@
 """CPU restatement of the learned window ranker, used ONLY as test
 infrastructure (tests/ import it as the checker; the product never does).
 
-* windows(): the dense local-fragment window schedule
-  (indialign_c/rescue.h:12-46 local_frag_lengths / local_jump, :65-78 loop
-  order), the candidates the ranker scores.
-* window_features(): the 16 features of a window, FP64.
+* candidates(): the candidate starts the ranker scores: local-fragment
+  windows, normal and dense (indialign_c/rescue.h:12-46 local_frag_lengths /
+  local_jump, :65-78 loop order), and threading-DP offsets (rescue.h:136-153)
+  as the segment of their overlap.
+* window_features(): the 16 features of a candidate segment, FP64.
 * mlp_forward() / mlp_backward() / loss(): the 16 -> 128 -> 128 -> 1 GELU
   MLP with the device's rounding points emulated (BF16 round-to-nearest-even
   of the standardised inputs, the hidden activations and the backward's
@@ -63,6 +64,23 @@ def local_jump(length: int, dense: bool) -> int:
     return max(1, min(j, max(1, length // 3)))
 
 
+def thread_offsets(plen: int, nlen: int) -> list[tuple[int, int, int]]:
+    """(overlap, ps, ns) of the threading-DP offsets (rescue.h:136-153)."""
+    if min(plen, nlen) < 3:
+        return []
+    step = max(1, min(plen, nlen) // 50)
+    out = []
+    for off in range(-(nlen - 3), plen - 2, step):
+        ps, ns = max(off, 0), max(-off, 0)
+        out.append((min(plen - ps, nlen - ns), ps, ns))
+    return out
+
+
+def candidates(plen: int, nlen: int, kind: int) -> list[tuple[int, int, int]]:
+    """Kind 0 local windows, 1 threading offsets, 2 dense windows."""
+    return thread_offsets(plen, nlen) if kind == 1 else windows(plen, nlen, kind == 2)
+
+
 def windows(plen: int, nlen: int, dense: bool = True) -> list[tuple[int, int, int]]:
     """(flen, ps, ns) in the reference's work order."""
     jp, jn = local_jump(plen, dense), local_jump(nlen, dense)
@@ -89,9 +107,10 @@ def kabsch(P: np.ndarray, Q: np.ndarray):
 
 
 def window_features(Pc: np.ndarray, Qc: np.ndarray, ssp: str, ssn: str, d0: float, lnorm: float,
-                    best: float, win: tuple[int, int, int]) -> np.ndarray:
-    """Features of window (flen, ps, ns) on compact coordinates Pc [plen,3],
-    Qc [nlen,3] and compact SS labels ('L' loop, '<' / '>' stem)."""
+                    best: float, win: tuple[int, int, int], kind: int) -> np.ndarray:
+    """Features of candidate segment (flen, ps, ns) of kind `kind` on compact
+    coordinates Pc [plen,3], Qc [nlen,3] and compact SS labels ('L' loop,
+    '<' / '>' stem)."""
     flen, ps, ns = win
     plen, nlen = Pc.shape[0], Qc.shape[0]
     ml = min(plen, nlen)
@@ -111,7 +130,7 @@ def window_features(Pc: np.ndarray, Qc: np.ndarray, ssp: str, ssn: str, d0: floa
     stem_n = sum(c != "L" for c in ssn[ns:ns + flen]) / flen
     f = [flen / ml, ps / max(1, plen - 1), ns / max(1, nlen - 1), s / ml, rmsd / 10.0,
          (1.0 / (1.0 + dd / d0sq)).sum() / lnorm, (dd < d0sq).sum() / ml, (dd < 4 * d0sq).sum() / ml,
-         (1.0 / (1.0 + dw / d0sq)).sum() / flen, stem_p, stem_n, np.log(ml) / 7.0, best, d0 / 10.0,
+         (1.0 / (1.0 + dw / d0sq)).sum() / flen, stem_p, stem_n, np.log(ml) / 7.0, best, 0.5 * kind,
          min(rmsd / d0, 10.0) / 10.0, (1.0 / (1.0 + d00 / d0sq)).sum() / lnorm]
     return np.array(f, np.float64)
 

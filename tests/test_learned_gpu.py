@@ -143,10 +143,14 @@ def test_training_reduces_loss(torch_cuda):
     t = (0.3 + 0.2 * np.tanh(x[:, 0] - 0.5 * x[:, 5]) + 0.05 * x[:, 3]).astype(np.float32)
     tr = ranker.Trainer(ranker.init_blob(x.mean(0), x.std(0), 0), batch=n, lr=3e-3, lam=0.2)
     X, T = torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda")
-    first = float(tr.step(X, T).item())
+
+    def mse():
+        return float(((tr.forward(X) - T) ** 2).mean().item())
+
+    first = mse()
     for _ in range(300):
-        last = tr.step(X, T)
-    assert float(last.item()) < 0.1 * first
+        tr.step(X, T)
+    assert mse() < 0.05 * first
 
 
 def _compact(p, ss):
@@ -170,30 +174,33 @@ def _d0(L):
     return max(d0, 0.3)
 
 
-def test_window_features_match_oracle(oracle):
+def test_candidate_features_match_oracle(oracle):
+    """COLLECT-mode features of all three candidate kinds vs the FP64
+    restatement (running best entering each pass from the stage trace)."""
     oracle.ora_assign_ss.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]
     pairs = [p for p in W.batch(24, 40, 160, seed=11, sigma_lo=6.0, sigma_hi=14.0)]
     stage_best = np.zeros(len(pairs) * ia.TRACE_STAGES * 13)
     ia.search(pairs, stage_best=stage_best)
-    (_, _, _), feat, label, woff = ia.collect_windows(pairs)
+    (_, _, _), feat, label, off = ia.collect_windows(pairs)
     sb = stage_best.reshape(len(pairs), ia.TRACE_STAGES, 13)
-    checked = 0
+    checked = np.zeros(3, int)
     rng = np.random.default_rng(0)
     for i, p in enumerate(pairs):
-        lab = label[woff[i]:woff[i + 1]]
-        if lab.size == 0 or np.isnan(lab).all():
-            continue
         ss = (_ss(oracle, p.pred, p.pred_valid), _ss(oracle, p.native, p.native_valid))
         Pc, Qc, ssp, ssn = _compact(p, ss)
-        ws = ro.windows(Pc.shape[0], Qc.shape[0], True)
-        assert len(ws) == lab.size
-        best = sb[i, 4, 0]  # running best entering the dense rescue
-        for w in rng.choice(len(ws), size=min(20, len(ws)), replace=False):
-            fo = ro.window_features(Pc, Qc, ssp, ssn, _d0(p.lnorm), p.lnorm, best, ws[w])
-            fg = feat[woff[i] + w].astype(np.float64)
-            np.testing.assert_allclose(fg, fo, rtol=1e-5, atol=2e-6, err_msg=f"pair {i} window {w}")
-            checked += 1
-    assert checked >= 40
+        for kind in range(ia.CAND_KINDS):
+            lab = label[off[kind, i]:off[kind, i + 1]]
+            if lab.size == 0 or np.isnan(lab).all():
+                continue
+            cs = ro.candidates(Pc.shape[0], Qc.shape[0], kind)
+            assert len(cs) == lab.size
+            best = sb[i, (2, 3, 4)[kind], 0]  # running best entering the pass
+            for w in rng.choice(len(cs), size=min(10, len(cs)), replace=False):
+                fo = ro.window_features(Pc, Qc, ssp, ssn, _d0(p.lnorm), p.lnorm, best, cs[w], kind)
+                fg = feat[off[kind, i] + w].astype(np.float64)
+                np.testing.assert_allclose(fg, fo, rtol=1e-5, atol=2e-6, err_msg=f"pair {i} kind {kind} cand {w}")
+                checked[kind] += 1
+    assert (checked >= 20).all(), checked
 
 
 def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True):
@@ -204,36 +211,40 @@ def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True
     opts.device = -1
     stats = np.zeros(ia.RANK_STATS, np.int64)
     ia.learned_options(opts, blob, k, margin, audit, seed, stats)
-    counts = [ia.window_count(int(p.pred_valid.sum()), int(p.native_valid.sum())) for p in pairs]
-    woff = np.r_[0, np.cumsum(counts)].astype(np.int64)
-    score = np.zeros(max(1, int(woff[-1])), np.float32)
-    sel = np.zeros((len(pairs), 33), np.int32)
+    off = ia.candidate_offsets(pairs)
+    C = int(off[-1, -1])
+    score = np.zeros(max(1, C), np.float32)
+    sel = np.zeros((ia.CAND_KINDS, len(pairs), 33), np.int32)
     if outputs:
         opts.win_score = score.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        opts.win_cap = int(woff[-1])
+        opts.win_cap = C
         opts.win_select = sel.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     cfg = ia.default_config()
     rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
     assert rc == 0, ia.last_error()
-    return abi.results_to_numpy(res, pk.n), stats, score, sel, woff
+    return abi.results_to_numpy(res, pk.n), stats.reshape(ia.CAND_KINDS, 8), score, sel, off
 
 
 def test_selection_matches_oracle():
     pairs = W.batch(48, 40, 200, seed=12, sigma_lo=5.0, sigma_hi=14.0)
     blob = _blob(7)
     for k, margin, audit, seed in ((8, 0.0, 0.0, 0), (8, 0.02, 0.3, 99), (3, 1e9, 0.0, 1), (32, 0.0, 0.0, 2)):
-        (sc, _, _), stats, score, sel, woff = _learned_run(pairs, blob, k, margin, audit, seed)
-        gated = 0
-        for i in range(len(pairs)):
-            s = score[woff[i]:woff[i + 1]]
-            if sel[i, 0] == -1 and (sel[i, 1:] == -1).all():
-                continue  # pair not gated into the dense rescue (or <= k windows)
-            gated += 1
-            c, lst = ro.select(s, k, margin, audit, seed, i)
-            assert sel[i, 0] == c, (i, k, margin, audit)
-            assert list(sel[i, 1:1 + k]) == lst
-        assert stats[0] >= gated > 0
-        assert stats[1] + stats[2] + stats[3] + stats[7] == stats[0]
+        (sc, _, _), stats, score, sel, off = _learned_run(pairs, blob, k, margin, audit, seed)
+        for kind in range(ia.CAND_KINDS):
+            gated = 0
+            for i in range(len(pairs)):
+                s = score[off[kind, i]:off[kind, i + 1]]
+                row = sel[kind, i]
+                if row[0] == -1 and (row[1:] == -1).all():
+                    continue  # pass not run for this pair (or at most k candidates)
+                gated += 1
+                c, lst = ro.select(s, k, margin, audit, seed, i)
+                assert row[0] == c, (kind, i, k, margin, audit)
+                assert list(row[1:1 + k]) == lst
+            st = stats[kind]
+            assert st[0] >= gated
+            assert st[1] + st[2] + st[3] + st[7] == st[0]
+        assert stats[:, 0].sum() > 0
 
 
 @pytest.fixture(scope="module")
@@ -246,37 +257,40 @@ def shipped():
 def test_learned_vs_plain_delta_tm(shipped):
     """The trained ranker on held-out pairs (L 40-1000, sigma 0.5-14, 5 %
     invalid): final TM-scores vs the plain search within the bars, and the
-    dense rescue refines a small fraction of the windows."""
+    rescue passes refine a small fraction of their candidates."""
     pairs = W.batch(256, 40, 1000, seed=4242)
     plain, _, _ = ia.search(pairs)
     (lsc, _, _), stats, _, _, _ = _learned_run(pairs, shipped, outputs=False)
     d = lsc - plain
     assert d.mean() >= -1e-4, d.mean()
     assert d.min() >= -1e-3, d.min()
-    assert stats[0] > 0
-    assert stats[5] < 0.5 * stats[4], stats  # windows refined vs windows
+    assert stats[:, 0].sum() > 0
+    assert stats[:, 5].sum() < 0.5 * stats[:, 4].sum(), stats  # refined vs candidates
 
 
 def test_trained_ranker_beats_untrained(shipped):
     """What the trained network gains: with the margin fallback and the
-    audit off, its top-8 windows contain the best window score far more
+    audit off, its top-8 candidates contain the best refined score far more
     often than an untrained network's."""
     pairs = W.batch(96, 40, 300, seed=777, sigma_lo=6.0, sigma_hi=14.0)
-    (_, _, _), _, label, woff = ia.collect_windows(pairs)
+    (_, _, _), _, label, off = ia.collect_windows(pairs)
 
     def hit_rate(blob):
         (_, _, _), _, score, sel, _ = _learned_run(pairs, blob, 8, -1.0, 0.0, 0)
         hits = tot = 0
-        for i in range(len(pairs)):
-            if sel[i, 0] != 8:
-                continue
-            lab = label[woff[i]:woff[i + 1]]
-            tot += 1
-            hits += lab[sel[i, 1:9]].max() >= lab.max()
+        for kind in range(ia.CAND_KINDS):
+            for i in range(len(pairs)):
+                if sel[kind, i, 0] != 8:
+                    continue
+                lab = label[off[kind, i]:off[kind, i + 1]]
+                if np.isnan(lab).any():
+                    continue
+                tot += 1
+                hits += lab[sel[kind, i, 1:9]].max() >= lab.max() - 1e-3
         return hits / max(tot, 1), tot
 
     h_tr, n_tr = hit_rate(shipped)
     untrained = ranker.init_blob(shipped[:16], shipped[16:32], 123)
     h_un, _ = hit_rate(untrained)
     assert n_tr >= 10
-    assert h_tr >= h_un + 0.2, (h_tr, h_un)
+    assert h_tr >= h_un + 0.15, (h_tr, h_un)

@@ -87,12 +87,13 @@ def test_bf16_rounding_is_nearest_even():
 
 @pytest.mark.parametrize("plen,nlen", [(3, 50), (4, 4), (40, 38), (64, 64), (170, 165), (300, 290),
                                        (380, 420), (999, 960)])
-def test_window_schedule_matches_library(plen, nlen):
-    ws = ro.windows(plen, nlen, True)
-    assert len(ws) == ia.window_count(plen, nlen, True)
-    assert len(ro.windows(plen, nlen, False)) == ia.window_count(plen, nlen, False)
-    for flen, ps, ns in ws:
-        assert 4 <= flen <= min(plen, nlen) and ps + flen <= plen and ns + flen <= nlen
+def test_candidate_schedules_match_library(plen, nlen):
+    for kind in range(ia.CAND_KINDS):
+        cs = ro.candidates(plen, nlen, kind)
+        assert len(cs) == ia.candidate_count(plen, nlen, kind), kind
+        for flen, ps, ns in cs:
+            assert 3 <= flen <= min(plen, nlen) and ps + flen <= plen and ns + flen <= nlen
+    assert ia.candidate_count(plen, nlen, 3) == 0 and ia.candidate_count(-1, nlen, 0) == 0
 
 
 def test_pair_rows_pairs_within_groups():
