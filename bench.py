@@ -1,26 +1,36 @@
 """Benchmark of the batched TM-score superposition search (one JSON line).
 
-Workload (default): batch4096 -- 4096 synthetic pairs, L ~ U(40,300),
-sigma ~ U(0.5,14) A, random rigid transform, 5 % invalid per mask, lnorm = L,
-default NativeConfig.  A step is one search over the whole batch.
+Workload (default, learned16384): the learned-vs-plain configuration --
+16384 synthetic pairs, L ~ U(40,1000), sigma ~ U(0.5,14) A, random rigid
+transform, 5 % invalid residues per mask, lnorm = L, default NativeConfig.
+A step is one search call over a batch of --step-pairs pairs (2048: eight
+steps cover the 16384 pairs; warm-up and timed steps take consecutive
+batches).
 
-  value  pairs/s with inputs resident in HBM (indialign_tmscore_search_device),
-         device-timed with CUDA events on the call's stream, L2 flushed
-         (256 MB write) between steps, max over ranks.
-  e2e    the same through the C-ABI batch call with host buffers: the
-         host->device copy of the inputs and the device->host read of the
-         results are inside the timed region.
-  roofline  for the NW-chain kernel (the dominant kernel): algorithmic FP64
-         flops (18 per NW cell: 13 score-matrix + 5 DP; 55 per Kabsch/refine
-         residue visit) / its summed device time, against the measured FP64
-         FMA peak of the GPU (indialign_fp64_peak).
+  value    pairs/s of the LEARNED search (the rescue passes refine the
+           ranker's top-8 candidates per pair, margin 0.02, 2 % audit), inputs
+           resident in HBM (indialign_tmscore_search_device), device-timed
+           with CUDA events on the call's stream, L2 flushed (256 MB write)
+           before every step, max over ranks.
+  plain    the PLAIN search (every candidate refined, the reference's
+           algorithm) on the same timed batches, same timing; its ratio to
+           `value` and the per-pair final TM-score change of the learned
+           search against it (mean, worst) are reported.
+  e2e      the learned search through the C-ABI batch call with host
+           buffers: host->device copies of the inputs and the device->host
+           read of the results inside the timed region.
+  roofline the dominant kernel of the learned step (by summed device time):
+           algorithmic FP64 flops / its device time against the measured FP64
+           FMA peak of the GPU (indialign_fp64_peak); NW chains: 18 flop per
+           NW cell + 55 per refine residue visit, bank: 55 per residue visit.
   cpu_baseline  the reference's own build (oracle/_ref, OpenMP batch entry)
-         on this host's cores, on a stratified subsample of the workload.
+           on this host's cores over a stratified sample of the timed pairs,
+           bounded to ~25 s.
 
 Multi-GPU (torchrun): pairs are independent, so each rank searches its own
-batch of the same shape (weak scaling, no data-path collective); value = all
-ranks' pairs / max rank time.  --impl reference: the reference build on the
-host cores, rank 0 only.
+batches of the same shape (weak scaling, no data-path collective); value =
+all ranks' pairs / max rank time.  --impl reference: the reference build on
+the host cores, rank 0 only.
 """
 from __future__ import annotations
 
@@ -44,21 +54,29 @@ METRIC = "pairs/sec on 1 B200, learned-seed vs plain GPU search at mean ΔTM ≥
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libindialign_ref.so")
 FLOP_PER_CELL = 18.0
 FLOP_PER_VISIT = 55.0
+STAGES = ["seeds", "seed_bank", "ss", "gapless", "local_fragment", "threading_dp",
+          "dense_local_fragment", "topk", "dp_refine", "offset_dp", "weighted", "total"]
 
 
-def workload(name: str, seed_shift: int = 0):
-    if name == "batch4096":
-        return W.batch(4096, 40, 300, seed=1 + seed_shift), \
-            "batch4096: 4096 pairs, L~U(40,300), sigma~U(0.5,14), 5% invalid per mask"
-    if name == "hard1024":
-        return W.hard(1024, seed=2 + seed_shift), \
-            "hard1024: 1024 pairs, L log-uniform 30..1500, half hard (30-60% stems kept)"
-    if name == "single":
-        return W.single(0), "single: L=64, sigma=2.0, all valid"
-    if name.startswith("batch"):
-        n = int(name[5:])
-        return W.batch(n, 40, 300, seed=1 + seed_shift), f"batch{n}: L~U(40,300), sigma~U(0.5,14)"
-    raise SystemExit(f"unknown workload {name}")
+def workload(name: str, step_pairs: int, n_steps: int, rank: int = 0):
+    """The pairs of n_steps consecutive batches of `name` for this rank."""
+    if name == "learned16384":
+        total = 16384
+        n = min(total, step_pairs * n_steps) if rank == 0 else step_pairs * n_steps
+        pairs = W.parallel_batch(n, 40, 1000, seed=4 + 1000 * rank)
+        desc = ("learned16384: 16384 pairs, L~U(40,1000), sigma~U(0.5,14) A, random rigid transform, "
+                "5% invalid per mask, lnorm=L")
+    elif name == "batch4096":
+        pairs = W.parallel_batch(min(4096, step_pairs * n_steps), 40, 300, seed=1 + 1000 * rank)
+        desc = "batch4096: 4096 pairs, L~U(40,300), sigma~U(0.5,14), 5% invalid per mask"
+    elif name == "hard1024":
+        pairs = W.hard(1024, seed=2 + 1000 * rank)
+        desc = "hard1024: 1024 pairs, L log-uniform 30..1500, half hard (30-60% stems kept)"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    batches = [pairs[(k * step_pairs) % len(pairs):(k * step_pairs) % len(pairs) + step_pairs]
+               for k in range(n_steps)]
+    return batches, desc
 
 
 class Clocks:
@@ -111,39 +129,48 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(pairs, n_sample=64, seed=7):
-    """The reference build on this host's cores over a stratified subsample."""
+def cpu_baseline(pairs, n_sample=32, budget_s=25.0, seed=7):
+    """The reference build on this host's cores over a stratified sample of
+    `pairs`, in chunks of one pair per core until `budget_s` is spent."""
     if not os.path.exists(REF_SO):
         return None
     sample = W.subsample(pairs, n_sample, seed=seed)
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
     ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
-    t0 = time.perf_counter()
-    rc, s, _, _ = abi.run_batch(ref, sample)
-    dt = time.perf_counter() - t0
-    return {"value": len(sample) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
-            "sample": f"{len(sample)}-pair length-stratified subsample of the workload (seed {seed}), "
-                      f"reference build, OpenMP batch entry, {dt:.1f} s"}, sample, s
+    rng = np.random.default_rng(seed)
+    order = list(rng.permutation(len(sample)))
+    done, scores, dt = [], [], 0.0
+    while order and dt < budget_s:
+        chunk = [sample[i] for i in order[:cores]]
+        order = order[cores:]
+        t0 = time.perf_counter()
+        _, s, _, _ = abi.run_batch(ref, chunk)
+        dt += time.perf_counter() - t0
+        done.extend(chunk)
+        scores.extend(list(s))
+    return {"value": len(done) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
+            "sample": f"{len(done)} pairs of a {len(sample)}-pair length-stratified sample of the timed "
+                      f"batches (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}, \
+        done, np.array(scores)
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    pairs, desc = workload(args.workload)
     if not os.path.exists(REF_SO):
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
         return
+    batches, desc = workload(args.workload, args.step_pairs, args.warmup + args.steps)
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
     ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
-    warm = W.subsample(pairs, 4, seed=3)
-    for _ in range(args.warmup):
-        abi.run_batch(ref, warm)
+    for k in range(args.warmup):
+        abi.run_batch(ref, W.subsample(batches[k], 2, seed=3 + k))
     times, n_done = [], 0
     for k in range(args.steps):
-        sample = W.subsample(pairs, args.ref_pairs, seed=100 + k)
+        sample = W.subsample(batches[args.warmup + k], args.ref_pairs, seed=100 + k)
         t0 = time.perf_counter()
         abi.run_batch(ref, sample)
         times.append(time.perf_counter() - t0)
@@ -153,7 +180,8 @@ def run_reference_arm(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "step": f"{args.ref_pairs}-pair stratified subsample per step",
+            "config": {"workload": desc,
+                       "step": f"{args.ref_pairs}-pair stratified sample of one {args.step_pairs}-pair batch",
                        "host_threads": cores},
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
                              "sample": f"{args.ref_pairs} pairs per step x {args.steps} steps"},
@@ -162,65 +190,88 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+class DeviceBatch:
+    """One batch packed back to back in HBM (torch tensors as plumbing)."""
+
+    def __init__(self, torch, pairs):
+        self.n = len(pairs)
+        lens = [p.pred.shape[0] for p in pairs]
+        self.off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+
+        def cat(f, dt):
+            return torch.from_numpy(np.ascontiguousarray(
+                np.concatenate([np.asarray(f(p), dt).reshape(-1) for p in pairs]))).cuda()
+
+        self.pred, self.nat = cat(lambda p: p.pred, np.float64), cat(lambda p: p.native, np.float64)
+        self.v, self.pv, self.nv = (cat(lambda p: p.valid, np.uint8), cat(lambda p: p.pred_valid, np.uint8),
+                                    cat(lambda p: p.native_valid, np.uint8))
+        self.lnorm = np.array([p.lnorm for p in pairs], np.float64)
+        self.out = torch.zeros(self.n * 13, dtype=torch.float64, device="cuda")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batch4096")
-    ap.add_argument("--ref-pairs", type=int, default=48)
-    ap.add_argument("--cpu-sample", type=int, default=64)
+    ap.add_argument("--workload", default="learned16384")
+    ap.add_argument("--step-pairs", type=int, default=2048)
+    ap.add_argument("--top-k", type=int, default=8)
+    ap.add_argument("--margin", type=float, default=0.02)
+    ap.add_argument("--audit", type=float, default=0.02)
+    ap.add_argument("--ref-pairs", type=int, default=8)
+    ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
 
-    import torch
-    import indialign_b200 as ia
-
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    batches, desc = workload(args.workload, args.step_pairs, args.warmup + args.steps, rank)
+
+    import torch
+    import indialign_b200 as ia
+    from indialign_b200 import ranker
+
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    pairs, desc = workload(args.workload, seed_shift=1000 * rank)
-    n = len(pairs)
     lib = ia.load()
     cfg = ia.default_config()
-    # inputs resident in HBM
-    lens = [p.pred.shape[0] for p in pairs]
-    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
-    cat = lambda f, dt: torch.from_numpy(np.ascontiguousarray(
-        np.concatenate([np.asarray(f(p), dt).reshape(-1) for p in pairs]))).cuda()
-    d_pred, d_nat = cat(lambda p: p.pred, np.float64), cat(lambda p: p.native, np.float64)
-    d_v, d_pv, d_nv = (cat(lambda p: p.valid, np.uint8), cat(lambda p: p.pred_valid, np.uint8),
-                       cat(lambda p: p.native_valid, np.uint8))
-    lnorm = np.array([p.lnorm for p in pairs], np.float64)
-    d_out = torch.zeros(n * 13, dtype=torch.float64, device="cuda")
+    blob = ranker.default_weights()
+    dev = [DeviceBatch(torch, b) for b in batches]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
-    kern = np.zeros(6)
-    ctr = np.zeros(12, np.int64)
-    stage_ms = np.zeros(12)
-    opts = ia.BatchOptions()
-    opts.device = local
-    opts.stream = ctypes.c_void_p(stream.cuda_stream)
-    opts.kernel_ms = kern.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-    opts.counters = ctr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
-    opts.stage_ms = stage_ms.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
-    def step():
+    def make_opts(learned: bool):
+        o = ia.BatchOptions()
+        o.device = local
+        o.stream = ctypes.c_void_p(stream.cuda_stream)
+        o.kern = np.zeros(6)
+        o.ctr = np.zeros(12, np.int64)
+        o.stg = np.zeros(12)
+        o.rst = np.zeros(ia.RANK_STATS, np.int64)
+        o.kernel_ms = o.kern.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        o.counters = o.ctr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
+        o.stage_ms = o.stg.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if learned:
+            ia.learned_options(o, blob, args.top_k, args.margin, args.audit, 1234 + rank, o.rst)
+        return o
+
+    def device_step(db, o):
         rc = lib.indialign_tmscore_search_device(
-            n, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), d_pred.data_ptr(), d_nat.data_ptr(),
-            d_v.data_ptr(), d_pv.data_ptr(), d_nv.data_ptr(),
-            lnorm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(cfg),
-            ctypes.byref(opts), d_out.data_ptr())
+            db.n, db.off.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), db.pred.data_ptr(), db.nat.data_ptr(),
+            db.v.data_ptr(), db.pv.data_ptr(), db.nv.data_ptr(),
+            db.lnorm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(cfg), ctypes.byref(o),
+            db.out.data_ptr())
         if rc != 0:
             raise SystemExit(f"search failed rc={rc}: {ia.last_error()}")
 
@@ -228,111 +279,156 @@ def main():
         if dist:
             dist.barrier()
 
-    for _ in range(args.warmup):
+    def timed(fn):
         flush.zero_()
-        step()
-    torch.cuda.synchronize()
-    times, kms, cells, visits, launches, cyc, stg = [], [], [], [], [], [], []
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            step()
-            e1.record(stream)
-            torch.cuda.synchronize()
-            barrier()
-            times.append(e0.elapsed_time(e1))
-            kms.append(kern[0])
-            cells.append(ctr[0])
-            visits.append(ctr[1])
-            launches.append(int(ctr[7]) + 2)  # + repack and export
-            cyc.append(ctr[8:12].copy())
-            stg.append(stage_ms.copy())
-    clocks = clk.summary()
-    ms = float(np.mean(times))
-    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
-    value = n * world / (ms_max / 1e3)
-    scores = d_out.view(n, 13)[:, 0].cpu().numpy()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return e0.elapsed_time(e1)
 
-    # end to end through the C-ABI batch entry (host buffers)
+    def run_mode(learned: bool, clocks=None):
+        o = make_opts(learned)
+        for k in range(args.warmup):
+            timed(lambda: device_step(dev[k], o))
+        rec = dict(ms=[], kern=[], ctr=[], stg=[], rst=[], scores=[])
+        ctx = clocks if clocks is not None else _Null()
+        with ctx:
+            for k in range(args.steps):
+                db = dev[args.warmup + k]
+                rec["ms"].append(timed(lambda: device_step(db, o)))
+                rec["kern"].append(o.kern.copy())
+                rec["ctr"].append(o.ctr.copy())
+                rec["stg"].append(o.stg.copy())
+                rec["rst"].append(o.rst.copy())
+                rec["scores"].append(db.out.view(db.n, 13)[:, 0].cpu().numpy())
+        return rec
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clk = Clocks(local)
+    lrn = run_mode(True, clk)
+    clocks = clk.summary()
+    n_timed = sum(dev[args.warmup + k].n for k in range(args.steps))
+    l_ms = max_over_ranks(float(np.sum(lrn["ms"])))
+    value = n_timed * world / (l_ms / 1e3)
+    l_scores = np.concatenate(lrn["scores"])
+
+    plain = None
+    if not args.no_plain:
+        pl = run_mode(False)
+        p_ms = max_over_ranks(float(np.sum(pl["ms"])))
+        p_scores = np.concatenate(pl["scores"])
+        d = l_scores - p_scores
+        plain = {"value": n_timed * world / (p_ms / 1e3), "unit": "pairs/s",
+                 "ms_per_step": p_ms / args.steps, "learned_over_plain": (n_timed * world / (l_ms / 1e3)) /
+                 (n_timed * world / (p_ms / 1e3)),
+                 "delta_tm": {"mean": float(d.mean()), "worst": float(d.min()), "best": float(d.max()),
+                              "pairs_below_-1e-4": int(np.sum(d < -1e-4)),
+                              "pairs_below_-1e-3": int(np.sum(d < -1e-3)), "pairs": int(d.size)},
+                 "stage_ms": dict(zip(STAGES, [round(float(x), 2) for x in np.mean(pl["stg"], 0)])),
+                 "kernel_ms": {"k_chain": float(np.mean([k[0] for k in pl["kern"]])),
+                               "k_bank": float(np.mean([k[1] for k in pl["kern"]]))}}
+    else:
+        p_scores = None
+
+    # end to end: the learned search through the C-ABI batch entry with host buffers
     e2e = None
     if not args.no_e2e:
-        pk = abi.PackedInputs(pairs)
-        res = (abi.NativePairResult * n)()
-        eopts = ia.BatchOptions()
-        eopts.device = local
-        eopts.stream = ctypes.c_void_p(stream.cuda_stream)
-        etimes = []
-        for k in range(1 + min(args.steps, 2)):
-            flush.zero_()
-            torch.cuda.synchronize()
-            barrier()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            rc = lib.indialign_tmscore_search_batch_ex(n, pk.arr, ctypes.byref(cfg), ctypes.byref(eopts), res)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            barrier()
-            assert rc == 0, ia.last_error()
-            if k > 0:
-                etimes.append(e0.elapsed_time(e1))
-        em = torch.tensor([float(np.mean(etimes))], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(em, op=dist.ReduceOp.MAX)
-        es, _, _ = abi.results_to_numpy(res, n)
-        assert np.array_equal(es, scores), "host and device entry points disagree"
-        h2d = int(sum(p.pred.shape[0] * (48 + 3) + 8 for p in pairs))
-        e2e = {"value": n * world / (em.item() / 1e3), "unit": "pairs/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 104 * n}
+        eo = make_opts(True)
+        eo.kernel_ms = eo.counters = eo.stage_ms = None
+        packs = [abi.PackedInputs(b) for b in batches[args.warmup:args.warmup + args.steps]]
+        res = [(abi.NativePairResult * p.n)() for p in packs]
+        timed(lambda: lib.indialign_tmscore_search_batch_ex(packs[0].n, packs[0].arr, ctypes.byref(cfg),
+                                                            ctypes.byref(eo), res[0]))
+        et = []
+        for k, pk in enumerate(packs):
+            rc = []
+            et.append(timed(lambda: rc.append(lib.indialign_tmscore_search_batch_ex(
+                pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(eo), res[k]))))
+            assert rc[0] == 0, ia.last_error()
+        es = np.concatenate([abi.results_to_numpy(r, p.n)[0] for r, p in zip(res, packs)])
+        assert np.array_equal(es, l_scores), "host and device entry points disagree"
+        e_ms = max_over_ranks(float(np.sum(et)))
+        pairs_t = [p for b in batches[args.warmup:] for p in b]
+        h2d = int(sum(p.pred.shape[0] * (48 + 3) + 8 for p in pairs_t)) // args.steps
+        e2e = {"value": n_timed * world / (e_ms / 1e3), "unit": "pairs/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": 104 * n_timed // args.steps}
 
-    line = None
     if rank == 0:
         peak = ia.fp64_peak_tflops(local)
-        flops = FLOP_PER_CELL * float(np.mean(cells)) + FLOP_PER_VISIT * float(np.mean(visits))
-        k_ms = float(np.mean(kms))
-        achieved = flops / (k_ms / 1e3) / 1e12 if k_ms > 0 else None
-        roofline = {"kernel": "k_chain (NW chains: score matrix + NW + Kabsch + refine)",
-                    "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        kern = np.mean(lrn["kern"], 0)
+        ctr = np.mean(lrn["ctr"], 0)
+        step_ms = l_ms / args.steps
+        if kern[0] >= kern[1]:
+            flops = FLOP_PER_CELL * ctr[0] + FLOP_PER_VISIT * ctr[1]
+            kname, kms = "k_chain (NW chains: score matrix + NW + Kabsch + refine)", kern[0]
+        else:
+            flops = FLOP_PER_VISIT * ctr[2]
+            kname, kms = "k_bank (seed x cutoff refine items)", kern[1]
+        achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else None
+        cyc = ctr[8:12]
+        roofline = {"kernel": kname, "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak if achieved else None, "traffic": None,
                     "peak_source": "measured FP64 FMA rate (indialign_fp64_peak) in this run",
-                    "kernel_ms_per_step": k_ms, "kernel_share": k_ms / ms,
-                    "nw_cells_per_step": int(np.mean(cells)),
-                    "refine_visits_per_step": int(np.mean(visits)),
+                    "kernel_ms_per_step": float(kms), "kernel_share": float(kms / step_ms),
+                    "kernel_ms": {"k_chain": float(kern[0]), "k_bank": float(kern[1]), "k_rank": float(kern[4])},
+                    "nw_cells_per_step": int(ctr[0]), "chain_visits_per_step": int(ctr[1]),
+                    "bank_visits_per_step": int(ctr[2]),
                     "warp_cycle_split": dict(zip(["nw_fill", "traceback", "detailed", "kabsch"],
-                                                 [float(x) for x in np.mean(cyc, 0) / max(1.0, np.mean(cyc, 0).sum())]))}
+                                                 [float(x) for x in cyc / max(1.0, cyc.sum())]))}
+        rst = np.sum(lrn["rst"], 0).reshape(ia.CAND_KINDS, 8)
+        rank_info = {}
+        for k, nm in enumerate(ia.CAND_NAMES):
+            g = max(int(rst[k, 0]), 1)
+            rank_info[nm] = {"pairs": int(rst[k, 0]), "fallback_rate": rst[k, 1] / g, "audit_rate": rst[k, 2] / g,
+                             "pruned_rate": rst[k, 3] / g, "refined_fraction": rst[k, 5] / max(int(rst[k, 4]), 1),
+                             "audit_misses": int(rst[k, 6])}
         cpu = None
         if not args.no_cpu_baseline:
-            r = cpu_baseline(pairs, args.cpu_sample)
+            timed_pairs = [p for b in batches[args.warmup:] for p in b]
+            r = cpu_baseline(timed_pairs, args.cpu_sample)
             if r:
-                cpu, sample, ref_s = r
-                pos = {id(p): k for k, p in enumerate(pairs)}
-                idx = [pos[id(p)] for p in sample]
-                d = scores[idx] - ref_s
-                cpu["parity_on_sample"] = {"min_dTM": float(d.min()), "max_abs_dTM": float(np.abs(d).max()),
-                                           "pairs_below_ref_minus_1e-6": int(np.sum(d < -1e-6))}
+                cpu, done, ref_s = r
+                if p_scores is not None:
+                    pos = {id(p): k for k, p in enumerate(timed_pairs)}
+                    idx = [pos[id(p)] for p in done]
+                    d = p_scores[idx] - ref_s
+                    cpu["plain_parity_on_sample"] = {"min_dTM": float(d.min()),
+                                                     "max_abs_dTM": float(np.abs(d).max()),
+                                                     "pairs_below_ref_minus_1e-6": int(np.sum(d < -1e-6))}
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": desc, "pairs_per_gpu": n, "mode": "plain",
+                "config": {"workload": desc, "step_pairs": args.step_pairs, "pairs_timed_per_gpu": n_timed,
+                           "mode": f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit})",
+                           "ranker": "indialign_b200/ranker_weights.npy",
                            "l2": "flushed by a 256 MB write before every step",
                            "parallelism": f"independent pairs per GPU x{world}"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(np.mean(launches)), "clocks": clocks,
-                "stage_ms": dict(zip(["seeds", "seed_bank", "ss", "gapless", "local_fragment",
-                                      "threading_dp", "dense_local_fragment", "topk", "dp_refine",
-                                      "offset_dp", "weighted", "total"],
-                                     [round(float(x), 2) for x in np.mean(stg, 0)])),
-                "mean_tm": float(scores.mean())}
+                "plain": plain, "rank": rank_info, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(ctr[7]) + 2, "clocks": clocks,
+                "stage_ms": dict(zip(STAGES, [round(float(x), 2) for x in np.mean(lrn["stg"], 0)])),
+                "mean_tm": float(l_scores.mean())}
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
 
 
 if __name__ == "__main__":

@@ -20,28 +20,15 @@ from __future__ import annotations
 
 import argparse
 import json
-import multiprocessing as mp
 import sys
 import time
 
 import numpy as np
 
 
-def _gen(args):
+def generate(n: int, lo: int, hi: int, seed: int, procs: int = 8):
     from indialign_b200 import workloads as W
-    n, lo, hi, seed = args
-    return W.batch(n, lo, hi, seed=seed)
-
-
-def generate(n: int, lo: int, hi: int, seed: int, chunk: int = 256, procs: int = 8):
-    """n pairs in chunks generated by a spawn pool (started before any GPU
-    work); chunk c uses seed * 100003 + c."""
-    jobs = [(min(chunk, n - s), lo, hi, seed * 100003 + c) for c, s in enumerate(range(0, n, chunk))]
-    with mp.get_context("spawn").Pool(procs) as pool:
-        out = []
-        for part in pool.imap(_gen, jobs):
-            out.extend(part)
-    return out
+    return W.parallel_batch(n, lo, hi, seed, procs=procs)
 
 
 def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):

@@ -206,7 +206,25 @@ def hard(n: int = 1024, seed: int = 2) -> list[Pair]:
 
 
 def learned(n: int = 16384, seed: int = 4) -> list[Pair]:
+    """Learned-vs-plain workload: n pairs, L~U(40,1000), as batch()."""
     return batch(n, 40, 1000, seed)
+
+
+def _batch_job(args):
+    n, lo, hi, seed = args
+    return batch(n, lo, hi, seed=seed)
+
+
+def parallel_batch(n: int, lo: int, hi: int, seed: int, chunk: int = 256, procs: int = 8) -> list[Pair]:
+    """batch()-distributed pairs generated in chunks by a spawn process pool
+    (safe to start before or after CUDA initialisation); chunk c draws from
+    seed * 100003 + c, so the result depends only on (n, lo, hi, seed, chunk)."""
+    import multiprocessing as mp
+    jobs = [(min(chunk, n - s), lo, hi, seed * 100003 + c) for c, s in enumerate(range(0, n, chunk))]
+    if procs <= 1 or len(jobs) == 1:
+        return [p for j in jobs for p in _batch_job(j)]
+    with mp.get_context("spawn").Pool(min(procs, len(jobs))) as pool:
+        return [p for part in pool.imap(_batch_job, jobs) for p in part]
 
 
 def subsample(pairs: list[Pair], k: int, seed: int = 7) -> list[Pair]:
