@@ -11,7 +11,7 @@
    threading-DP offsets, dense windows; pairs whose pass ran only).  Per pair
    and kind at most --per-pair candidates are kept: the best --keep-top by
    label plus a random draw of the rest.
-3. Training: MSE + pairwise ranking loss, Adam (lr 1e-3, batch 8192 windows,
+3. Training: MSE + 10 x pairwise ranking loss (--lam), Adam (lr 1e-3, batch 8192,
    --epochs), every step on the library's BF16 tensor-core kernels.
 4. Held-out evaluation: how often the top-k predicted windows contain the
    pair's best window score, and the margin-fallback rate.
@@ -121,7 +121,7 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--lam", type=float, default=1.0)
+    ap.add_argument("--lam", type=float, default=10.0)
     ap.add_argument("--chunk", type=int, default=512)
     ap.add_argument("--procs", type=int, default=8)
     ap.add_argument("--out", default="ranker_weights.npy")
