@@ -109,13 +109,18 @@ typedef struct {
                                 then ms and launches of the window-ranker kernel */
     double *stage_best;      /* optional [n_pairs*INDIALIGN_TRACE_STAGES*13]: running
                                 best {score,R,t} after each search stage */
-    /* ---- learned candidate ranker of the rescue passes ----
+    /* ---- learned candidate ranker ----
      * The local-fragment, threading-DP and dense local-fragment passes
      * (rescue.h) each refine a list of candidate starts per pair (windows /
-     * offsets, INDIALIGN_CAND_*).  LEARNED mode scores them with the ranker
-     * and refines the top_k of each pair.  Per-candidate arrays below hold
-     * the three kinds back to back, each kind pair by pair, pair p with
-     * indialign_candidate_count(plen_p, nlen_p, kind) entries. */
+     * offsets), and every detailed search (align.h:15-50, in the SS seeds
+     * and in dp_refine) refines a list of fragment seeds of an alignment
+     * (INDIALIGN_CAND_*).  LEARNED mode scores them with the ranker and
+     * refines the top_k of each pair (of each alignment for detailed
+     * searches).  Per-candidate arrays below hold the four kinds back to
+     * back, each kind pair by pair, pair p with
+     * indialign_candidate_count(plen_p, nlen_p, kind) entries (detailed
+     * searches: two alignment slots of equal size; COLLECT keeps the last
+     * detailed search that ran on a slot, normally dp_refine's). */
     int mode;                /* INDIALIGN_MODE_PLAIN (0), _LEARNED or _COLLECT */
     const float *ranker;     /* LEARNED (or COLLECT with predictions): host FP32
                                 parameter blob of INDIALIGN_RANKER_FLOATS floats */
@@ -125,9 +130,10 @@ typedef struct {
     double audit_rate;       /* LEARNED: fraction of pairs refined on all candidates */
     unsigned long long seed; /* LEARNED: audit draw */
     long long *rank_stats;   /* LEARNED: optional [INDIALIGN_RANK_STATS] out, per kind
-                                8 counts: pairs ranked, margin fallbacks, audits,
-                                pruned pairs, candidates, candidates refined, audit
-                                misses, pairs with at most top_k candidates */
+                                8 counts summed over the batch's searches: lists
+                                ranked, margin fallbacks, audits, pruned lists,
+                                candidates, candidates refined, audit misses, lists
+                                with at most top_k candidates */
     float *win_feat;         /* COLLECT: out [candidates][16] raw features */
     float *win_label;        /* COLLECT: out [candidates] refined score, NaN where
                                 the pair's pass did not run */
@@ -135,10 +141,12 @@ typedef struct {
                                 per-candidate outputs */
     float *win_score;        /* optional out [candidates] (LEARNED, or COLLECT with a
                                 ranker): predicted score of every candidate */
-    int *win_select;         /* optional out [3][n_pairs][33] (LEARNED): per kind and
-                                pair the candidates refined (-1: all, margin
-                                fallback, pass not run or at most top_k; -2: all,
-                                audit), then the top_k candidates ascending */
+    int *win_select;         /* optional out [5*n_pairs][33] (LEARNED): rows per kind
+                                back to back (n_pairs each, 2*n_pairs alignment
+                                slots for detailed searches, the batch's last one):
+                                candidates refined (-1: all, margin fallback, not
+                                run or at most top_k; -2: all, audit), then the
+                                top_k candidates ascending */
 } IndialignBatchOptions;
 
 #define INDIALIGN_MODE_PLAIN 0   /* the reference's search, every candidate refined */
@@ -147,8 +155,9 @@ typedef struct {
 #define INDIALIGN_CAND_LOCAL 0   /* local-fragment windows (rescue.h:50-117) */
 #define INDIALIGN_CAND_THREAD 1  /* threading-DP offsets (rescue.h:121-190) */
 #define INDIALIGN_CAND_DENSE 2   /* dense local-fragment windows */
+#define INDIALIGN_CAND_DET 3     /* detailed-search fragment seeds (align.h:15-50) */
 #define INDIALIGN_RANKER_FLOATS 18849
-#define INDIALIGN_RANK_STATS 24
+#define INDIALIGN_RANK_STATS 32
 
 /* Stages recorded in stage_best, in search order: seed bank, SS seeds,
  * gapless threading, local fragment DP, threading DP, dense local fragment
@@ -202,7 +211,8 @@ int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap,
                                int *d_an, int *d_na, void *stream);
 
 /* Candidates of kind INDIALIGN_CAND_* of a pair with plen / nlen valid pred /
- * native residues (the schedules of rescue.h:12-46 and :136-142). */
+ * native residues (the schedules of rescue.h:12-46 and :136-142; for
+ * detailed searches the room of both alignment slots). */
 int indialign_candidate_count(int plen, int nlen, int kind);
 
 /* ---- ranker training on caller-owned device buffers (no counterpart in the

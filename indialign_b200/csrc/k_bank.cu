@@ -88,7 +88,7 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         const int li = (c - chunk_begin[ti]) * kBankChunk + threadIdx.x;
         const bool active = li < T.n_items;
         const int C = T.C > 0 ? T.C : 1;
-        const int k = active ? li / C : 0, ci = active ? li % C : 0;
+        const int k = active ? (T.slist ? T.slist[li / C] : li / C) : 0, ci = active ? li % C : 0;
         const double cut = T.cut[ci];
         const double cut2 = cut * cut;
         double R[9], t[3];

@@ -16,7 +16,7 @@
 //             FP64), then the 16 -> 128 -> 128 -> 1 GELU MLP runs on BF16
 //             tensor cores (mma.sync m16n8k16, FP32 accumulation) over the
 //             warp's 16-candidate tile, with the weights in shared memory.
-//   k_select  warp per pair: top-k by (predicted score desc, index asc),
+//   k_select  warp per task: top-k by (predicted score desc, index asc),
 //             margin fallback, audit draw, list in ascending order (so the
 //             stage's reduction keeps the reference's first-max rule).
 //   k_audit   audited pairs: did the top-k contain the best refined score?
@@ -182,10 +182,12 @@ IA_DEV void mlp_tile(const MlpSmem &S, const float *xt, float &y_g, float &y_g8,
 //   11 log(ml) / 7                12 running best score     13 candidate kind / 2
 //   14 min(RMSD / d0, 10) / 10    15 TM along the same-index diagonal
 // (ml = min(plen, nlen); indices are compact valid-residue positions.)
+// Detailed-search seeds are segments of an aligned set (plen == nlen == the
+// aligned count, SS labels absent: stem fractions 0).
 IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, const PairInfo &I,
-                            double best, int kind, int w, float (&f)[kFeatures]) {
+                            int plen, int nlen, double best, int kind, int w, float (&f)[kFeatures]) {
     const int lane = threadIdx.x & 31;
-    const int plen = I.plen, nlen = I.nlen, ml = plen < nlen ? plen : nlen;
+    const int ml = plen < nlen ? plen : nlen;
     int flen, ps, ns;
     cand_at(kind, plen, nlen, w, flen, ps, ns);
     double R[9], t[3];
@@ -197,8 +199,10 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
         const double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
         sd2 += d2;
         stm += 1.0 / (1.0 + d2 * inv);
-        sp += Lp[ps + i] != 'L' ? 1.0 : 0.0;
-        sn += Ln[ns + i] != 'L' ? 1.0 : 0.0;
+        if (Lp) {
+            sp += Lp[ps + i] != 'L' ? 1.0 : 0.0;
+            sn += Ln[ns + i] != 'L' ? 1.0 : 0.0;
+        }
     }
     const int s = ns - ps;
     const int lo = s < 0 ? -s : 0, hi = plen < nlen - s ? plen : nlen - s;
@@ -241,16 +245,52 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
     f[15] = (float)(tm0 / I.lnorm);
 }
 
+// The candidate set of ranking task t: a pair (windows, offsets) or a
+// (pair, alignment slot) of a detailed search, with its point set.
+struct RankTask {
+    int p, W, plen, nlen;
+    bool on;
+    Pts x;
+    const uint8_t *Lp, *Ln;
+};
+
+IA_DEV RankTask rank_task(const DevBatch &b, const RankArgs &a, int t) {
+    RankTask r;
+    if (a.kind == CAND_DET) {
+        r.p = t / kDetSlots;
+        const int g = t % kDetSlots;
+        const PairInfo &I = b.info[r.p];
+        const PairState &S = b.state[r.p];
+        const int na = S.na[g];
+        // the detailed searches' own gates (align.h:115-118, ss.h:96-99)
+        r.on = I.status == 0 && na >= 3 && (a.det_ss ? (g == 0 && S.flag != 0) : S.active[g] != 0);
+        const size_t base = 3 * (kDetSlots * (size_t)I.off + (size_t)g * I.N);
+        r.x = {a.alP + base, a.alQ + base};
+        r.plen = r.nlen = na;
+        r.Lp = r.Ln = nullptr;
+        r.W = r.on ? cand_count(CAND_DET, na, na) : 0;
+    } else {
+        r.p = t;
+        const PairInfo &I = b.info[t];
+        r.on = I.status == 0 && b.state[t].flag != 0;
+        r.x = {b.predc + 3 * (size_t)I.off, b.natc + 3 * (size_t)I.off};
+        r.plen = I.plen;
+        r.nlen = I.nlen;
+        r.Lp = reinterpret_cast<const uint8_t *>(b.sspc + I.off);
+        r.Ln = reinterpret_cast<const uint8_t *>(b.ssnc + I.off);
+        r.W = r.on ? cand_count(a.kind, I.plen, I.nlen) : 0;
+    }
+    return r;
+}
+
 }  // namespace
 
-// ---- ranking: features + MLP over the windows of gated pairs ------------------
-__global__ void k_plan_rank(DevBatch b, int kind, int *counts) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= b.n) return;
-    const PairInfo &I = b.info[p];
-    const int W = cand_count(kind, I.plen, I.nlen);
-    const bool on = I.status == 0 && b.state[p].flag && W > 0;
-    counts[p] = on ? (W + kRankChunk - 1) / kRankChunk : 0;
+// ---- ranking: features + MLP over the candidates of gated tasks -----------------
+__global__ void k_plan_rank(DevBatch b, RankArgs a, int *counts) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ntasks) return;
+    const RankTask r = rank_task(b, a, t);
+    counts[t] = r.on && r.W > 0 ? (r.W + kRankChunk - 1) / kRankChunk : 0;
 }
 
 __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int *__restrict__ chunk_begin,
@@ -267,7 +307,7 @@ __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int 
             const int c = atomicAdd(counter, 1);
             int t = -1;
             if (c < total) {
-                int lo = 0, hi = b.n;
+                int lo = 0, hi = a.ntasks;
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
                     if (chunk_begin[mid] <= c) lo = mid + 1; else hi = mid;
@@ -278,23 +318,21 @@ __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int 
             s_pair = t;
         }
         __syncthreads();
-        const int c = s_chunk, p = s_pair;
-        if (c >= total || p < 0) break;
-        const PairInfo &I = b.info[p];
-        const int W = cand_count(a.kind, I.plen, I.nlen);
-        const int w0 = (c - chunk_begin[p]) * kRankChunk + warp * 16;
+        const int c = s_chunk, ti = s_pair;
+        if (c >= total || ti < 0) break;
+        const RankTask rt = rank_task(b, a, ti);
+        const PairInfo &I = b.info[rt.p];
+        const int W = rt.W;
+        const int w0 = (c - chunk_begin[ti]) * kRankChunk + warp * 16;
         if (w0 < W) {
-            const Pts x = {b.predc + 3 * (size_t)I.off, b.natc + 3 * (size_t)I.off};
-            const uint8_t *Lp = reinterpret_cast<const uint8_t *>(b.sspc + I.off);
-            const uint8_t *Ln = reinterpret_cast<const uint8_t *>(b.ssnc + I.off);
-            const double best = b.state[p].rec[REC_BEST][0];
-            const long long wb = a.wbase[p];
+            const double best = b.state[rt.p].rec[REC_BEST][0];
+            const long long wb = a.wbase[ti];
             for (int r = 0; r < 16; r++) {
                 const int w = w0 + r;
                 float mine = 0.f;
                 if (w < W) {
                     float f[kFeatures];
-                    window_features(x, Lp, Ln, I, best, a.kind, w, f);
+                    window_features(rt.x, rt.Lp, rt.Ln, I, rt.plen, rt.nlen, best, a.kind, w, f);
 #pragma unroll
                     for (int j = 0; j < kFeatures; j++)
                         if (lane == j) mine = f[j];
@@ -327,16 +365,17 @@ IA_DEV unsigned long long mix64(unsigned long long z) {  // splitmix64 finaliser
 }
 
 __global__ void k_select(DevBatch b, SelectArgs a) {
-    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (p >= b.n) return;
-    const PairInfo &I = b.info[p];
-    int *list = a.wlist + (size_t)p * kMaxTopK;
-    if (I.status != 0 || !b.state[p].flag) {
-        if (lane == 0) a.wcount[p] = -1;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (t >= a.task.ntasks) return;
+    const RankTask rt = rank_task(b, a.task, t);
+    const int p = rt.p;  // audit draws are per pair
+    int *list = a.wlist + (size_t)t * kMaxTopK;
+    if (!rt.on) {
+        if (lane == 0) a.wcount[t] = -1;
         list[lane] = -1;
         return;
     }
-    const int W = cand_count(a.kind, I.plen, I.nlen);
+    const int W = rt.W;
     const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
     if (lane == 0) {
         atomicAdd(a.stats + RS_GATED, 1ull);
@@ -345,13 +384,13 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
     if (W <= k) {
         list[lane] = -1;
         if (lane == 0) {
-            a.wcount[p] = -1;
+            a.wcount[t] = -1;
             atomicAdd(a.stats + RS_SMALL, 1ull);
             atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
         }
         return;
     }
-    const float *sc = a.score + a.wbase[p];
+    const float *sc = a.score + a.wbase[t];
     // k rounds of "next in (score desc, window asc) order"
     float prev_s = INFINITY, top1 = 0.f;
     int prev_i = -1;
@@ -389,15 +428,15 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
         const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)p + 0x9e3779b97f4a7c15ull)) >> 11) *
                          (1.0 / 9007199254740992.0);
         if (u < a.audit_rate) {
-            a.wcount[p] = -2;
+            a.wcount[t] = -2;
             atomicAdd(a.stats + RS_AUDIT, 1ull);
             atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
         } else if (top1 - prev_s < a.margin) {
-            a.wcount[p] = -1;
+            a.wcount[t] = -1;
             atomicAdd(a.stats + RS_FALLBACK, 1ull);
             atomicAdd(a.stats + RS_REFINED, (unsigned long long)W);
         } else {
-            a.wcount[p] = k;
+            a.wcount[t] = k;
             atomicAdd(a.stats + RS_PRUNED, 1ull);
             atomicAdd(a.stats + RS_REFINED, (unsigned long long)k);
         }
@@ -407,8 +446,17 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
 // A candidate's refined score: the dp_refine result over its two gap chains
 // (later chain only if strictly better, indialign_c/align.h:131-145); for a
 // threading offset the better of that and its detailed search
-// (rescue.h:163-165).  -inf for an offset that was not searched.
-IA_DEV double cand_score(const CandRes &r, int p, int w) {
+// (rescue.h:163-165), -inf for an offset that was not searched; for a
+// detailed-search seed the best of its cutoff items.
+IA_DEV double cand_score(const CandRes &r, int kind, int det_ss, int t, int w) {
+    if (kind == CAND_DET) {
+        const BankTask &T = r.btasks[det_ss ? t / kDetSlots : t];
+        double s = -INFINITY;
+        for (int ci = 0; ci < kDetC; ci++)
+            s = fmax(s, r.item_res[((size_t)T.item_base + (size_t)w * kDetC + ci) * kRec]);
+        return s;
+    }
+    const int p = t;
     const double *res = r.chain_res + (size_t)r.chain_base[p] * kRec;
     const double s0 = res[(size_t)(2 * w) * kRec], s1 = res[(size_t)(2 * w + 1) * kRec];
     double s = s1 > s0 ? s1 : s0;
@@ -423,14 +471,15 @@ IA_DEV double cand_score(const CandRes &r, int p, int w) {
 // Audited pairs ran every candidate: count those whose selected candidates
 // miss the best refined score.
 __global__ void k_audit(DevBatch b, SelectArgs a, CandRes r) {
-    const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (p >= b.n || a.wcount[p] != -2) return;
-    const PairInfo &I = b.info[p];
-    const int W = cand_count(a.kind, I.plen, I.nlen);
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (t >= a.task.ntasks || a.wcount[t] != -2) return;
+    const RankTask rt = rank_task(b, a.task, t);
+    const int W = rt.W, kind = a.task.kind, ds = a.task.det_ss;
     const int k = a.top_k < kMaxTopK ? (a.top_k > 0 ? a.top_k : 1) : kMaxTopK;
     double full = -INFINITY, sel = -INFINITY;
-    for (int w = lane; w < W; w += 32) full = fmax(full, cand_score(r, p, w));
-    for (int j = lane; j < k; j += 32) sel = fmax(sel, cand_score(r, p, a.wlist[(size_t)p * kMaxTopK + j]));
+    for (int w = lane; w < W; w += 32) full = fmax(full, cand_score(r, kind, ds, t, w));
+    for (int j = lane; j < k; j += 32)
+        sel = fmax(sel, cand_score(r, kind, ds, t, a.wlist[(size_t)t * kMaxTopK + j]));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         full = fmax(full, __shfl_xor_sync(kAllLanes, full, o));
@@ -441,14 +490,16 @@ __global__ void k_audit(DevBatch b, SelectArgs a, CandRes r) {
 
 // Training labels: every candidate's refined score for pairs that ran the
 // stage on all candidates, NaN elsewhere.
-__global__ void k_collect_labels(DevBatch b, const long long *wbase, CandRes r, int kind, float *label) {
-    const int p = blockIdx.x;
-    const PairInfo &I = b.info[p];
-    const int W = cand_count(kind, I.plen, I.nlen);
-    const bool on = I.status == 0 && b.state[p].flag;
-    float *out = label + wbase[p];
-    for (int w = threadIdx.x; w < W; w += blockDim.x) {
-        const double s = on ? cand_score(r, p, w) : -INFINITY;
+// The label array starts as NaN (the host fills it before the search) and
+// tasks of a pass that did not run are left alone, so a detailed-search slot
+// keeps the (features, labels) of the last search that ran on it.
+__global__ void k_collect_labels(DevBatch b, RankArgs a, CandRes r, float *label) {
+    const int t = blockIdx.x;
+    const RankTask rt = rank_task(b, a, t);
+    if (!rt.on) return;
+    float *out = label + a.wbase[t];
+    for (int w = threadIdx.x; w < rt.W; w += blockDim.x) {
+        const double s = cand_score(r, a.kind, a.det_ss, t, w);
         out[w] = s > -1e299 ? (float)s : NAN;
     }
 }
@@ -711,8 +762,8 @@ cudaError_t rank_set_attributes() {
     return e;
 }
 
-void launch_plan_rank(const DevBatch &b, int kind, int *counts, cudaStream_t st) {
-    if (b.n > 0) k_plan_rank<<<(b.n + 127) / 128, 128, 0, st>>>(b, kind, counts);
+void launch_plan_rank(const DevBatch &b, const RankArgs &a, int *counts, cudaStream_t st) {
+    if (a.ntasks > 0) k_plan_rank<<<(a.ntasks + 127) / 128, 128, 0, st>>>(b, a, counts);
 }
 
 void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
@@ -721,16 +772,18 @@ void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, c
 }
 
 void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st) {
-    if (b.n > 0) k_select<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a);
+    const int nt = a.task.ntasks;
+    if (nt > 0) k_select<<<(nt * 32 + 127) / 128, 128, 0, st>>>(b, a);
 }
 
 void launch_audit(const DevBatch &b, const SelectArgs &a, const CandRes &r, cudaStream_t st) {
-    if (b.n > 0) k_audit<<<(b.n * 32 + 127) / 128, 128, 0, st>>>(b, a, r);
+    const int nt = a.task.ntasks;
+    if (nt > 0) k_audit<<<(nt * 32 + 127) / 128, 128, 0, st>>>(b, a, r);
 }
 
-void launch_collect_labels(const DevBatch &b, const long long *wbase, const CandRes &r, int kind,
-                           float *label, cudaStream_t st) {
-    if (b.n > 0) k_collect_labels<<<b.n, 256, 0, st>>>(b, wbase, r, kind, label);
+void launch_collect_labels(const DevBatch &b, const RankArgs &a, const CandRes &r, float *label,
+                           cudaStream_t st) {
+    if (a.ntasks > 0) k_collect_labels<<<a.ntasks, 256, 0, st>>>(b, a, r, label);
 }
 
 void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st) {

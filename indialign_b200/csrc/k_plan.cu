@@ -34,6 +34,7 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
     T.V = b.v + I.off;
     T.PV = T.NV = nullptr;
     T.table = nullptr;
+    T.slist = nullptr;
     T.bits = b.bits + I.bitoff;
     T.words = I.words;
     T.cut = I.cut;
@@ -79,6 +80,13 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
         T.early_term = 1.0;
         T.out_rec = REC_DET0 + g;
         on = on && na >= 3 && (c.kind == BK_DET_SS ? S.flag : S.active[g]);
+        if (c.wcount) {  // ranked: the selected seeds only (task = pair x slot)
+            const int task = kDetSlots * p + g;
+            if (c.wcount[task] >= 0) {
+                T.K = c.wcount[task];
+                T.slist = c.wlist + (size_t)task * kMaxTopK;
+            }
+        }
         break;
     }
     case BK_GAPLESS: {  // gapless threading (threading.h:41-80)

@@ -120,13 +120,18 @@ struct MlpSave {
 
 struct RankArgs {
     const MlpPacked *mlp;      // nullptr: features only
-    const long long *wbase;    // [n] first candidate of a pair in the candidate arrays
+    const long long *wbase;    // [ntasks] first candidate of a task in the candidate arrays
     float *score;              // [candidates] predicted refined score
     float *feat;               // optional [candidates][16] raw features
     int kind;                  // CandKind
+    int ntasks;                // pairs, or pairs x kDetSlots for CAND_DET
+    int det_ss;                // CAND_DET: the SS detailed search (slot 0 under the
+                               // stage flag) instead of dp_refine's (active slots)
+    const double *alP, *alQ;   // CAND_DET: aligned coordinates (2 slots per pair)
 };
 
 struct SelectArgs {
+    RankArgs task;              // candidate sets (kind, tasks, aligned sets)
     const long long *wbase;
     const float *score;
     int *wcount;               // [n] selected windows, -1 = all
@@ -141,15 +146,19 @@ struct SelectArgs {
 
 // Where the refined results of a stage's candidates live: two gap-chain
 // records per candidate (chain_res + chain_base[p]), and for threading
-// offsets also the detailed-search record (det + det_base[p] + offset).
+// offsets also the detailed-search record (det + det_base[p] + offset); for
+// detailed-search seeds the bank items (kDetC cutoffs per seed) of the bank
+// task of each (pair, slot).
 struct CandRes {
     const double *chain_res;
     const long long *chain_base;
     const double *det;
     const int *det_base;
+    const double *item_res;
+    const BankTask *btasks;
 };
 
-void launch_plan_rank(const DevBatch &b, int kind, int *counts, cudaStream_t st);
+void launch_plan_rank(const DevBatch &b, const RankArgs &a, int *counts, cudaStream_t st);
 void launch_rank(const DevBatch &b, const RankArgs &a, const int *chunk_begin, const ScanOut *scan,
                  int *counter, int grid, cudaStream_t st);
 cudaError_t rank_set_attributes();
@@ -157,8 +166,8 @@ size_t rank_smem_bytes();
 const void *rank_kernel_ptr();
 void launch_select(const DevBatch &b, const SelectArgs &a, cudaStream_t st);
 void launch_audit(const DevBatch &b, const SelectArgs &a, const CandRes &r, cudaStream_t st);
-void launch_collect_labels(const DevBatch &b, const long long *wbase, const CandRes &r, int kind,
-                           float *label, cudaStream_t st);
+void launch_collect_labels(const DevBatch &b, const RankArgs &a, const CandRes &r, float *label,
+                           cudaStream_t st);
 void launch_mlp_pack(const float *blob, MlpPacked *out, cudaStream_t st);
 void launch_mlp_forward(const MlpPacked *mlp, const float *x, int n, float *y, const MlpSave *save,
                         cudaStream_t st);

@@ -80,6 +80,7 @@ struct BankTask {
     const double *P, *Q;
     const uint8_t *V, *PV, *NV;
     const int2 *table;
+    const int *slist;    // SEED_ARITH: the K seed indices to refine (nullptr: 0..K-1)
     const uint32_t *bits;
     const double *cut;
     int n, K, C, mode, ms, max_iter, use_d8, words;
@@ -170,11 +171,14 @@ constexpr int kHidden = 128;
 constexpr int kMaxTopK = 32;
 constexpr int kRankChunk = 64;  // candidates per CTA chunk of the ranker (4 warps x 16)
 
-// Candidate starts the ranker scores, in search order: local-fragment
-// windows (rescue.h:50-117, dense = false), threading-DP offsets
-// (rescue.h:121-190), dense local-fragment windows.  Each is a segment
-// (flen, ps, ns) of compact pred / native positions.
-enum CandKind { CAND_LOCAL = 0, CAND_THREAD = 1, CAND_DENSE = 2, kCandKinds = 3 };
+// Candidate starts the ranker scores: local-fragment windows
+// (rescue.h:50-117, dense = false), threading-DP offsets (rescue.h:121-190),
+// dense local-fragment windows -- each a segment (flen, ps, ns) of compact
+// pred / native positions of a pair -- and the seeds of the detailed searches
+// on an NW alignment (align.h:15-50, fragments of the aligned set, two
+// alignment slots per pair).
+enum CandKind { CAND_LOCAL = 0, CAND_THREAD = 1, CAND_DENSE = 2, CAND_DET = 3, kCandKinds = 4 };
+constexpr int kDetSlots = 2;  // detailed-search alignment slots per pair (gap chains)
 
 // FP32 parameter blob: mean[16] std[16] W1[16][128] b1[128] W2[128][128]
 // b2[128] w3[128] b3, weights stored [in][out] row-major.  mean/std

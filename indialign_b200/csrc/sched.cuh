@@ -182,10 +182,14 @@ IA_HD void thread_at(int plen, int nlen, int o, int &ps, int &ns, int &ov) {
 // Ranked candidates of a kind (pipeline.h CandKind): windows, or threading
 // offsets as the segment of their overlap.
 IA_HD int cand_count(int kind, int plen, int nlen) {
+    if (kind == 3) return arith_seed_count(imin_(plen, nlen), 50, true);
     return kind == 1 ? thread_count(plen, nlen) : window_count(plen, nlen, kind == 2 ? 1 : 0);
 }
 IA_HD void cand_at(int kind, int plen, int nlen, int i, int &flen, int &ps, int &ns) {
-    if (kind == 1) {
+    if (kind == 3) {  // detailed-search seed on an aligned set of plen == nlen points
+        arith_seed(plen, 50, i, ps, flen);
+        ns = ps;
+    } else if (kind == 1) {
         thread_at(plen, nlen, i, ps, ns, flen);
     } else {
         window_at(plen, nlen, kind == 2 ? 1 : 0, i, flen, ps, ns);

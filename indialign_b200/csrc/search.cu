@@ -222,9 +222,13 @@ class Runner {
              const int *wcount = nullptr, const int *wlist = nullptr);
     int chain(int kind, Layout &L, int iters, double *recs = nullptr, double *recs2 = nullptr,
               bool reduce = true, const int *wcount = nullptr, const int *wlist = nullptr);
-    int rank_stage(int kind);
-    SelectArgs select_args(int kind);
-    int after_stage(int kind, const CandRes &r);
+    int rank_stage(int kind, int det_ss = 0);
+    RankArgs rank_args(int kind, int det_ss);
+    SelectArgs select_args(int kind, int det_ss);
+    int after_stage(int kind, const CandRes &r, int det_ss = 0);
+    int ntasks(int kind) const { return kind == CAND_DET ? kDetSlots * n_ : n_; }
+    // first selection row of a kind in the win_select output (kinds back to back)
+    long long sel_row(int kind) const { return kind == CAND_DET ? 3LL * n_ : (long long)kind * n_; }
     const int *sel_count() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wcount.p : nullptr; }
     const int *sel_list() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wlist.p : nullptr; }
     int glue(int op, double thr = 0.0, const double *recs = nullptr, const int *idx = nullptr);
@@ -235,7 +239,7 @@ class Runner {
     int n_;
     Layout L_pair, L_main, L_detss, L_detdp, L_gapless, L_thread, L_topk, L_localn, L_locald,
         L_threadch, L_single, L_offdp, L_offslots, L_cand[kCandKinds];
-    long long koff_[kCandKinds + 1] = {0, 0, 0, 0};
+    long long koff_[kCandKinds + 1] = {0, 0, 0, 0, 0};
     long long max_items_ = 0, max_chain_recs_ = 0, n_thread_ = 0, n_off_ = 0;
     int chain_grid_ = 0, chain_flags_ = 0, rank_grid_ = 1;
     size_t trace_words_ = 0;
@@ -313,8 +317,16 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     // callers can lay out per-candidate outputs from the valid counts alone),
     // kinds back to back
     for (int k = 0; k < kCandKinds; k++) {
-        L_cand[k].base.resize(n);
-        for (int p = 0; p < n; p++) L_cand[k].base[p] = cand_count(k, info[p].plen, info[p].nlen);
+        if (k == CAND_DET) {  // kDetSlots alignment slots per pair, each sized for the largest aligned set
+            L_cand[k].base.resize((size_t)kDetSlots * n);
+            for (int p = 0; p < n; p++) {
+                const int m = info[p].plen < info[p].nlen ? info[p].plen : info[p].nlen;
+                for (int g = 0; g < kDetSlots; g++) L_cand[k].base[(size_t)kDetSlots * p + g] = kdet_max(m);
+            }
+        } else {
+            L_cand[k].base.resize(n);
+            for (int p = 0; p < n; p++) L_cand[k].base[p] = cand_count(k, info[p].plen, info[p].nlen);
+        }
         finish_layout(L_cand[k]);
         koff_[k + 1] = koff_[k] + L_cand[k].total;
     }
@@ -344,7 +356,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     size_t ni = 0, nl = 0;
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
                       &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
-                      &L_cand[0], &L_cand[1], &L_cand[2]}) {
+                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3]}) {
         ni += L->pair.size() + L->aux.size();
         nl += L->base.size();
     }
@@ -356,7 +368,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     hl.reserve(nl);
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
                       &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
-                      &L_cand[0], &L_cand[1], &L_cand[2]}) {
+                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3]}) {
         L->d_pair = L->pair.empty() ? nullptr : c_->lay_i.p + hi.size();
         hi.insert(hi.end(), L->pair.begin(), L->pair.end());
         L->d_aux = L->aux.empty() ? nullptr : c_->lay_i.p + hi.size();
@@ -416,8 +428,8 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     if (cfg_.mode != INDIALIGN_MODE_PLAIN) {
         const size_t nw = (size_t)(windows() > 0 ? windows() : 1);
         CK(c_->wscore.ensure(nw));
-        CK(c_->wcount.ensure((size_t)kCandKinds * (n > 0 ? n : 1)));
-        CK(c_->wlist.ensure((size_t)kCandKinds * (n > 0 ? n : 1) * kMaxTopK));
+        CK(c_->wcount.ensure((size_t)kDetSlots * (n > 0 ? n : 1)));
+        CK(c_->wlist.ensure((size_t)kDetSlots * (n > 0 ? n : 1) * kMaxTopK));
         CK(c_->rstats.ensure(kCandKinds * kRankStats));
         if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
             CK(c_->wfeat.ensure(nw * kFeatures));
@@ -530,6 +542,11 @@ int Runner::glue(int op, double thr, const double *recs, const int *idx) {
     return INDIALIGN_OK;
 }
 
+// Where a detailed search's seed items are: the bank's items and tasks.
+static CandRes det_res(Ctx *c) {
+    return CandRes{nullptr, nullptr, nullptr, nullptr, c->item_res.p, c->btasks.p};
+}
+
 // dp_refine with fragment detailed searches (indialign_c/align.h:54-145,
 // d0_search_lite = false): per iteration one NW per gap chain, then the
 // detailed bank on each alignment, then the per-chain update.
@@ -537,7 +554,9 @@ int Runner::dp_full() {
     int rc;
     for (int it = 0; it < cfg_.dp_iter; it++) {
         if ((rc = chain(CH_DP_EMIT, L_pair, 1, nullptr, nullptr, false))) return rc;
-        if ((rc = bank(BK_DET_DP, L_detdp))) return rc;
+        if ((rc = rank_stage(CAND_DET, 0))) return rc;
+        if ((rc = bank(BK_DET_DP, L_detdp, nullptr, -1, -1, sel_count(), sel_list()))) return rc;
+        if ((rc = after_stage(CAND_DET, det_res(c_), 0))) return rc;
         if ((rc = glue(G_DP_STEP))) return rc;
     }
     return glue(G_DP_END);
@@ -547,18 +566,31 @@ int Runner::dp_full() {
 // its gate let in.  PLAIN: nothing.  LEARNED: features + MLP scores, then the
 // per-pair selection the pass's plan reads (wcount / wlist).  COLLECT: the
 // features of every candidate.
-int Runner::rank_stage(int kind) {
-    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return INDIALIGN_OK;
-    cudaStream_t st = c_->stream;
-    const bool learned = cfg_.mode == INDIALIGN_MODE_LEARNED;
-    launch_plan_rank(b, kind, c_->counts.p, st);
-    launch_scan(c_->counts.p, c_->begins.p, n_, c_->scan.p, c_->counter.p, st);
+RankArgs Runner::rank_args(int kind, int det_ss) {
     RankArgs ra;
     ra.mlp = use_mlp ? c_->mlp.p : nullptr;
     ra.wbase = L_cand[kind].d_base;
     ra.score = c_->wscore.p + koff_[kind];
-    ra.feat = learned ? nullptr : c_->wfeat.p + koff_[kind] * kFeatures;
+    ra.feat = cfg_.mode == INDIALIGN_MODE_COLLECT ? c_->wfeat.p + koff_[kind] * kFeatures : nullptr;
     ra.kind = kind;
+    ra.ntasks = ntasks(kind);
+    ra.det_ss = det_ss;
+    ra.alP = c_->alP.p;
+    ra.alQ = c_->alQ.p;
+    return ra;
+}
+
+int Runner::rank_stage(int kind, int det_ss) {
+    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return INDIALIGN_OK;
+    cudaStream_t st = c_->stream;
+    const RankArgs ra = rank_args(kind, det_ss);
+    if (kind == CAND_DET) {  // a slot's arrays hold its last search only (NaN beyond its seeds)
+        CK(cudaMemsetAsync(c_->wscore.p + koff_[kind], 0xff, (size_t)L_cand[kind].total * sizeof(float), st));
+        if (cfg_.mode == INDIALIGN_MODE_COLLECT)
+            CK(cudaMemsetAsync(c_->wlabel.p + koff_[kind], 0xff, (size_t)L_cand[kind].total * sizeof(float), st));
+    }
+    launch_plan_rank(b, ra, c_->counts.p, st);
+    launch_scan(c_->counts.p, c_->begins.p, ra.ntasks, c_->scan.p, c_->counter.p, st);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (timing) {
         e0 = new_event();
@@ -572,16 +604,17 @@ int Runner::rank_stage(int kind) {
     }
     launches_ += 3;
     rank_launches_++;
-    if (learned) {
-        launch_select(b, select_args(kind), st);
+    if (cfg_.mode == INDIALIGN_MODE_LEARNED) {
+        launch_select(b, select_args(kind, det_ss), st);
         launches_++;
     }
     CK(cudaGetLastError());
     return INDIALIGN_OK;
 }
 
-SelectArgs Runner::select_args(int kind) {
+SelectArgs Runner::select_args(int kind, int det_ss) {
     SelectArgs sa;
+    sa.task = rank_args(kind, det_ss);
     sa.wbase = L_cand[kind].d_base;
     sa.score = c_->wscore.p + koff_[kind];
     sa.wcount = c_->wcount.p;
@@ -595,20 +628,21 @@ SelectArgs Runner::select_args(int kind) {
     return sa;
 }
 
-// After a ranked pass: LEARNED checks the audited pairs, COLLECT records
+// After a ranked pass: LEARNED checks the audited tasks, COLLECT records
 // every candidate's refined score.
-int Runner::after_stage(int kind, const CandRes &r) {
+int Runner::after_stage(int kind, const CandRes &r, int det_ss) {
     cudaStream_t st = c_->stream;
     if (cfg_.mode == INDIALIGN_MODE_LEARNED) {
-        launch_audit(b, select_args(kind), r, st);
+        launch_audit(b, select_args(kind, det_ss), r, st);
         if (sel_out) {  // keep this pass's selection for the caller
-            CK(cudaMemcpyAsync(sel_out + (size_t)kind * n_, c_->wcount.p, n_ * sizeof(int),
-                               cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(sel_out + (size_t)kCandKinds * n_ + (size_t)kind * n_ * kMaxTopK, c_->wlist.p,
-                               (size_t)n_ * kMaxTopK * sizeof(int), cudaMemcpyDeviceToDevice, st));
+            const int nt = ntasks(kind);
+            CK(cudaMemcpyAsync(sel_out + sel_row(kind), c_->wcount.p, nt * sizeof(int), cudaMemcpyDeviceToDevice,
+                               st));
+            CK(cudaMemcpyAsync(sel_out + 5LL * n_ + sel_row(kind) * kMaxTopK, c_->wlist.p,
+                               (size_t)nt * kMaxTopK * sizeof(int), cudaMemcpyDeviceToDevice, st));
         }
     } else if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
-        launch_collect_labels(b, L_cand[kind].d_base, r, kind, c_->wlabel.p + koff_[kind], st);
+        launch_collect_labels(b, rank_args(kind, det_ss), r, c_->wlabel.p + koff_[kind], st);
     } else {
         return INDIALIGN_OK;
     }
@@ -633,13 +667,17 @@ int Runner::run_stages() {
     launches_++;
     RUN(glue(G_SS_BEGIN));
     RUN(chain(CH_SS2, L_pair, 1, nullptr, nullptr, false));
-    RUN(bank(BK_DET_SS, L_detss));
+    RUN(rank_stage(CAND_DET, 1));
+    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(), sel_list()));
+    RUN(after_stage(CAND_DET, det_res(c_), 1));
     RUN(glue(G_SS_DET));
     RUN(dp_full());
     RUN(glue(G_SS_DP));
     RUN(glue(G_SS4_START));
     RUN(chain(CH_SS4, L_pair, 1, nullptr, nullptr, false));
-    RUN(bank(BK_DET_SS, L_detss));
+    RUN(rank_stage(CAND_DET, 1));
+    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(), sel_list()));
+    RUN(after_stage(CAND_DET, det_res(c_), 1));
     RUN(glue(G_SS_DET));
     RUN(dp_full());
     RUN(glue(G_SS_DP));
@@ -655,7 +693,7 @@ int Runner::run_stages() {
     RUN(glue(G_GATE, cfg_.r1));
     RUN(rank_stage(CAND_LOCAL));
     RUN(chain(CH_LOCAL, L_localn, 0, nullptr, nullptr, true, sel_count(), sel_list()));
-    RUN(after_stage(CAND_LOCAL, CandRes{c_->chain_res.p, L_localn.d_base, nullptr, nullptr}));
+    RUN(after_stage(CAND_LOCAL, CandRes{c_->chain_res.p, L_localn.d_base, nullptr, nullptr, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
@@ -664,7 +702,8 @@ int Runner::run_stages() {
     RUN(rank_stage(CAND_THREAD));
     RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p, -1, -1, sel_count(), sel_list()));
     RUN(chain(CH_THREAD, L_threadch, 1, c_->thread_rec.p));
-    RUN(after_stage(CAND_THREAD, CandRes{c_->chain_res.p, L_threadch.d_base, c_->thread_rec.p, L_threadch.d_aux}));
+    RUN(after_stage(CAND_THREAD,
+                    CandRes{c_->chain_res.p, L_threadch.d_base, c_->thread_rec.p, L_threadch.d_aux, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
@@ -672,7 +711,7 @@ int Runner::run_stages() {
     RUN(glue(G_GATE, cfg_.r2));
     RUN(rank_stage(CAND_DENSE));
     RUN(chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, sel_count(), sel_list()));
-    RUN(after_stage(CAND_DENSE, CandRes{c_->chain_res.p, L_locald.d_base, nullptr, nullptr}));
+    RUN(after_stage(CAND_DENSE, CandRes{c_->chain_res.p, L_locald.d_base, nullptr, nullptr, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
     RUN(glue(G_STAGE_UPDATE));
@@ -940,10 +979,12 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         g_last_error = "per-window outputs: " + std::to_string(r.windows()) + " windows exceed win_cap";
         return INDIALIGN_E_INPUT;
     }
+    if (cfg.mode == INDIALIGN_MODE_COLLECT && r.windows() > 0)
+        CK(cudaMemsetAsync(c->wlabel.p, 0xff, (size_t)r.windows() * sizeof(float), st));  // NaN
     if (cfg.mode == INDIALIGN_MODE_LEARNED) {
         CK(cudaMemsetAsync(c->rstats.p, 0, kCandKinds * kRankStats * sizeof(unsigned long long), st));
         if (opts->win_select) {
-            CK(c->wsel.ensure((size_t)kCandKinds * n * (1 + kMaxTopK)));
+            CK(c->wsel.ensure((size_t)5 * n * (1 + kMaxTopK)));
             r.sel_out = c->wsel.p;
         }
     }
@@ -982,16 +1023,17 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaMemcpy(opts->win_score, c->wscore.p, (size_t)r.windows() * sizeof(float),
                       cudaMemcpyDeviceToHost));
     if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->win_select) {
-        std::vector<int> h((size_t)kCandKinds * n * (1 + kMaxTopK));
+        // rows: kinds back to back, n rows each, 2n for the detailed-search slots
+        const size_t rows = (size_t)5 * n;
+        std::vector<int> h(rows * (1 + kMaxTopK));
         CK(cudaMemcpy(h.data(), c->wsel.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
-        const int *wc = h.data(), *wl = h.data() + (size_t)kCandKinds * n;
-        for (int k = 0; k < kCandKinds; k++)
-            for (int p = 0; p < n; p++) {
-                int *o = opts->win_select + ((size_t)k * n + p) * (kMaxTopK + 1);
-                const int *l = wl + ((size_t)k * n + p) * kMaxTopK;
-                o[0] = wc[(size_t)k * n + p];
-                for (int j = 0; j < kMaxTopK; j++) o[1 + j] = j < cfg.top_k ? l[j] : -1;
-            }
+        const int *wc = h.data(), *wl = h.data() + rows;
+        for (size_t r0 = 0; r0 < rows; r0++) {
+            int *o = opts->win_select + r0 * (kMaxTopK + 1);
+            const int *l = wl + r0 * kMaxTopK;
+            o[0] = wc[r0];
+            for (int j = 0; j < kMaxTopK; j++) o[1 + j] = j < cfg.top_k ? l[j] : -1;
+        }
     }
     if (cfg.mode == INDIALIGN_MODE_COLLECT && r.windows() > 0) {
         if (opts->win_feat)
@@ -1269,6 +1311,7 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
 
 int indialign_candidate_count(int plen, int nlen, int kind) {
     if (plen < 0 || nlen < 0 || kind < 0 || kind >= ia::kCandKinds) return 0;
+    if (kind == ia::CAND_DET) return ia::kDetSlots * ia::kdet_max(plen < nlen ? plen : nlen);
     return ia::cand_count(kind, plen, nlen);
 }
 

@@ -31,9 +31,20 @@ def generate(n: int, lo: int, hi: int, seed: int, procs: int = 8):
     return W.parallel_batch(n, lo, hi, seed, procs=procs)
 
 
+def groups(off, kind: int, i: int):
+    """Candidate ranges [a, b) of pair i's lists of one kind: one list, or
+    the two alignment slots of the detailed searches."""
+    import indialign_b200 as ia
+    a, b = int(off[kind, i]), int(off[kind, i + 1])
+    if kind != ia.CAND_DET:
+        return [(a, b)]
+    h = (b - a) // 2
+    return [(a, a + h), (a + h, b)]
+
+
 def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):
-    """Features / labels / group ids of the kept candidates of every pair
-    and kind whose pass ran; a group is one (pair, kind)."""
+    """Features / labels / group ids of the kept candidates of every list
+    whose pass ran; a group is one list (pair, kind, slot)."""
     import indialign_b200 as ia
     rng = np.random.default_rng(seed)
     F, Y, G = [], [], []
@@ -43,17 +54,18 @@ def collect(pairs, chunk: int, per_pair: int, keep_top: int, seed: int, log):
         _, feat, label, off = ia.collect_windows(part)
         for kind in range(ia.CAND_KINDS):
             for i in range(len(part)):
-                lab = label[off[kind, i]:off[kind, i + 1]]
-                idx = np.flatnonzero(np.isfinite(lab))
-                if idx.size < 2:
-                    continue
-                if idx.size > per_pair:
-                    top = idx[np.argsort(-lab[idx], kind="stable")[:keep_top]]
-                    rest = np.setdiff1d(idx, top)
-                    idx = np.concatenate([top, rng.choice(rest, per_pair - keep_top, replace=False)])
-                F.append(feat[off[kind, i] + idx])
-                Y.append(lab[idx])
-                G.append(np.full(idx.size, 3 * (s + i) + kind, np.int64))
+                for slot, (a, b) in enumerate(groups(off, kind, i)):
+                    lab = label[a:b]
+                    idx = np.flatnonzero(np.isfinite(lab))
+                    if idx.size < 2:
+                        continue
+                    if idx.size > per_pair:
+                        top = idx[np.argsort(-lab[idx], kind="stable")[:keep_top]]
+                        rest = np.setdiff1d(idx, top)
+                        idx = np.concatenate([top, rng.choice(rest, per_pair - keep_top, replace=False)])
+                    F.append(feat[a + idx])
+                    Y.append(lab[idx])
+                    G.append(np.full(idx.size, 8 * (s + i) + 2 * kind + slot, np.int64))
         log(f"collect {min(s + chunk, len(pairs))}/{len(pairs)} pairs, {sum(y.size for y in Y)} windows, "
             f"{time.time() - t0:.0f} s")
     if not F:
@@ -68,19 +80,23 @@ def evaluate(blob, pairs, chunk: int, ks=(1, 4, 8, 16), margin: float = 0.02, lo
     candidates an 8-candidate selection with the margin fallback refines."""
     import indialign_b200 as ia
     res = {}
-    acc = [dict(tot=0, fb=0, frac=[], hits={k: 0 for k in ks}, near={k: 0 for k in ks}) for _ in range(3)]
+    acc = [dict(tot=0, fb=0, frac=[], hits={k: 0 for k in ks}, near={k: 0 for k in ks})
+           for _ in range(ia.CAND_KINDS)]
     dumps = []
     for s in range(0, len(pairs), chunk):
         part = pairs[s:s + chunk]
         _, feat, label, off, pred = ia.collect_windows(part, ranker=blob)
         for kind in range(ia.CAND_KINDS):
             a = acc[kind]
-            for i in range(len(part)):
-                lab = label[off[kind, i]:off[kind, i + 1]]
-                if lab.size == 0 or np.isnan(lab).all():
+            for i, (ga, gb) in ((i, g) for i in range(len(part)) for g in groups(off, kind, i)):
+                lab = label[ga:gb]
+                fin = np.isfinite(lab)
+                if not fin.any():
                     continue
-                lab = np.where(np.isfinite(lab), lab, -np.inf)
-                pr = pred[off[kind, i]:off[kind, i + 1]]
+                # a detailed-search slot holds its last search's seeds
+                n_used = int(np.flatnonzero(fin).max()) + 1
+                lab = np.where(fin, lab, -np.inf)[:n_used]
+                pr = pred[ga:ga + n_used]
                 order = np.lexsort((np.arange(lab.size), -pr))
                 a["tot"] += 1
                 for k in ks:

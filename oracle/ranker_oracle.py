@@ -76,8 +76,46 @@ def thread_offsets(plen: int, nlen: int) -> list[tuple[int, int, int]]:
     return out
 
 
+def frag_lengths(L: int) -> list[int]:
+    """fragment_lengths (seeds.h:15-22): {L, L/2, L/4, L/8, 64, 32, 16, 8, 4}
+    within [4, L], distinct, descending."""
+    out = []
+    for v in (L, L // 2, L // 4, L // 8, 64, 32, 16, 8, 4):
+        if 4 <= v <= L and v not in out:
+            out.append(v)
+    return sorted(out, reverse=True)
+
+
+def start_positions(n: int, frag: int, ms: int) -> list[int]:
+    """start_positions (seeds.h:24-37)."""
+    total = n - frag + 1
+    if total <= 0:
+        return []
+    if total <= ms:
+        return list(range(total))
+    step = max(1, total // ms)
+    out = list(range(0, total, step))
+    if out[-1] != total - 1:
+        out.append(total - 1)
+    return out
+
+
+def det_seeds(na: int, ms: int = 50) -> list[tuple[int, int, int]]:
+    """Seeds of a detailed search on na aligned points (align.h:33-37):
+    the whole set, then windows (len, s, s)."""
+    if na < 3:
+        return []
+    out = [(na, 0, 0)]
+    for f in frag_lengths(na):
+        out += [(f, s, s) for s in start_positions(na, f, ms)]
+    return out
+
+
 def candidates(plen: int, nlen: int, kind: int) -> list[tuple[int, int, int]]:
-    """Kind 0 local windows, 1 threading offsets, 2 dense windows."""
+    """Kind 0 local windows, 1 threading offsets, 2 dense windows, 3
+    detailed-search seeds (plen == nlen == aligned count)."""
+    if kind == 3:
+        return det_seeds(min(plen, nlen))
     return thread_offsets(plen, nlen) if kind == 1 else windows(plen, nlen, kind == 2)
 
 

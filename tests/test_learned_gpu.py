@@ -188,7 +188,7 @@ def test_candidate_features_match_oracle(oracle):
     for i, p in enumerate(pairs):
         ss = (_ss(oracle, p.pred, p.pred_valid), _ss(oracle, p.native, p.native_valid))
         Pc, Qc, ssp, ssn = _compact(p, ss)
-        for kind in range(ia.CAND_KINDS):
+        for kind in range(3):  # detailed-search seeds live on device-only alignments
             lab = label[off[kind, i]:off[kind, i + 1]]
             if lab.size == 0 or np.isnan(lab).all():
                 continue
@@ -214,7 +214,7 @@ def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True
     off = ia.candidate_offsets(pairs)
     C = int(off[-1, -1])
     score = np.zeros(max(1, C), np.float32)
-    sel = np.zeros((ia.CAND_KINDS, len(pairs), 33), np.int32)
+    sel = np.zeros((5 * len(pairs), 33), np.int32)
     if outputs:
         opts.win_score = score.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         opts.win_cap = C
@@ -225,6 +225,18 @@ def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True
     return abi.results_to_numpy(res, pk.n), stats.reshape(ia.CAND_KINDS, 8), score, sel, off
 
 
+def _lists(kind, n, off):
+    """(selection row, pair, candidate range) of every list of a kind."""
+    if kind < 3:
+        return [(kind * n + i, i, off[kind, i], off[kind, i + 1]) for i in range(n)]
+    out = []
+    for i in range(n):
+        a, b = off[kind, i], off[kind, i + 1]
+        h = (b - a) // 2
+        out += [(3 * n + 2 * i, i, a, a + h), (3 * n + 2 * i + 1, i, a + h, b)]
+    return out
+
+
 def test_selection_matches_oracle():
     pairs = W.batch(48, 40, 200, seed=12, sigma_lo=5.0, sigma_hi=14.0)
     blob = _blob(7)
@@ -232,12 +244,15 @@ def test_selection_matches_oracle():
         (sc, _, _), stats, score, sel, off = _learned_run(pairs, blob, k, margin, audit, seed)
         for kind in range(ia.CAND_KINDS):
             gated = 0
-            for i in range(len(pairs)):
-                s = score[off[kind, i]:off[kind, i + 1]]
-                row = sel[kind, i]
+            for r, i, a, b in _lists(kind, len(pairs), off):
+                row = sel[r]
                 if row[0] == -1 and (row[1:] == -1).all():
-                    continue  # pass not run for this pair (or at most k candidates)
+                    continue  # pass not run for this list (or at most k candidates)
                 gated += 1
+                s = score[a:b]
+                if kind == 3:  # the slot's last detailed search: scores up to its seed count
+                    fin = np.isfinite(s)
+                    s = s[:int(np.argmin(fin)) if not fin.all() else s.size]
                 c, lst = ro.select(s, k, margin, audit, seed, i)
                 assert row[0] == c, (kind, i, k, margin, audit)
                 assert list(row[1:1 + k]) == lst
@@ -278,15 +293,15 @@ def test_trained_ranker_beats_untrained(shipped):
     def hit_rate(blob):
         (_, _, _), _, score, sel, _ = _learned_run(pairs, blob, 8, -1.0, 0.0, 0)
         hits = tot = 0
-        for kind in range(ia.CAND_KINDS):
-            for i in range(len(pairs)):
-                if sel[kind, i, 0] != 8:
+        for kind in range(3):  # rescue passes: the same candidates in both runs
+            for r, i, a, b in _lists(kind, len(pairs), off):
+                if sel[r, 0] != 8:
                     continue
-                lab = label[off[kind, i]:off[kind, i + 1]]
+                lab = label[a:b]
                 if np.isnan(lab).any():
                     continue
                 tot += 1
-                hits += lab[sel[kind, i, 1:9]].max() >= lab.max() - 1e-3
+                hits += lab[sel[r, 1:9]].max() >= lab.max() - 1e-3
         return hits / max(tot, 1), tot
 
     h_tr, n_tr = hit_rate(shipped)

@@ -88,12 +88,18 @@ def test_bf16_rounding_is_nearest_even():
 @pytest.mark.parametrize("plen,nlen", [(3, 50), (4, 4), (40, 38), (64, 64), (170, 165), (300, 290),
                                        (380, 420), (999, 960)])
 def test_candidate_schedules_match_library(plen, nlen):
-    for kind in range(ia.CAND_KINDS):
+    for kind in range(3):
         cs = ro.candidates(plen, nlen, kind)
         assert len(cs) == ia.candidate_count(plen, nlen, kind), kind
         for flen, ps, ns in cs:
             assert 3 <= flen <= min(plen, nlen) and ps + flen <= plen and ns + flen <= nlen
-    assert ia.candidate_count(plen, nlen, 3) == 0 and ia.candidate_count(-1, nlen, 0) == 0
+    # detailed searches: two slots, each room for the largest aligned set
+    m = min(plen, nlen)
+    room = max([len(ro.det_seeds(k)) for k in range(m + 1)])
+    assert ia.candidate_count(plen, nlen, ia.CAND_DET) == 2 * room
+    for flen, ps, ns in ro.det_seeds(m):
+        assert flen >= 3 and ps == ns and ps + flen <= m
+    assert ia.candidate_count(plen, nlen, 4) == 0 and ia.candidate_count(-1, nlen, 0) == 0
 
 
 def test_pair_rows_pairs_within_groups():
