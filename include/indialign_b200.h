@@ -141,6 +141,8 @@ typedef struct {
                                 per-candidate outputs */
     float *win_score;        /* optional out [candidates] (LEARNED, or COLLECT with a
                                 ranker): predicted score of every candidate */
+    int rank_mask;           /* LEARNED / COLLECT: INDIALIGN_RANK_* bits of the lists
+                                to rank (0: INDIALIGN_RANK_DEFAULT) */
     int *win_select;         /* optional out [5*n_pairs][33] (LEARNED): rows per kind
                                 back to back (n_pairs each, 2*n_pairs alignment
                                 slots for detailed searches, the batch's last one):
@@ -156,6 +158,17 @@ typedef struct {
 #define INDIALIGN_CAND_THREAD 1  /* threading-DP offsets (rescue.h:121-190) */
 #define INDIALIGN_CAND_DENSE 2   /* dense local-fragment windows */
 #define INDIALIGN_CAND_DET 3     /* detailed-search fragment seeds (align.h:15-50) */
+#define INDIALIGN_RANK_LOCAL 1   /* local-fragment windows */
+#define INDIALIGN_RANK_THREAD 2  /* threading-DP offsets */
+#define INDIALIGN_RANK_DENSE 4   /* dense local-fragment windows */
+#define INDIALIGN_RANK_DET_SS 8  /* detailed searches of the SS seeds (ss.h:87-164) */
+#define INDIALIGN_RANK_DET_DP 16 /* detailed searches of the final dp_refine (indialign.cpp:188-193) */
+/* default: every list but the final dp_refine's detailed searches, which
+ * stay exhaustive so that the final refinement of the best transform is the
+ * plain search's (measured: pruning them too costs most of the worst-case
+ * TM-score loss for a few percent of speed) */
+#define INDIALIGN_RANK_DEFAULT (INDIALIGN_RANK_LOCAL | INDIALIGN_RANK_THREAD | INDIALIGN_RANK_DENSE | \
+                                INDIALIGN_RANK_DET_SS)
 #define INDIALIGN_RANKER_FLOATS 18849
 #define INDIALIGN_RANK_STATS 32
 

@@ -28,6 +28,7 @@ KERNEL_MS = 6
 MODE_PLAIN, MODE_LEARNED, MODE_COLLECT = 0, 1, 2
 CAND_LOCAL, CAND_THREAD, CAND_DENSE, CAND_DET = 0, 1, 2, 3
 CAND_KINDS = 4
+RANK_LOCAL, RANK_THREAD, RANK_DENSE, RANK_DET_SS, RANK_DET_DP = 1, 2, 4, 8, 16
 CAND_NAMES = ("local", "threading", "dense", "detailed")
 RANKER_FLOATS = 18849
 RANK_STATS = 32
@@ -60,6 +61,7 @@ class BatchOptions(ctypes.Structure):
                 ("win_label", ctypes.POINTER(ctypes.c_float)),
                 ("win_cap", ctypes.c_longlong),
                 ("win_score", ctypes.POINTER(ctypes.c_float)),
+                ("rank_mask", ctypes.c_int),
                 ("win_select", ctypes.POINTER(ctypes.c_int))]
 
 
@@ -132,7 +134,7 @@ def _fptr(a: np.ndarray):
 
 def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, margin: float = 0.02,
                     audit_rate: float = 0.02, seed: int = 0,
-                    rank_stats: np.ndarray | None = None) -> BatchOptions:
+                    rank_stats: np.ndarray | None = None, rank_mask: int = 0) -> BatchOptions:
     """Fill the learned-mode fields of `opts` (keeps `ranker` referenced by
     the caller, which must outlive the call)."""
     assert ranker.dtype == np.float32 and ranker.size == RANKER_FLOATS and ranker.flags.c_contiguous
@@ -142,6 +144,7 @@ def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, marg
     opts.margin = float(margin)
     opts.audit_rate = float(audit_rate)
     opts.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    opts.rank_mask = int(rank_mask)
     if rank_stats is not None:
         assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [4][8]
         opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))

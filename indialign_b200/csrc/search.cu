@@ -160,7 +160,7 @@ struct Cfg {
     int use_frag, max_iter, dp_iter;
     double r1, r2, early;
     // dense-rescue mode (INDIALIGN_MODE_*) and ranker selection parameters
-    int mode = INDIALIGN_MODE_PLAIN, top_k = 8;
+    int mode = INDIALIGN_MODE_PLAIN, top_k = 8, rank_mask = INDIALIGN_RANK_DEFAULT;
     double margin = 0.02, audit = 0.02;
     unsigned long long seed = 0;
 };
@@ -229,10 +229,21 @@ class Runner {
     int ntasks(int kind) const { return kind == CAND_DET ? kDetSlots * n_ : n_; }
     // first selection row of a kind in the win_select output (kinds back to back)
     long long sel_row(int kind) const { return kind == CAND_DET ? 3LL * n_ : (long long)kind * n_; }
-    const int *sel_count() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wcount.p : nullptr; }
-    const int *sel_list() const { return cfg_.mode == INDIALIGN_MODE_LEARNED ? c_->wlist.p : nullptr; }
+    // ranked candidate lists this call: bit of INDIALIGN_RANK_* per pass
+    int rank_bit(int kind, int det_ss) const {
+        return kind == CAND_DET ? (det_ss ? INDIALIGN_RANK_DET_SS : INDIALIGN_RANK_DET_DP) : (1 << kind);
+    }
+    bool ranked(int kind, int det_ss = 0) const {
+        return cfg_.mode != INDIALIGN_MODE_PLAIN && (cfg_.rank_mask & rank_bit(kind, det_ss)) != 0;
+    }
+    const int *sel_count(int kind, int det_ss = 0) const {
+        return cfg_.mode == INDIALIGN_MODE_LEARNED && ranked(kind, det_ss) ? c_->wcount.p : nullptr;
+    }
+    const int *sel_list(int kind, int det_ss = 0) const {
+        return cfg_.mode == INDIALIGN_MODE_LEARNED && ranked(kind, det_ss) ? c_->wlist.p : nullptr;
+    }
     int glue(int op, double thr = 0.0, const double *recs = nullptr, const int *idx = nullptr);
-    int dp_full();
+    int dp_full(int det_ss);
 
     Ctx *c_;
     Cfg cfg_;
@@ -550,13 +561,15 @@ static CandRes det_res(Ctx *c) {
 // dp_refine with fragment detailed searches (indialign_c/align.h:54-145,
 // d0_search_lite = false): per iteration one NW per gap chain, then the
 // detailed bank on each alignment, then the per-chain update.
-int Runner::dp_full() {
+int Runner::dp_full(int det_ss) {
     int rc;
     for (int it = 0; it < cfg_.dp_iter; it++) {
         if ((rc = chain(CH_DP_EMIT, L_pair, 1, nullptr, nullptr, false))) return rc;
-        if ((rc = rank_stage(CAND_DET, 0))) return rc;
-        if ((rc = bank(BK_DET_DP, L_detdp, nullptr, -1, -1, sel_count(), sel_list()))) return rc;
-        if ((rc = after_stage(CAND_DET, det_res(c_), 0))) return rc;
+        if ((rc = rank_stage(CAND_DET, det_ss))) return rc;
+        if ((rc = bank(BK_DET_DP, L_detdp, nullptr, -1, -1, sel_count(CAND_DET, det_ss),
+                       sel_list(CAND_DET, det_ss))))
+            return rc;
+        if ((rc = after_stage(CAND_DET, det_res(c_), det_ss))) return rc;
         if ((rc = glue(G_DP_STEP))) return rc;
     }
     return glue(G_DP_END);
@@ -581,7 +594,7 @@ RankArgs Runner::rank_args(int kind, int det_ss) {
 }
 
 int Runner::rank_stage(int kind, int det_ss) {
-    if (cfg_.mode == INDIALIGN_MODE_PLAIN) return INDIALIGN_OK;
+    if (!ranked(kind, det_ss)) return INDIALIGN_OK;
     cudaStream_t st = c_->stream;
     const RankArgs ra = rank_args(kind, det_ss);
     if (kind == CAND_DET) {  // a slot's arrays hold its last search only (NaN beyond its seeds)
@@ -631,6 +644,7 @@ SelectArgs Runner::select_args(int kind, int det_ss) {
 // After a ranked pass: LEARNED checks the audited tasks, COLLECT records
 // every candidate's refined score.
 int Runner::after_stage(int kind, const CandRes &r, int det_ss) {
+    if (!ranked(kind, det_ss)) return INDIALIGN_OK;
     cudaStream_t st = c_->stream;
     if (cfg_.mode == INDIALIGN_MODE_LEARNED) {
         launch_audit(b, select_args(kind, det_ss), r, st);
@@ -668,18 +682,18 @@ int Runner::run_stages() {
     RUN(glue(G_SS_BEGIN));
     RUN(chain(CH_SS2, L_pair, 1, nullptr, nullptr, false));
     RUN(rank_stage(CAND_DET, 1));
-    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(), sel_list()));
+    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(CAND_DET, 1), sel_list(CAND_DET, 1)));
     RUN(after_stage(CAND_DET, det_res(c_), 1));
     RUN(glue(G_SS_DET));
-    RUN(dp_full());
+    RUN(dp_full(1));
     RUN(glue(G_SS_DP));
     RUN(glue(G_SS4_START));
     RUN(chain(CH_SS4, L_pair, 1, nullptr, nullptr, false));
     RUN(rank_stage(CAND_DET, 1));
-    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(), sel_list()));
+    RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(CAND_DET, 1), sel_list(CAND_DET, 1)));
     RUN(after_stage(CAND_DET, det_res(c_), 1));
     RUN(glue(G_SS_DET));
-    RUN(dp_full());
+    RUN(dp_full(1));
     RUN(glue(G_SS_DP));
     launch_rescore(b, REC_SS, 0, st);
     launches_++;
@@ -692,7 +706,7 @@ int Runner::run_stages() {
     // 3. rescue ladder (indialign.cpp:125-152)
     RUN(glue(G_GATE, cfg_.r1));
     RUN(rank_stage(CAND_LOCAL));
-    RUN(chain(CH_LOCAL, L_localn, 0, nullptr, nullptr, true, sel_count(), sel_list()));
+    RUN(chain(CH_LOCAL, L_localn, 0, nullptr, nullptr, true, sel_count(CAND_LOCAL), sel_list(CAND_LOCAL)));
     RUN(after_stage(CAND_LOCAL, CandRes{c_->chain_res.p, L_localn.d_base, nullptr, nullptr, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
@@ -700,7 +714,7 @@ int Runner::run_stages() {
     mark(3);
     RUN(glue(G_GATE, cfg_.r1));
     RUN(rank_stage(CAND_THREAD));
-    RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p, -1, -1, sel_count(), sel_list()));
+    RUN(bank(BK_THREAD, L_thread, c_->thread_rec.p, -1, -1, sel_count(CAND_THREAD), sel_list(CAND_THREAD)));
     RUN(chain(CH_THREAD, L_threadch, 1, c_->thread_rec.p));
     RUN(after_stage(CAND_THREAD,
                     CandRes{c_->chain_res.p, L_threadch.d_base, c_->thread_rec.p, L_threadch.d_aux, nullptr, nullptr}));
@@ -710,7 +724,7 @@ int Runner::run_stages() {
     mark(4);
     RUN(glue(G_GATE, cfg_.r2));
     RUN(rank_stage(CAND_DENSE));
-    RUN(chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, sel_count(), sel_list()));
+    RUN(chain(CH_LOCAL, L_locald, 1, nullptr, nullptr, true, sel_count(CAND_DENSE), sel_list(CAND_DENSE)));
     RUN(after_stage(CAND_DENSE, CandRes{c_->chain_res.p, L_locald.d_base, nullptr, nullptr, nullptr, nullptr}));
     launch_rescore(b, REC_STAGE, 1, st);
     launches_++;
@@ -724,7 +738,7 @@ int Runner::run_stages() {
     mark(6);
     // 5. DP refinement (indialign.cpp:179-228)
     RUN(glue(G_DPF_BEGIN));
-    RUN(dp_full());
+    RUN(dp_full(0));
     launch_rescore(b, REC_DP, 0, st);
     launches_++;
     RUN(glue(G_DPF_UPDATE));
@@ -1112,6 +1126,7 @@ static Cfg make_cfg(const NativeConfig *cfg, const IndialignBatchOptions *opts) 
         c.margin = opts->margin;
         c.audit = opts->audit_rate;
         c.seed = opts->seed;
+        c.rank_mask = opts->rank_mask ? opts->rank_mask : INDIALIGN_RANK_DEFAULT;
     }
     return c;
 }
