@@ -72,6 +72,9 @@ def workload(name: str, step_pairs: int, n_steps: int, rank: int = 0):
     elif name == "hard1024":
         pairs = W.hard(1024, seed=2 + 1000 * rank)
         desc = "hard1024: 1024 pairs, L log-uniform 30..1500, half hard (30-60% stems kept)"
+    elif name.startswith("batch") and name[5:].isdigit():
+        pairs = W.parallel_batch(int(name[5:]), 40, 300, seed=1 + 1000 * rank)
+        desc = f"{name}: {len(pairs)} pairs, L~U(40,300), sigma~U(0.5,14), 5% invalid per mask"
     else:
         raise SystemExit(f"unknown workload {name}")
     batches = [pairs[(k * step_pairs) % len(pairs):(k * step_pairs) % len(pairs) + step_pairs]
@@ -216,6 +219,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="learned16384")
+    ap.add_argument("--mode", default="learned", choices=["learned", "plain"],
+                    help="search timed for `value`; with learned, the plain search is timed beside it")
     ap.add_argument("--step-pairs", type=int, default=2048)
     ap.add_argument("--top-k", type=int, default=8)
     ap.add_argument("--margin", type=float, default=0.02)
@@ -314,8 +319,9 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    learned_mode = args.mode == "learned"
     clk = Clocks(local)
-    lrn = run_mode(True, clk)
+    lrn = run_mode(learned_mode, clk)
     clocks = clk.summary()
     n_timed = sum(dev[args.warmup + k].n for k in range(args.steps))
     l_ms = max_over_ranks(float(np.sum(lrn["ms"])))
@@ -323,7 +329,7 @@ def main():
     l_scores = np.concatenate(lrn["scores"])
 
     plain = None
-    if not args.no_plain:
+    if learned_mode and not args.no_plain:
         pl = run_mode(False)
         p_ms = max_over_ranks(float(np.sum(pl["ms"])))
         p_scores = np.concatenate(pl["scores"])
@@ -343,7 +349,7 @@ def main():
     # end to end: the learned search through the C-ABI batch entry with host buffers
     e2e = None
     if not args.no_e2e:
-        eo = make_opts(True)
+        eo = make_opts(learned_mode)
         eo.kernel_ms = eo.counters = eo.stage_ms = None
         packs = [abi.PackedInputs(b) for b in batches[args.warmup:args.warmup + args.steps]]
         res = [(abi.NativePairResult * p.n)() for p in packs]
@@ -410,7 +416,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": desc, "step_pairs": args.step_pairs, "pairs_timed_per_gpu": n_timed,
-                           "mode": f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit})",
+                           "mode": (f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit})"
+                                    if learned_mode else "plain"),
                            "ranker": "indialign_b200/ranker_weights.npy",
                            "l2": "flushed by a 256 MB write before every step",
                            "parallelism": f"independent pairs per GPU x{world}"},
