@@ -92,7 +92,7 @@ int indialign_cuda_available(void);
 typedef struct {
     void *stream;            /* cudaStream_t to run on (NULL: library stream) */
     int device;              /* CUDA device ordinal (-1: current) */
-    int use_graph;           /* capture the stage sequence in a CUDA graph and replay it */
+    int use_graph;           /* reserved: accepted and ignored (the stage kernels are persistent) */
     int profile;             /* 1: print per-stage device times to stderr */
     double *stage_ms;        /* optional [INDIALIGN_STAGES] per-stage device ms:
                                 seeds, seed bank, SS, gapless, local fragment,
