@@ -193,6 +193,21 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+def reduce_max(dist, x: float, device: str) -> float:
+    """Max of a per-rank time over all ranks (identity without a process
+    group); every rank calls it at the same point."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(pairs_per_rank: int, world: int, max_ms: float) -> float:
+    """pairs/s of the whole job: every rank's pairs over the slowest rank's time."""
+    return pairs_per_rank * world / (max_ms / 1e3)
+
+
 class DeviceBatch:
     """One batch packed back to back in HBM (torch tensors as plumbing)."""
 
@@ -314,10 +329,7 @@ def main():
         return rec
 
     def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        if dist:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(dist, x, "cuda")
 
     learned_mode = args.mode == "learned"
     clk = Clocks(local)
@@ -325,7 +337,7 @@ def main():
     clocks = clk.summary()
     n_timed = sum(dev[args.warmup + k].n for k in range(args.steps))
     l_ms = max_over_ranks(float(np.sum(lrn["ms"])))
-    value = n_timed * world / (l_ms / 1e3)
+    value = whole_job_rate(n_timed, world, l_ms)
     l_scores = np.concatenate(lrn["scores"])
 
     plain = None
