@@ -198,6 +198,17 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
                                     const double *lnorm, const NativeConfig *cfg,
                                     const IndialignBatchOptions *opts, double *d_out);
 
+/* Padded device batch, the (B, N, 3) shape of the reference's torch scorer
+ * (scoring/_tmscore_gpu/search.py:492-540): row p of d_pred / d_nat [B*N*3]
+ * and of the masks d_v / d_pv / d_nv [B*N] holds pair p in its first
+ * lengths[p] (host array, 1..N) residues; lnorm[B] host array; results
+ * {score, R[9], t[3]} to d_out [B*13] on the device.  The search of each pair
+ * is the reference's (only the first lengths[p] residues take part). */
+int indialign_tmscore_search_padded(int n_pairs, int N, const int *lengths, const double *d_pred,
+                                    const double *d_nat, const uint8_t *d_v, const uint8_t *d_pv,
+                                    const uint8_t *d_nv, const double *lnorm, const NativeConfig *cfg,
+                                    const IndialignBatchOptions *opts, double *d_out);
+
 /* Needleman-Wunsch alignment of one explicit score matrix; replaces the
  * reference's nw_dp + nw_traceback pair (indialign_c/nw.h:10-68): zero
  * boundaries, a gap move out of a diagonally reached cell pays `gap`, ties

@@ -97,6 +97,11 @@ def load(path: str | None = None) -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(NativeConfig),
         ctypes.POINTER(BatchOptions), ctypes.c_void_p]
     lib.indialign_tmscore_search_device.restype = ctypes.c_int
+    lib.indialign_tmscore_search_padded.argtypes = [
+        ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+        ctypes.POINTER(NativeConfig), ctypes.POINTER(BatchOptions), ctypes.c_void_p]
+    lib.indialign_tmscore_search_padded.restype = ctypes.c_int
     lib.indialign_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.indialign_fp64_peak.restype = ctypes.c_int
     lib.indialign_candidate_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
@@ -251,6 +256,48 @@ def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None,
         raise IndialignError(f"indialign_tmscore_search_batch_ex(collect) rc={rc}: {last_error()}")
     out = (abi.results_to_numpy(res, pk.n), feat[:W], label[:W], woff)
     return out + (score[:W],) if ranker is not None else out
+
+
+def search_tensors(pred, native, valid=None, pred_valid=None, native_valid=None, lengths=None,
+                   lnorm=None, cfg: NativeConfig | None = None, ranker: np.ndarray | None = None,
+                   top_k: int = 8, margin: float = 0.02, audit_rate: float = 0.02, seed: int = 0):
+    """Search a padded batch of CUDA tensors, the (B, N, 3) shape of the
+    reference's torch scorer: pred / native (B, N, 3), masks (B, N) (bool or
+    uint8; pred_valid / native_valid default to valid, valid to all ones),
+    lengths (B,) residues in use per row (default N), lnorm (B,) (default the
+    lengths).  Runs on the current torch stream; returns torch tensors
+    score (B,), R (B, 9), t (B, 3) on the device.  float64 contiguous inputs
+    are read in place."""
+    import torch
+    lib = load()
+    cfg = cfg or default_config()
+    if pred.ndim != 3 or pred.shape != native.shape or pred.shape[2] != 3 or not pred.is_cuda:
+        raise ValueError("pred and native must be matching (B, N, 3) CUDA tensors")
+    B, N, _ = pred.shape
+    dev = pred.device
+    P = pred.to(torch.float64).contiguous()
+    Q = native.to(torch.float64).contiguous()
+    ones = torch.ones((B, N), dtype=torch.uint8, device=dev)
+    V = ones if valid is None else valid.to(device=dev, dtype=torch.uint8).contiguous()
+    PV = V if pred_valid is None else pred_valid.to(device=dev, dtype=torch.uint8).contiguous()
+    NV = V if native_valid is None else native_valid.to(device=dev, dtype=torch.uint8).contiguous()
+    lens = np.full(B, N, np.int32) if lengths is None else np.ascontiguousarray(
+        torch.as_tensor(lengths).cpu().numpy(), np.int32)
+    ln = lens.astype(np.float64) if lnorm is None else np.ascontiguousarray(
+        torch.as_tensor(lnorm).cpu().numpy(), np.float64)
+    out = torch.empty((B, 13), dtype=torch.float64, device=dev)
+    opts = BatchOptions()
+    opts.device = dev.index if dev.index is not None else -1
+    opts.stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    if ranker is not None:
+        learned_options(opts, ranker, top_k, margin, audit_rate, seed)
+    rc = lib.indialign_tmscore_search_padded(
+        B, N, lens.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), P.data_ptr(), Q.data_ptr(), V.data_ptr(),
+        PV.data_ptr(), NV.data_ptr(), ln.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(cfg),
+        ctypes.byref(opts), out.data_ptr())
+    if rc != 0:
+        raise IndialignError(f"indialign_tmscore_search_padded rc={rc}: {last_error()}")
+    return out[:, 0], out[:, 1:10], out[:, 10:13]
 
 
 def fp64_peak_tflops(device: int = 0) -> float:

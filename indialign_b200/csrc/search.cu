@@ -807,8 +807,11 @@ struct Source {
     const int *off = nullptr;
     const double *pred = nullptr, *nat = nullptr, *lnorm = nullptr;
     const uint8_t *v = nullptr, *pv = nullptr, *nv = nullptr;
+    const int *lens = nullptr;  // optional lengths (padded rows: off[p] = p * N)
     int n() const { return host.empty() ? n_dev : (int)host.size(); }
-    int len(int p) const { return host.empty() ? off[p + 1] - off[p] : host[p]->length; }
+    int len(int p) const {
+        return host.empty() ? (lens ? lens[p] : off[p + 1] - off[p]) : host[p]->length;
+    }
 };
 
 // Inputs -> packed device batch; runs the search; writes {score,R,t} per
@@ -1328,6 +1331,52 @@ int indialign_candidate_count(int plen, int nlen, int kind) {
     if (plen < 0 || nlen < 0 || kind < 0 || kind >= ia::kCandKinds) return 0;
     if (kind == ia::CAND_DET) return ia::kDetSlots * ia::kdet_max(plen < nlen ? plen : nlen);
     return ia::cand_count(kind, plen, nlen);
+}
+
+int indialign_tmscore_search_padded(int n_pairs, int N, const int *lengths, const double *d_pred,
+                                    const double *d_nat, const uint8_t *d_v, const uint8_t *d_pv,
+                                    const uint8_t *d_nv, const double *lnorm, const NativeConfig *cfg,
+                                    const IndialignBatchOptions *opts, double *d_out) {
+    ia::g_last_error.clear();
+    if (ia::g_inject.load() > 0) {
+        ia::g_inject.fetch_sub(1);
+        ia::g_last_error = "injected failure";
+        return INDIALIGN_E_INJECTED;
+    }
+    if (n_pairs <= 0) return INDIALIGN_OK;
+    if (!lengths || !d_pred || !d_nat || !d_v || !d_pv || !d_nv || !lnorm || !cfg || !d_out || N < 1 ||
+        N > 65535) {
+        ia::g_last_error = "padded: null pointer or row length outside 1..65535";
+        return INDIALIGN_E_INPUT;
+    }
+    for (int p = 0; p < n_pairs; p++)
+        if (lengths[p] < 1 || lengths[p] > N) {
+            ia::g_last_error = "pair " + std::to_string(p) + ": length must be in 1..N";
+            return INDIALIGN_E_INPUT;
+        }
+    if (int rc = ia::check_mode(opts)) return rc;
+    std::vector<int> off((size_t)n_pairs + 1);
+    for (int p = 0; p <= n_pairs; p++) off[p] = p * N;
+    if ((long long)n_pairs * N > 0x7fffffffLL) {
+        ia::g_last_error = "padded: batch too large";
+        return INDIALIGN_E_INPUT;
+    }
+    ia::Source src;
+    src.n_dev = n_pairs;
+    src.off = off.data();
+    src.lens = lengths;
+    src.pred = d_pred;
+    src.nat = d_nat;
+    src.v = d_v;
+    src.pv = d_pv;
+    src.nv = d_nv;
+    src.lnorm = lnorm;
+    ia::Ctx *c = nullptr;
+    int rc = ia::acquire(opts ? opts->device : -1, &c);
+    if (rc) return rc;
+    rc = ia::run_batch(c, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
+    ia::release(c);
+    return rc;
 }
 
 const char *indialign_last_error(void) { return ia::g_last_error.c_str(); }

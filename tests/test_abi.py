@@ -107,3 +107,17 @@ def test_no_device_fails_loudly():
     assert ia.load().indialign_cuda_available() == 0
     with pytest.raises(ia.IndialignError, match="rc=-2"):
         ia.search(W.single(0))
+
+
+def test_padded_entry_rejects_bad_lengths_before_device_work():
+    lib = ia.load()
+    cfg = ia.default_config()
+    lens = (ctypes.c_int * 2)(10, 40)
+    ln = (ctypes.c_double * 2)(10.0, 40.0)
+    dummy = ctypes.c_void_p(16)  # never dereferenced: validation fails first
+    rc = lib.indialign_tmscore_search_padded(2, 32, lens, dummy, dummy, dummy, dummy, dummy, ln,
+                                             ctypes.byref(cfg), None, dummy)
+    assert rc == -4 and "length" in ia.last_error()
+    rc = lib.indialign_tmscore_search_padded(2, 0, lens, dummy, dummy, dummy, dummy, dummy, ln,
+                                             ctypes.byref(cfg), None, dummy)
+    assert rc == -4

@@ -309,3 +309,31 @@ def test_trained_ranker_beats_untrained(shipped):
     h_un, _ = hit_rate(untrained)
     assert n_tr >= 10
     assert h_tr >= h_un + 0.15, (h_tr, h_un)
+
+
+def test_learned_mode_with_full_fallback_is_the_plain_search():
+    """With every list falling back (margin above any score gap) or no list
+    ranked, the learned search refines every candidate in the plain order:
+    results are bit-identical to the plain search."""
+    pairs = W.batch(32, 40, 200, seed=21, sigma_lo=4.0, sigma_hi=14.0)
+    s0, R0, t0 = ia.search(pairs)
+    blob = _blob(9)
+    for mask, margin in ((0, 1e9), (32, 0.0)):
+        lib = ia.load()
+        pk = abi.PackedInputs(pairs)
+        res = (abi.NativePairResult * pk.n)()
+        opts = ia.BatchOptions()
+        opts.device = -1
+        stats = np.zeros(ia.RANK_STATS, np.int64)
+        ia.learned_options(opts, blob, 8, margin, 0.0, 0, stats, mask)
+        cfg = ia.default_config()
+        assert lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res) == 0
+        s, R, t = abi.results_to_numpy(res, pk.n)
+        np.testing.assert_array_equal(s, s0)
+        np.testing.assert_array_equal(R, R0)
+        np.testing.assert_array_equal(t, t0)
+        st = stats.reshape(ia.CAND_KINDS, 8)
+        if mask == 0:
+            assert st[:, 0].sum() > 0 and st[:, 3].sum() == 0  # ranked, never pruned
+        else:
+            assert st.sum() == 0

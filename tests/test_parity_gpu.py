@@ -179,3 +179,29 @@ def test_nw_explicit_bit_exact_vs_reference():
         np.testing.assert_array_equal(an[:n].cpu().numpy(), z[f"an{k}"], err_msg=f"case {k}")
         k += 1
     assert k >= 90
+
+
+def test_padded_tensor_entry_matches_host_entry():
+    """The (B, N, 3) padded-tensor entry gives the same results as the host
+    batch entry on the same pairs (padding rows hold garbage on purpose)."""
+    import torch
+    pairs = W.batch(6, 40, 120, seed=99)
+    s_h, R_h, t_h = ia.search(pairs)
+    N = max(p.pred.shape[0] for p in pairs) + 7
+    B = len(pairs)
+    rng = np.random.default_rng(0)
+    P = rng.normal(0, 50, (B, N, 3))
+    Q = rng.normal(0, 50, (B, N, 3))
+    V, PV, NV = (np.ones((B, N), np.uint8) for _ in range(3))
+    lens = np.zeros(B, np.int32)
+    for i, p in enumerate(pairs):
+        L = p.pred.shape[0]
+        lens[i] = L
+        P[i, :L], Q[i, :L] = p.pred, p.native
+        V[i, :L], PV[i, :L], NV[i, :L] = p.valid, p.pred_valid, p.native_valid
+    t = lambda a: torch.tensor(a, device="cuda")
+    s, R, tt = ia.search_tensors(t(P), t(Q), t(V), t(PV), t(NV), lengths=lens,
+                                 lnorm=np.array([p.lnorm for p in pairs]))
+    np.testing.assert_array_equal(s.cpu().numpy(), s_h)
+    np.testing.assert_array_equal(R.cpu().numpy(), R_h)
+    np.testing.assert_array_equal(tt.cpu().numpy(), t_h)
