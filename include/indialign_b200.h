@@ -143,6 +143,9 @@ typedef struct {
                                 ranker): predicted score of every candidate */
     int rank_mask;           /* LEARNED / COLLECT: INDIALIGN_RANK_* bits of the lists
                                 to rank (0: INDIALIGN_RANK_DEFAULT) */
+    int rank_min_len;        /* LEARNED: pairs with fewer valid pred or native
+                                residues refine every candidate (0:
+                                INDIALIGN_RANK_MIN_LEN; negative: rank all) */
     int *win_select;         /* optional out [5*n_pairs][33] (LEARNED): rows per kind
                                 back to back (n_pairs each, 2*n_pairs alignment
                                 slots for detailed searches, the batch's last one):
@@ -169,6 +172,9 @@ typedef struct {
  * TM-score loss for a few percent of speed) */
 #define INDIALIGN_RANK_DEFAULT (INDIALIGN_RANK_LOCAL | INDIALIGN_RANK_THREAD | INDIALIGN_RANK_DENSE | \
                                 INDIALIGN_RANK_DET_SS)
+/* short pairs cost little and lose most from pruning (measured on the hard
+ * workload: the worst TM-score changes were pairs of L < 50) */
+#define INDIALIGN_RANK_MIN_LEN 100
 #define INDIALIGN_RANKER_FLOATS 18849
 #define INDIALIGN_RANK_STATS 32
 

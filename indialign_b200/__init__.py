@@ -62,6 +62,7 @@ class BatchOptions(ctypes.Structure):
                 ("win_cap", ctypes.c_longlong),
                 ("win_score", ctypes.POINTER(ctypes.c_float)),
                 ("rank_mask", ctypes.c_int),
+                ("rank_min_len", ctypes.c_int),
                 ("win_select", ctypes.POINTER(ctypes.c_int))]
 
 
@@ -139,7 +140,8 @@ def _fptr(a: np.ndarray):
 
 def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, margin: float = 0.02,
                     audit_rate: float = 0.02, seed: int = 0,
-                    rank_stats: np.ndarray | None = None, rank_mask: int = 0) -> BatchOptions:
+                    rank_stats: np.ndarray | None = None, rank_mask: int = 0,
+                    rank_min_len: int = 0) -> BatchOptions:
     """Fill the learned-mode fields of `opts` (keeps `ranker` referenced by
     the caller, which must outlive the call)."""
     assert ranker.dtype == np.float32 and ranker.size == RANKER_FLOATS and ranker.flags.c_contiguous
@@ -150,6 +152,7 @@ def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, marg
     opts.audit_rate = float(audit_rate)
     opts.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     opts.rank_mask = int(rank_mask)
+    opts.rank_min_len = int(rank_min_len)
     if rank_stats is not None:
         assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [4][8]
         opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))

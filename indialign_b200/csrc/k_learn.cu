@@ -290,7 +290,9 @@ __global__ void k_plan_rank(DevBatch b, RankArgs a, int *counts) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.ntasks) return;
     const RankTask r = rank_task(b, a, t);
-    counts[t] = r.on && r.W > 0 ? (r.W + kRankChunk - 1) / kRankChunk : 0;
+    const PairInfo &I = b.info[r.p];
+    const bool small = (I.plen < I.nlen ? I.plen : I.nlen) < a.min_len;
+    counts[t] = r.on && !small && r.W > 0 ? (r.W + kRankChunk - 1) / kRankChunk : 0;
 }
 
 __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int *__restrict__ chunk_begin,
@@ -381,7 +383,8 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
         atomicAdd(a.stats + RS_GATED, 1ull);
         atomicAdd(a.stats + RS_WINDOWS, (unsigned long long)W);
     }
-    if (W <= k) {
+    const PairInfo &I = b.info[p];
+    if (W <= k || (I.plen < I.nlen ? I.plen : I.nlen) < a.task.min_len) {  // short list or short pair
         list[lane] = -1;
         if (lane == 0) {
             a.wcount[t] = -1;

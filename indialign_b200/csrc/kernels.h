@@ -128,6 +128,8 @@ struct RankArgs {
     int det_ss;                // CAND_DET: the SS detailed search (slot 0 under the
                                // stage flag) instead of dp_refine's (active slots)
     const double *alP, *alQ;   // CAND_DET: aligned coordinates (2 slots per pair)
+    int min_len;               // LEARNED: pairs with min(plen, nlen) below this refine
+                               // every candidate (not ranked); 0 in COLLECT
 };
 
 struct SelectArgs {

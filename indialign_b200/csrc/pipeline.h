@@ -202,7 +202,8 @@ enum RankStat {
     RS_WINDOWS,        // windows of the gated pairs
     RS_REFINED,        // windows refined
     RS_AUDIT_MISS,     // audited pairs whose top-k windows miss the best window score
-    RS_SMALL,          // gated pairs with at most k windows (all refined)
+    RS_SMALL,          // gated lists with at most k candidates or of a pair shorter than
+                       // the ranking length threshold (all refined)
     kRankStats
 };
 

@@ -160,7 +160,8 @@ struct Cfg {
     int use_frag, max_iter, dp_iter;
     double r1, r2, early;
     // dense-rescue mode (INDIALIGN_MODE_*) and ranker selection parameters
-    int mode = INDIALIGN_MODE_PLAIN, top_k = 8, rank_mask = INDIALIGN_RANK_DEFAULT;
+    int mode = INDIALIGN_MODE_PLAIN, top_k = 8, rank_mask = INDIALIGN_RANK_DEFAULT,
+        min_len = INDIALIGN_RANK_MIN_LEN;
     double margin = 0.02, audit = 0.02;
     unsigned long long seed = 0;
 };
@@ -590,6 +591,7 @@ RankArgs Runner::rank_args(int kind, int det_ss) {
     ra.det_ss = det_ss;
     ra.alP = c_->alP.p;
     ra.alQ = c_->alQ.p;
+    ra.min_len = cfg_.mode == INDIALIGN_MODE_LEARNED ? cfg_.min_len : 0;
     return ra;
 }
 
@@ -1130,6 +1132,7 @@ static Cfg make_cfg(const NativeConfig *cfg, const IndialignBatchOptions *opts) 
         c.audit = opts->audit_rate;
         c.seed = opts->seed;
         c.rank_mask = opts->rank_mask ? opts->rank_mask : INDIALIGN_RANK_DEFAULT;
+        c.min_len = opts->rank_min_len > 0 ? opts->rank_min_len : (opts->rank_min_len < 0 ? 0 : INDIALIGN_RANK_MIN_LEN);
     }
     return c;
 }

@@ -203,14 +203,14 @@ def test_candidate_features_match_oracle(oracle):
     assert (checked >= 20).all(), checked
 
 
-def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True):
+def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True, min_len=-1):
     lib = ia.load()
     pk = abi.PackedInputs(pairs)
     res = (abi.NativePairResult * pk.n)()
     opts = ia.BatchOptions()
     opts.device = -1
     stats = np.zeros(ia.RANK_STATS, np.int64)
-    ia.learned_options(opts, blob, k, margin, audit, seed, stats)
+    ia.learned_options(opts, blob, k, margin, audit, seed, stats, rank_min_len=min_len)
     off = ia.candidate_offsets(pairs)
     C = int(off[-1, -1])
     score = np.zeros(max(1, C), np.float32)
@@ -275,7 +275,7 @@ def test_learned_vs_plain_delta_tm(shipped):
     rescue passes refine a small fraction of their candidates."""
     pairs = W.batch(256, 40, 1000, seed=4242)
     plain, _, _ = ia.search(pairs)
-    (lsc, _, _), stats, _, _, _ = _learned_run(pairs, shipped, outputs=False)
+    (lsc, _, _), stats, _, _, _ = _learned_run(pairs, shipped, outputs=False, min_len=0)
     d = lsc - plain
     assert d.mean() >= -1e-4, d.mean()
     assert d.min() >= -1e-3, d.min()
