@@ -30,7 +30,9 @@
 
 namespace ia {
 
+#if IA_BANK_FLAT
 constexpr int kBankUnroll = IA_BANK_UNROLL;
+#endif
 
 // ---- the bank kernel -------------------------------------------------------
 struct BankSmem {
