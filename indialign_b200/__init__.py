@@ -303,6 +303,66 @@ def search_tensors(pred, native, valid=None, pred_valid=None, native_valid=None,
     return out[:, 0], out[:, 1:10], out[:, 10:13]
 
 
+def shard_pairs(pairs: Sequence, n_shards: int) -> list[list[int]]:
+    """Length-balanced split of a batch over n_shards devices: pairs sorted by
+    an L^3 work estimate (the rescue passes' NW work grows as windows x L^2),
+    each placed on the least-loaded shard (longest-processing-time greedy).
+    Returns the pair indices of every shard, ascending."""
+    n_shards = max(1, int(n_shards))
+    cost = [float(p.pred.shape[0]) ** 3 for p in pairs]
+    order = sorted(range(len(pairs)), key=lambda i: (-cost[i], i))
+    load = [0.0] * n_shards
+    out: list[list[int]] = [[] for _ in range(n_shards)]
+    for i in order:
+        k = min(range(n_shards), key=lambda j: (load[j], j))
+        out[k].append(i)
+        load[k] += cost[i]
+    return [sorted(o) for o in out]
+
+
+def search_multi(pairs: Sequence, devices: Sequence[int], cfg: NativeConfig | None = None,
+                 ranker: np.ndarray | None = None, **learned):
+    """Search a batch over several GPUs of this process: shard_pairs() split,
+    one host thread per device (each call has its own device context and
+    stream), results gathered in the batch's order.  No collective: pairs
+    are independent."""
+    import threading
+    lib = load()
+    cfg = cfg or default_config()
+    shards = shard_pairs(pairs, len(devices))
+    n = len(pairs)
+    score = np.zeros(n)
+    R = np.zeros((n, 9))
+    t = np.zeros((n, 3))
+    errors: list[str] = []
+
+    def work(dev: int, idx: list[int]):
+        if not idx:
+            return
+        sub = [pairs[i] for i in idx]
+        pk = abi.PackedInputs(sub)
+        res = (NativePairResult * pk.n)()
+        opts = BatchOptions()
+        opts.device = int(dev)
+        if ranker is not None:
+            learned_options(opts, ranker, **learned)
+        rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
+        if rc != 0:
+            errors.append(f"device {dev}: rc={rc} {last_error()}")
+            return
+        s_, R_, t_ = abi.results_to_numpy(res, pk.n)
+        score[idx], R[idx], t[idx] = s_, R_, t_
+
+    threads = [threading.Thread(target=work, args=(d, ix)) for d, ix in zip(devices, shards)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    if errors:
+        raise IndialignError("; ".join(errors))
+    return score, R, t
+
+
 def fp64_peak_tflops(device: int = 0) -> float:
     """Measured FP64 FMA throughput (TFLOP/s) of the device."""
     v = ctypes.c_double(0.0)

@@ -56,3 +56,17 @@ def test_two_gloo_ranks_shard_and_take_max_time():
     assert s0[:n] != s1[:n]                          # different pairs per rank
     assert m0 == m1 == 15.0                          # max over ranks, agreed everywhere
     assert v0 == v1 == pytest.approx(2 * 24 / 0.015)
+
+
+def test_shard_pairs_is_a_balanced_partition():
+    import indialign_b200 as ia
+    from indialign_b200 import workloads as W
+    pairs = W.batch(40, 40, 600, seed=5)
+    for k in (1, 2, 3, 8):
+        sh = ia.shard_pairs(pairs, k)
+        assert len(sh) == k
+        flat = sorted(i for s in sh for i in s)
+        assert flat == list(range(len(pairs)))
+        cost = [sum(pairs[i].pred.shape[0] ** 3 for i in s) for s in sh]
+        biggest = max(p.pred.shape[0] ** 3 for p in pairs)
+        assert max(cost) - min(cost) <= biggest  # LPT: spread below one job

@@ -205,3 +205,16 @@ def test_padded_tensor_entry_matches_host_entry():
     np.testing.assert_array_equal(s.cpu().numpy(), s_h)
     np.testing.assert_array_equal(R.cpu().numpy(), R_h)
     np.testing.assert_array_equal(tt.cpu().numpy(), t_h)
+
+
+def test_search_multi_matches_single_call():
+    """Sharded over the visible devices (listed twice to exercise concurrent
+    contexts on one GPU): same results as one batched call."""
+    import torch
+    pairs = W.batch(10, 40, 150, seed=31)
+    s0, R0, t0 = ia.search(pairs)
+    devs = list(range(torch.cuda.device_count())) * 2
+    s, R, t = ia.search_multi(pairs, devs)
+    np.testing.assert_array_equal(s, s0)
+    np.testing.assert_array_equal(R, R0)
+    np.testing.assert_array_equal(t, t0)
