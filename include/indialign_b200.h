@@ -116,8 +116,9 @@ typedef struct {
      * and in dp_refine) refines a list of fragment seeds of an alignment
      * (INDIALIGN_CAND_*).  LEARNED mode scores them with the ranker and
      * refines the top_k of each pair (of each alignment for detailed
-     * searches).  Per-candidate arrays below hold the four kinds back to
-     * back, each kind pair by pair, pair p with
+     * searches); the main seed bank's seeds can be ranked too
+     * (INDIALIGN_RANK_MAIN).  Per-candidate arrays below hold the five kinds
+     * back to back, each kind pair by pair, pair p with
      * indialign_candidate_count(plen_p, nlen_p, kind) entries (detailed
      * searches: two alignment slots of equal size; COLLECT keeps the last
      * detailed search that ran on a slot, normally dp_refine's). */
@@ -146,7 +147,7 @@ typedef struct {
     int rank_min_len;        /* LEARNED: pairs with fewer valid pred or native
                                 residues refine every candidate (0:
                                 INDIALIGN_RANK_MIN_LEN; negative: rank all) */
-    int *win_select;         /* optional out [5*n_pairs][33] (LEARNED): rows per kind
+    int *win_select;         /* optional out [6*n_pairs][33] (LEARNED): rows per kind
                                 back to back (n_pairs each, 2*n_pairs alignment
                                 slots for detailed searches, the batch's last one):
                                 candidates refined (-1: all, margin fallback, not
@@ -161,11 +162,13 @@ typedef struct {
 #define INDIALIGN_CAND_THREAD 1  /* threading-DP offsets (rescue.h:121-190) */
 #define INDIALIGN_CAND_DENSE 2   /* dense local-fragment windows */
 #define INDIALIGN_CAND_DET 3     /* detailed-search fragment seeds (align.h:15-50) */
+#define INDIALIGN_CAND_MAIN 4    /* main seed-bank seeds (windows + anchors, seeds.h:41-283) */
 #define INDIALIGN_RANK_LOCAL 1   /* local-fragment windows */
 #define INDIALIGN_RANK_THREAD 2  /* threading-DP offsets */
 #define INDIALIGN_RANK_DENSE 4   /* dense local-fragment windows */
 #define INDIALIGN_RANK_DET_SS 8  /* detailed searches of the SS seeds (ss.h:87-164) */
 #define INDIALIGN_RANK_DET_DP 16 /* detailed searches of the final dp_refine (indialign.cpp:188-193) */
+#define INDIALIGN_RANK_MAIN 32   /* the main seed bank (indialign.cpp:90-104) */
 /* default: every list but the final dp_refine's detailed searches, which
  * stay exhaustive so that the final refinement of the best transform is the
  * plain search's (measured: pruning them too costs most of the worst-case
@@ -176,7 +179,7 @@ typedef struct {
  * workload: the worst TM-score changes were pairs of L < 50) */
 #define INDIALIGN_RANK_MIN_LEN 100
 #define INDIALIGN_RANKER_FLOATS 18849
-#define INDIALIGN_RANK_STATS 32
+#define INDIALIGN_RANK_STATS 40
 
 /* Stages recorded in stage_best, in search order: seed bank, SS seeds,
  * gapless threading, local fragment DP, threading DP, dense local fragment

@@ -26,12 +26,12 @@ COUNTERS = 12
 TRACE_STAGES = 10
 KERNEL_MS = 6
 MODE_PLAIN, MODE_LEARNED, MODE_COLLECT = 0, 1, 2
-CAND_LOCAL, CAND_THREAD, CAND_DENSE, CAND_DET = 0, 1, 2, 3
-CAND_KINDS = 4
-RANK_LOCAL, RANK_THREAD, RANK_DENSE, RANK_DET_SS, RANK_DET_DP = 1, 2, 4, 8, 16
-CAND_NAMES = ("local", "threading", "dense", "detailed")
+CAND_LOCAL, CAND_THREAD, CAND_DENSE, CAND_DET, CAND_MAIN = 0, 1, 2, 3, 4
+CAND_KINDS = 5
+RANK_LOCAL, RANK_THREAD, RANK_DENSE, RANK_DET_SS, RANK_DET_DP, RANK_MAIN = 1, 2, 4, 8, 16, 32
+CAND_NAMES = ("local", "threading", "dense", "detailed", "seed_bank")
 RANKER_FLOATS = 18849
-RANK_STATS = 32
+RANK_STATS = 40
 RANK_STAT_NAMES = ("gated", "fallback", "audit", "pruned", "windows", "refined",
                    "audit_miss", "small")
 FEATURES = 16
@@ -154,7 +154,7 @@ def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, marg
     opts.rank_mask = int(rank_mask)
     opts.rank_min_len = int(rank_min_len)
     if rank_stats is not None:
-        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [4][8]
+        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [5][8]
         opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
     return opts
 
@@ -165,7 +165,7 @@ def candidate_count(plen: int, nlen: int, kind: int = 2) -> int:
 
 
 def candidate_offsets(pairs: Sequence) -> np.ndarray:
-    """[4, n+1] start of each pair's candidates per kind in the per-candidate
+    """[5, n+1] start of each pair's candidates per kind in the per-candidate
     arrays (kinds back to back): pair p of kind k at off[k, p]:off[k, p+1]
     (for CAND_DET the pair's two alignment slots of equal size)."""
     n = len(pairs)
@@ -231,7 +231,7 @@ def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None,
                     ranker: np.ndarray | None = None):
     """Plain search in COLLECT mode: every rescue candidate's 16 raw features
     and refined score.  Returns (results, feat[C,16] f32, label[C] f32 (NaN
-    where the pair's pass did not run), off[4, n+1]) with pair p's candidates
+    where the pair's pass did not run), off[5, n+1]) with pair p's candidates
     of kind k at off[k, p]:off[k, p+1].  With `ranker`, also the predicted
     scores: (results, feat, label, off, score)."""
     lib = load()

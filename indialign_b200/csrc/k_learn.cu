@@ -245,7 +245,87 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
     f[15] = (float)(tm0 / I.lnorm);
 }
 
-// The candidate set of ranking task t: a pair (windows, offsets) or a
+// Features of seed w of a pair's main seed bank (seeds.h:41-283): a window
+// [s, s+len) of the full pair or an anchor bitmask, restricted to valid
+// residues.  Every lane returns all 16:
+//   0 selected / valid residues   1 first selected / N     2 selected span / N
+//   3 bitmask seed (0/1)          4 seed Kabsch RMSD / 10  5 same-index TM of the
+//   seed's Kabsch over all valid residues                  6, 7, 9 fraction of the
+//   valid residues within d0, 2 d0, d0_search              8 TM over the seed
+//   10 0                          11 log(N) / 7            12 0
+//   13 candidate kind / 2         14 min(RMSD / d0, 10) / 10
+//   15 TM over the seed / lnorm
+IA_DEV void main_seed_features(const DevBatch &b, const PairInfo &I, int p, int w, float (&f)[kFeatures]) {
+    const int lane = threadIdx.x & 31, N = I.N;
+    const int2 e = b.seeds[(size_t)p * kMaxSeeds + w];
+    const bool bitm = e.x < 0;
+    const uint32_t *brow = bitm ? b.bits + I.bitoff + (size_t)(-1 - e.x) * I.words : nullptr;
+    const int lo = bitm ? 0 : e.x, hi = bitm ? N : min(N, e.x + e.y);
+    const double *P = b.pred + 3 * (size_t)I.off, *Q = b.nat + 3 * (size_t)I.off;
+    const uint8_t *V = b.v + I.off;
+    auto sel = [&](int i) {
+        const uint8_t v = V[i];
+        return bitm ? (((brow[i >> 5] >> (i & 31)) & 1u) && (v & 1u)) : (v != 0);
+    };
+    Moments m;
+    m.clear();
+    int first = 0x7fffffff, last = -1;
+    for (int i = lo + lane; i < hi; i += 32)
+        if (sel(i)) {
+            m.add(P[3 * i], P[3 * i + 1], P[3 * i + 2], Q[3 * i], Q[3 * i + 1], Q[3 * i + 2]);
+            first = min(first, i);
+            last = max(last, i);
+        }
+    m.group_sum(32);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        first = min(first, __shfl_xor_sync(kAllLanes, first, o));
+        last = max(last, __shfl_xor_sync(kAllLanes, last, o));
+    }
+    double R[9], t[3];
+    kabsch_from_moments(m, 3.0, R, t);
+    const double d0sq = I.d0 * I.d0, inv = 1.0 / d0sq, dssq = I.d0s * I.d0s;
+    double tm = 0.0, c1 = 0.0, c2 = 0.0, cs = 0.0, sd2 = 0.0, stm = 0.0;
+    for (int i = lane; i < N; i += 32) {
+        if (!V[i]) continue;
+        const double d2 = dist2(R, t, P[3 * i], P[3 * i + 1], P[3 * i + 2], Q[3 * i], Q[3 * i + 1], Q[3 * i + 2]);
+        const double term = 1.0 / (1.0 + d2 * inv);
+        tm += term;
+        c1 += d2 < d0sq ? 1.0 : 0.0;
+        c2 += d2 < 4.0 * d0sq ? 1.0 : 0.0;
+        cs += d2 < dssq ? 1.0 : 0.0;
+        if (i >= lo && i < hi && sel(i)) {
+            sd2 += d2;
+            stm += term;
+        }
+    }
+    tm = warp_sum(tm);
+    c1 = warp_sum(c1);
+    c2 = warp_sum(c2);
+    cs = warp_sum(cs);
+    sd2 = warp_sum(sd2);
+    stm = warp_sum(stm);
+    const double cnt = fmax(m.w, 1.0), vc = (double)(I.vcount > 0 ? I.vcount : 1), Nd = (double)(N > 0 ? N : 1);
+    const double rmsd = sqrt(sd2 / cnt);
+    f[0] = (float)(m.w / vc);
+    f[1] = (float)((last >= 0 ? first : 0) / Nd);
+    f[2] = (float)((last >= 0 ? last - first + 1 : 0) / Nd);
+    f[3] = bitm ? 1.f : 0.f;
+    f[4] = (float)(rmsd / 10.0);
+    f[5] = (float)(tm / I.lnorm);
+    f[6] = (float)(c1 / vc);
+    f[7] = (float)(c2 / vc);
+    f[8] = (float)(stm / cnt);
+    f[9] = (float)(cs / vc);
+    f[10] = 0.f;
+    f[11] = (float)(log(Nd) / 7.0);
+    f[12] = 0.f;
+    f[13] = 0.5f * (float)CAND_MAIN;
+    f[14] = (float)(fmin(rmsd / I.d0, 10.0) / 10.0);
+    f[15] = (float)(stm / I.lnorm);
+}
+
+// The candidate set of ranking task t: a pair (windows, offsets, seeds) or a
 // (pair, alignment slot) of a detailed search, with its point set.
 struct RankTask {
     int p, W, plen, nlen;
@@ -269,6 +349,15 @@ IA_DEV RankTask rank_task(const DevBatch &b, const RankArgs &a, int t) {
         r.plen = r.nlen = na;
         r.Lp = r.Ln = nullptr;
         r.W = r.on ? cand_count(CAND_DET, na, na) : 0;
+    } else if (a.kind == CAND_MAIN) {
+        r.p = t;
+        const PairInfo &I = b.info[t];
+        r.on = I.status == 0 && I.K > 0;
+        r.x = {nullptr, nullptr};
+        r.plen = I.plen;
+        r.nlen = I.nlen;
+        r.Lp = r.Ln = nullptr;
+        r.W = r.on ? I.K : 0;
     } else {
         r.p = t;
         const PairInfo &I = b.info[t];
@@ -334,7 +423,10 @@ __global__ void __launch_bounds__(128) k_rank(DevBatch b, RankArgs a, const int 
                 float mine = 0.f;
                 if (w < W) {
                     float f[kFeatures];
-                    window_features(rt.x, rt.Lp, rt.Ln, I, rt.plen, rt.nlen, best, a.kind, w, f);
+                    if (a.kind == CAND_MAIN)
+                        main_seed_features(b, I, rt.p, w, f);
+                    else
+                        window_features(rt.x, rt.Lp, rt.Ln, I, rt.plen, rt.nlen, best, a.kind, w, f);
 #pragma unroll
                     for (int j = 0; j < kFeatures; j++)
                         if (lane == j) mine = f[j];
@@ -452,11 +544,11 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
 // (rescue.h:163-165), -inf for an offset that was not searched; for a
 // detailed-search seed the best of its cutoff items.
 IA_DEV double cand_score(const CandRes &r, int kind, int det_ss, int t, int w) {
-    if (kind == CAND_DET) {
-        const BankTask &T = r.btasks[det_ss ? t / kDetSlots : t];
+    if (kind == CAND_DET || kind == CAND_MAIN) {  // best of the seed's cutoff items
+        const BankTask &T = r.btasks[kind == CAND_DET && det_ss ? t / kDetSlots : t];
         double s = -INFINITY;
-        for (int ci = 0; ci < kDetC; ci++)
-            s = fmax(s, r.item_res[((size_t)T.item_base + (size_t)w * kDetC + ci) * kRec]);
+        for (int ci = 0; ci < T.C; ci++)
+            s = fmax(s, r.item_res[((size_t)T.item_base + (size_t)w * T.C + ci) * kRec]);
         return s;
     }
     const int p = t;

@@ -61,6 +61,10 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
         T.table = b.seeds + (size_t)p * kMaxSeeds;
         T.K = I.K;
         T.out_rec = REC_BEST;
+        if (c.wcount && c.wcount[p] >= 0) {  // ranked: the selected seeds only
+            T.K = c.wcount[p];
+            T.slist = c.wlist + (size_t)p * kMaxTopK;
+        }
         break;
     case BK_DET_SS:  // detailed search with fragments on an SS alignment
     case BK_DET_DP: {  // ... or on a dp_refine alignment (align.h:115-118)

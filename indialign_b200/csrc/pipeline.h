@@ -176,8 +176,9 @@ constexpr int kRankChunk = 64;  // candidates per CTA chunk of the ranker (4 war
 // dense local-fragment windows -- each a segment (flen, ps, ns) of compact
 // pred / native positions of a pair -- and the seeds of the detailed searches
 // on an NW alignment (align.h:15-50, fragments of the aligned set, two
-// alignment slots per pair).
-enum CandKind { CAND_LOCAL = 0, CAND_THREAD = 1, CAND_DENSE = 2, CAND_DET = 3, kCandKinds = 4 };
+// alignment slots per pair) and the seeds of the main seed bank (fragment
+// windows and anchor bitmasks of the full pair, seeds.h:41-283).
+enum CandKind { CAND_LOCAL = 0, CAND_THREAD = 1, CAND_DENSE = 2, CAND_DET = 3, CAND_MAIN = 4, kCandKinds = 5 };
 constexpr int kDetSlots = 2;  // detailed-search alignment slots per pair (gap chains)
 
 // FP32 parameter blob: mean[16] std[16] W1[16][128] b1[128] W2[128][128]

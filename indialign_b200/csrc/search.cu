@@ -229,9 +229,12 @@ class Runner {
     int after_stage(int kind, const CandRes &r, int det_ss = 0);
     int ntasks(int kind) const { return kind == CAND_DET ? kDetSlots * n_ : n_; }
     // first selection row of a kind in the win_select output (kinds back to back)
-    long long sel_row(int kind) const { return kind == CAND_DET ? 3LL * n_ : (long long)kind * n_; }
+    long long sel_row(int kind) const {
+        return kind == CAND_MAIN ? 5LL * n_ : (kind == CAND_DET ? 3LL * n_ : (long long)kind * n_);
+    }
     // ranked candidate lists this call: bit of INDIALIGN_RANK_* per pass
     int rank_bit(int kind, int det_ss) const {
+        if (kind == CAND_MAIN) return INDIALIGN_RANK_MAIN;
         return kind == CAND_DET ? (det_ss ? INDIALIGN_RANK_DET_SS : INDIALIGN_RANK_DET_DP) : (1 << kind);
     }
     bool ranked(int kind, int det_ss = 0) const {
@@ -251,7 +254,7 @@ class Runner {
     int n_;
     Layout L_pair, L_main, L_detss, L_detdp, L_gapless, L_thread, L_topk, L_localn, L_locald,
         L_threadch, L_single, L_offdp, L_offslots, L_cand[kCandKinds];
-    long long koff_[kCandKinds + 1] = {0, 0, 0, 0, 0};
+    long long koff_[kCandKinds + 1] = {0, 0, 0, 0, 0, 0};
     long long max_items_ = 0, max_chain_recs_ = 0, n_thread_ = 0, n_off_ = 0;
     int chain_grid_ = 0, chain_flags_ = 0, rank_grid_ = 1;
     size_t trace_words_ = 0;
@@ -335,6 +338,8 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
                 const int m = info[p].plen < info[p].nlen ? info[p].plen : info[p].nlen;
                 for (int g = 0; g < kDetSlots; g++) L_cand[k].base[(size_t)kDetSlots * p + g] = kdet_max(m);
             }
+        } else if (k == CAND_MAIN) {  // room for the largest seed table
+            L_cand[k].base.assign(n, (long long)kMaxSeeds);
         } else {
             L_cand[k].base.resize(n);
             for (int p = 0; p < n; p++) L_cand[k].base[p] = cand_count(k, info[p].plen, info[p].nlen);
@@ -368,7 +373,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     size_t ni = 0, nl = 0;
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
                       &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
-                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3]}) {
+                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3], &L_cand[4]}) {
         ni += L->pair.size() + L->aux.size();
         nl += L->base.size();
     }
@@ -380,7 +385,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     hl.reserve(nl);
     for (Layout *L : {&L_pair, &L_main, &L_detss, &L_detdp, &L_gapless, &L_thread, &L_topk,
                       &L_localn, &L_locald, &L_threadch, &L_single, &L_offdp, &L_offslots,
-                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3]}) {
+                      &L_cand[0], &L_cand[1], &L_cand[2], &L_cand[3], &L_cand[4]}) {
         L->d_pair = L->pair.empty() ? nullptr : c_->lay_i.p + hi.size();
         hi.insert(hi.end(), L->pair.begin(), L->pair.end());
         L->d_aux = L->aux.empty() ? nullptr : c_->lay_i.p + hi.size();
@@ -599,7 +604,7 @@ int Runner::rank_stage(int kind, int det_ss) {
     if (!ranked(kind, det_ss)) return INDIALIGN_OK;
     cudaStream_t st = c_->stream;
     const RankArgs ra = rank_args(kind, det_ss);
-    if (kind == CAND_DET) {  // a slot's arrays hold its last search only (NaN beyond its seeds)
+    if (kind == CAND_DET || kind == CAND_MAIN) {  // hold this search only (NaN beyond its seeds)
         CK(cudaMemsetAsync(c_->wscore.p + koff_[kind], 0xff, (size_t)L_cand[kind].total * sizeof(float), st));
         if (cfg_.mode == INDIALIGN_MODE_COLLECT)
             CK(cudaMemsetAsync(c_->wlabel.p + koff_[kind], 0xff, (size_t)L_cand[kind].total * sizeof(float), st));
@@ -654,7 +659,7 @@ int Runner::after_stage(int kind, const CandRes &r, int det_ss) {
             const int nt = ntasks(kind);
             CK(cudaMemcpyAsync(sel_out + sel_row(kind), c_->wcount.p, nt * sizeof(int), cudaMemcpyDeviceToDevice,
                                st));
-            CK(cudaMemcpyAsync(sel_out + 5LL * n_ + sel_row(kind) * kMaxTopK, c_->wlist.p,
+            CK(cudaMemcpyAsync(sel_out + 6LL * n_ + sel_row(kind) * kMaxTopK, c_->wlist.p,
                                (size_t)nt * kMaxTopK * sizeof(int), cudaMemcpyDeviceToDevice, st));
         }
     } else if (cfg_.mode == INDIALIGN_MODE_COLLECT) {
@@ -676,7 +681,9 @@ int Runner::after_stage(int kind, const CandRes &r, int det_ss) {
 int Runner::run_stages() {
     cudaStream_t st = c_->stream;
     // 2. seed bank (indialign.cpp:90-104)
-    RUN(bank(BK_MAIN, L_main));
+    RUN(rank_stage(CAND_MAIN));
+    RUN(bank(BK_MAIN, L_main, nullptr, -1, -1, sel_count(CAND_MAIN), sel_list(CAND_MAIN)));
+    RUN(after_stage(CAND_MAIN, det_res(c_)));
     mark(0);
     // 2b. SS seeds IA2 + IA4, rescored (indialign.cpp:106-116, ss.h:87-164)
     launch_ss(b, st);
@@ -1003,7 +1010,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     if (cfg.mode == INDIALIGN_MODE_LEARNED) {
         CK(cudaMemsetAsync(c->rstats.p, 0, kCandKinds * kRankStats * sizeof(unsigned long long), st));
         if (opts->win_select) {
-            CK(c->wsel.ensure((size_t)5 * n * (1 + kMaxTopK)));
+            CK(c->wsel.ensure((size_t)6 * n * (1 + kMaxTopK)));
             r.sel_out = c->wsel.p;
         }
     }
@@ -1043,7 +1050,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
                       cudaMemcpyDeviceToHost));
     if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->win_select) {
         // rows: kinds back to back, n rows each, 2n for the detailed-search slots
-        const size_t rows = (size_t)5 * n;
+        const size_t rows = (size_t)6 * n;
         std::vector<int> h(rows * (1 + kMaxTopK));
         CK(cudaMemcpy(h.data(), c->wsel.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost));
         const int *wc = h.data(), *wl = h.data() + rows;
@@ -1333,6 +1340,7 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
 int indialign_candidate_count(int plen, int nlen, int kind) {
     if (plen < 0 || nlen < 0 || kind < 0 || kind >= ia::kCandKinds) return 0;
     if (kind == ia::CAND_DET) return ia::kDetSlots * ia::kdet_max(plen < nlen ? plen : nlen);
+    if (kind == ia::CAND_MAIN) return ia::kMaxSeeds;
     return ia::cand_count(kind, plen, nlen);
 }
 

@@ -203,18 +203,18 @@ def test_candidate_features_match_oracle(oracle):
     assert (checked >= 20).all(), checked
 
 
-def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True, min_len=-1):
+def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True, min_len=-1, mask=0):
     lib = ia.load()
     pk = abi.PackedInputs(pairs)
     res = (abi.NativePairResult * pk.n)()
     opts = ia.BatchOptions()
     opts.device = -1
     stats = np.zeros(ia.RANK_STATS, np.int64)
-    ia.learned_options(opts, blob, k, margin, audit, seed, stats, rank_min_len=min_len)
+    ia.learned_options(opts, blob, k, margin, audit, seed, stats, rank_mask=mask, rank_min_len=min_len)
     off = ia.candidate_offsets(pairs)
     C = int(off[-1, -1])
     score = np.zeros(max(1, C), np.float32)
-    sel = np.zeros((5 * len(pairs), 33), np.int32)
+    sel = np.zeros((6 * len(pairs), 33), np.int32)
     if outputs:
         opts.win_score = score.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         opts.win_cap = C
@@ -229,6 +229,8 @@ def _lists(kind, n, off):
     """(selection row, pair, candidate range) of every list of a kind."""
     if kind < 3:
         return [(kind * n + i, i, off[kind, i], off[kind, i + 1]) for i in range(n)]
+    if kind == 4:
+        return [(5 * n + i, i, off[kind, i], off[kind, i + 1]) for i in range(n)]
     out = []
     for i in range(n):
         a, b = off[kind, i], off[kind, i + 1]
@@ -241,7 +243,9 @@ def test_selection_matches_oracle():
     pairs = W.batch(48, 40, 200, seed=12, sigma_lo=5.0, sigma_hi=14.0)
     blob = _blob(7)
     for k, margin, audit, seed in ((8, 0.0, 0.0, 0), (8, 0.02, 0.3, 99), (3, 1e9, 0.0, 1), (32, 0.0, 0.0, 2)):
-        (sc, _, _), stats, score, sel, off = _learned_run(pairs, blob, k, margin, audit, seed)
+        (sc, _, _), stats, score, sel, off = _learned_run(pairs, blob, k, margin, audit, seed,
+                                                          mask=(ia.RANK_LOCAL | ia.RANK_THREAD | ia.RANK_DENSE |
+                                                                ia.RANK_DET_SS | ia.RANK_MAIN))
         for kind in range(ia.CAND_KINDS):
             gated = 0
             for r, i, a, b in _lists(kind, len(pairs), off):
@@ -250,7 +254,7 @@ def test_selection_matches_oracle():
                     continue  # pass not run for this list (or at most k candidates)
                 gated += 1
                 s = score[a:b]
-                if kind == 3:  # the slot's last detailed search: scores up to its seed count
+                if kind >= 3:  # this search's seeds only: scores up to its seed count
                     fin = np.isfinite(s)
                     s = s[:int(np.argmin(fin)) if not fin.all() else s.size]
                 c, lst = ro.select(s, k, margin, audit, seed, i)

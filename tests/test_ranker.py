@@ -99,7 +99,9 @@ def test_candidate_schedules_match_library(plen, nlen):
     assert ia.candidate_count(plen, nlen, ia.CAND_DET) == 2 * room
     for flen, ps, ns in ro.det_seeds(m):
         assert flen >= 3 and ps == ns and ps + flen <= m
-    assert ia.candidate_count(plen, nlen, 4) == 0 and ia.candidate_count(-1, nlen, 0) == 0
+    # main seed bank: room for the largest seed table
+    assert ia.candidate_count(plen, nlen, ia.CAND_MAIN) == 1024
+    assert ia.candidate_count(plen, nlen, 5) == 0 and ia.candidate_count(-1, nlen, 0) == 0
 
 
 def test_pair_rows_pairs_within_groups():
