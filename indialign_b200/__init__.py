@@ -227,13 +227,17 @@ def search(pairs: Sequence, cfg: NativeConfig | None = None, profile: bool = Fal
     return abi.results_to_numpy(res, pk.n)
 
 
+RANK_ALL = RANK_LOCAL | RANK_THREAD | RANK_DENSE | RANK_DET_SS | RANK_DET_DP | RANK_MAIN
+
+
 def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None,
-                    ranker: np.ndarray | None = None):
+                    ranker: np.ndarray | None = None, rank_mask: int = RANK_ALL):
     """Plain search in COLLECT mode: every rescue candidate's 16 raw features
     and refined score.  Returns (results, feat[C,16] f32, label[C] f32 (NaN
     where the pair's pass did not run), off[5, n+1]) with pair p's candidates
     of kind k at off[k, p]:off[k, p+1].  With `ranker`, also the predicted
-    scores: (results, feat, label, off, score)."""
+    scores: (results, feat, label, off, score).  rank_mask picks the lists
+    recorded (default every kind)."""
     lib = load()
     cfg = cfg or default_config()
     pk = abi.PackedInputs(pairs)
@@ -245,6 +249,7 @@ def collect_windows(pairs: Sequence, cfg: NativeConfig | None = None,
     opts = BatchOptions()
     opts.device = -1
     opts.mode = MODE_COLLECT
+    opts.rank_mask = int(rank_mask)
     opts.win_feat = _fptr(feat)
     opts.win_label = _fptr(label)
     opts.win_cap = W
