@@ -240,6 +240,8 @@ def main():
     ap.add_argument("--top-k", type=int, default=8)
     ap.add_argument("--margin", type=float, default=0.02)
     ap.add_argument("--audit", type=float, default=0.02)
+    ap.add_argument("--rank-mask", type=int, default=0, help="INDIALIGN_RANK_* bits (0: library default)")
+    ap.add_argument("--weights", default=None, help="ranker blob (.npy; default the shipped weights)")
     ap.add_argument("--ref-pairs", type=int, default=8)
     ap.add_argument("--cpu-sample", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -266,7 +268,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lib = ia.load()
     cfg = ia.default_config()
-    blob = ranker.default_weights()
+    blob = (np.ascontiguousarray(np.load(args.weights), np.float32) if args.weights
+            else ranker.default_weights())
     dev = [DeviceBatch(torch, b) for b in batches]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
@@ -283,7 +286,8 @@ def main():
         o.counters = o.ctr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
         o.stage_ms = o.stg.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         if learned:
-            ia.learned_options(o, blob, args.top_k, args.margin, args.audit, 1234 + rank, o.rst)
+            ia.learned_options(o, blob, args.top_k, args.margin, args.audit, 1234 + rank, o.rst,
+                               args.rank_mask)
         return o
 
     def device_step(db, o):
@@ -428,7 +432,8 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": desc, "step_pairs": args.step_pairs, "pairs_timed_per_gpu": n_timed,
-                           "mode": (f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit})"
+                           "mode": (f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit}, "
+                                    f"rank_mask {args.rank_mask or 'default'})"
                                     if learned_mode else "plain"),
                            "ranker": "indialign_b200/ranker_weights.npy",
                            "l2": "flushed by a 256 MB write before every step",
