@@ -322,7 +322,7 @@ def test_learned_mode_with_full_fallback_is_the_plain_search():
     pairs = W.batch(32, 40, 200, seed=21, sigma_lo=4.0, sigma_hi=14.0)
     s0, R0, t0 = ia.search(pairs)
     blob = _blob(9)
-    for mask, margin in ((0, 1e9), (32, 0.0)):
+    for mask, margin in ((0, 1e9), (1 << 10, 0.0)):  # 1 << 10 names no list kind
         lib = ia.load()
         pk = abi.PackedInputs(pairs)
         res = (abi.NativePairResult * pk.n)()
