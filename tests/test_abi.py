@@ -121,3 +121,22 @@ def test_padded_entry_rejects_bad_lengths_before_device_work():
     rc = lib.indialign_tmscore_search_padded(2, 0, lens, dummy, dummy, dummy, dummy, dummy, ln,
                                              ctypes.byref(cfg), None, dummy)
     assert rc == -4
+
+
+def test_batch_options_layout_matches_header(tmp_path):
+    """The Python mirror of IndialignBatchOptions has the C struct's size and
+    field offsets (a C program compiled against the header prints them)."""
+    fields = [f[0] for f in ia.BatchOptions._fields_]
+    src = tmp_path / "layout.c"
+    body = "\n".join(f'    printf("%s %zu\\n", "{f}", offsetof(IndialignBatchOptions, {f}));' for f in fields)
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "indialign_b200.h"\n'
+                   'int main(void) {\n' + body +
+                   '\n    printf("sizeof %zu\\n", sizeof(IndialignBatchOptions));\n    return 0;\n}\n')
+    exe = tmp_path / "layout"
+    import subprocess
+    subprocess.run(["/usr/bin/gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                        text=True).stdout.splitlines())
+    for f in fields:
+        assert int(out[f]) == getattr(ia.BatchOptions, f).offset, f
+    assert int(out["sizeof"]) == ctypes.sizeof(ia.BatchOptions)
