@@ -1,0 +1,103 @@
+"""C1' traces from PDB text, and search pairs of structures of unequal
+length.
+
+The search compares pred[i] with native[i] (same index); structures of
+different lengths or with missing residues become one padded pair: residue
+slots of the union of residue numbers, each side's missing slots marked
+invalid in its own mask (pred_valid / native_valid), valid = both.  The
+search's cross-index passes (NW, threading, local fragments) then find
+offset correspondences, as for the reference's benchmark pairs
+(benchmark/pdb_hard_benchmark.py:134-224: C1' extraction per model / chain,
+pairing by residue number, lnorm = residues valid on both sides).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .workloads import Pair
+
+
+def _atom_c1(line: str):
+    """(chain, resnum, xyz) of a C1' ATOM record, else None."""
+    if not line.startswith("ATOM") or line[12:16].strip() != "C1'":
+        return None
+    xyz = (float(line[30:38]), float(line[38:46]), float(line[46:54]))
+    return line[21], int(line[22:26]), np.array(xyz, np.float64)
+
+
+def c1_models(text: str) -> list[np.ndarray]:
+    """C1' coordinates of every model, in file order ([N, 3] each)."""
+    models, cur = [], []
+    for line in text.splitlines():
+        rec = line[:6].strip()
+        if rec == "MODEL":
+            cur = []
+        elif rec == "ENDMDL":
+            if cur:
+                models.append(np.array(cur))
+            cur = []
+        else:
+            a = _atom_c1(line)
+            if a is not None:
+                cur.append(a[2])
+    if cur:  # a file without MODEL records, or a last model without ENDMDL
+        models.append(np.array(cur))
+    return models
+
+
+def c1_by_chain(text: str) -> dict[str, dict[int, np.ndarray]]:
+    """{chain: {residue number: C1' xyz}} of the first model."""
+    chains: dict[str, dict[int, np.ndarray]] = {}
+    for line in text.splitlines():
+        if line[:6].strip() == "ENDMDL":
+            break
+        a = _atom_c1(line)
+        if a is not None:
+            chains.setdefault(a[0], {})[a[1]] = a[2]
+    return chains
+
+
+def pair_by_resnum(pred: dict[int, np.ndarray], native: dict[int, np.ndarray]) -> Pair:
+    """One padded pair over the union of residue numbers (ascending)."""
+    res = sorted(set(pred) | set(native))
+    N = len(res)
+    P = np.zeros((N, 3))
+    Q = np.zeros((N, 3))
+    pv = np.zeros(N, np.uint8)
+    nv = np.zeros(N, np.uint8)
+    for k, r in enumerate(res):
+        if r in pred:
+            P[k], pv[k] = pred[r], 1
+        if r in native:
+            Q[k], nv[k] = native[r], 1
+    v = (pv & nv).astype(np.uint8)
+    return Pair(P, Q, v, pv, nv, float(max(int(v.sum()), 1)), 0.0, False)
+
+
+def pair_padded(pred: np.ndarray, native: np.ndarray, lnorm: float | None = None) -> Pair:
+    """Two traces of possibly different lengths, without residue numbers:
+    both padded to the longer one with invalid slots.  lnorm defaults to the
+    native length (the reference structure's)."""
+    Lp, Ln = len(pred), len(native)
+    N = max(Lp, Ln)
+    P = np.zeros((N, 3))
+    Q = np.zeros((N, 3))
+    P[:Lp], Q[:Ln] = pred, native
+    pv = np.zeros(N, np.uint8)
+    nv = np.zeros(N, np.uint8)
+    pv[:Lp], nv[:Ln] = 1, 1
+    v = (pv & nv).astype(np.uint8)
+    return Pair(P, Q, v, pv, nv, float(lnorm if lnorm is not None else Ln), 0.0, False)
+
+
+def c1_pdb_text(coords: np.ndarray, valid: np.ndarray | None = None, chain: str = "A",
+                first_resnum: int = 1) -> str:
+    """PDB ATOM records of a C1' trace (residues with valid == 0 left out)."""
+    lines = []
+    for i, (x, y, z) in enumerate(np.asarray(coords, np.float64)):
+        if valid is not None and not valid[i]:
+            continue
+        r = first_resnum + i
+        lines.append(f"ATOM  {len(lines) + 1:>5d}  C1'   A {chain}{r:>4d}    "
+                     f"{x:>8.3f}{y:>8.3f}{z:>8.3f}  1.00  0.00           C")
+    return "\n".join(lines) + "\nEND\n"

@@ -1,0 +1,71 @@
+"""C1' traces from PDB text and padded pairs of unequal length; the oracle
+(C restatement) against the reference build on such pairs.  (The final score
+stays the reference's same-index TM-score over residues valid on both
+sides, so it is not a measure of the offset correspondence.)"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from indialign_b200 import abi, pdb, workloads as W
+
+
+def _trace(L, seed):
+    return W.make_trace(L, np.random.default_rng(seed))
+
+
+def test_c1_roundtrip_and_models():
+    x = _trace(30, 1)
+    keep = np.ones(30, bool)
+    keep[[3, 4, 17]] = False
+    txt = pdb.c1_pdb_text(x, keep, chain="B", first_resnum=10)
+    ch = pdb.c1_by_chain(txt)
+    assert list(ch) == ["B"]
+    assert sorted(ch["B"]) == [10 + i for i in range(30) if keep[i]]
+    got = np.array([ch["B"][10 + i] for i in range(30) if keep[i]])
+    np.testing.assert_allclose(got, x[keep], atol=5e-4)
+    two = "MODEL        1\n" + txt.replace("END\n", "") + "ENDMDL\nMODEL        2\n" + \
+        pdb.c1_pdb_text(x[:12]).replace("END\n", "") + "ENDMDL\nEND\n"
+    models = pdb.c1_models(two)
+    assert [m.shape for m in models] == [(27, 3), (12, 3)]
+    assert [m.shape for m in pdb.c1_models(txt)] == [(27, 3)]
+
+
+def test_pair_by_resnum_marks_each_side():
+    a = {1: np.zeros(3), 2: np.ones(3), 5: np.full(3, 2.0)}
+    b = {2: np.ones(3), 3: np.zeros(3), 5: np.zeros(3)}
+    p = pdb.pair_by_resnum(a, b)
+    assert p.pred.shape == (4, 3)
+    assert p.pred_valid.tolist() == [1, 1, 0, 1]
+    assert p.native_valid.tolist() == [0, 1, 1, 1]
+    assert p.valid.tolist() == [0, 1, 0, 1] and p.lnorm == 2.0
+
+
+def _cross_pairs():
+    out = []
+    for k, (Lp, Ln) in enumerate([(60, 48), (45, 70), (90, 90)]):
+        x = _trace(max(Lp, Ln), 10 + k)
+        rng = np.random.default_rng(20 + k)
+        nat = x[:Ln] + rng.normal(0, 1.5, (Ln, 3))
+        nat = nat @ W.random_rotation(rng).T + rng.uniform(-30, 30, 3)
+        pred = x[max(Lp, Ln) - Lp:] if Lp < Ln else x[:Lp]  # a shifted segment when shorter
+        out.append(pdb.pair_padded(pred, nat))
+    return out
+
+
+def test_cross_length_pairs_oracle_matches_reference(oracle, ref):
+    pairs = _cross_pairs()
+    rc, so, _, _ = abi.run_batch(oracle, pairs, prefix="ora_")
+    rc2, sr, _, _ = abi.run_batch(ref, pairs)
+    assert rc == 0 and rc2 == 0
+    np.testing.assert_allclose(so, sr, atol=1e-9)
+
+
+@pytest.mark.gpu
+def test_cross_length_pairs_gpu_vs_oracle(oracle):
+    import indialign_b200 as ia
+    pairs = _cross_pairs()
+    s, _, _ = ia.search(pairs)
+    rc, so, _, _ = abi.run_batch(oracle, pairs, prefix="ora_")
+    assert rc == 0
+    assert np.all(s >= so - 1e-6), (s, so)
