@@ -92,8 +92,9 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="indialign_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
