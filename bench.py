@@ -171,7 +171,7 @@ def run_reference_arm(args):
     os.environ["OMP_NUM_THREADS"] = str(cores)
     ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
     for k in range(args.warmup):
-        abi.run_batch(ref, W.subsample(batches[k], 2, seed=3 + k))
+        abi.run_batch(ref, sorted(batches[k], key=lambda p: p.pred.shape[0])[:1])  # shortest pair
     times, n_done = [], 0
     for k in range(args.steps):
         sample = W.subsample(batches[args.warmup + k], args.ref_pairs, seed=100 + k)
