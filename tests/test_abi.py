@@ -140,3 +140,11 @@ def test_batch_options_layout_matches_header(tmp_path):
     for f in fields:
         assert int(out[f]) == getattr(ia.BatchOptions, f).offset, f
     assert int(out["sizeof"]) == ctypes.sizeof(ia.BatchOptions)
+
+
+def test_search_tensors_rejects_bad_shapes_before_device_work():
+    torch = pytest.importorskip("torch")
+    with pytest.raises(ValueError):
+        ia.search_tensors(torch.zeros(2, 5, 3), torch.zeros(2, 6, 3))
+    with pytest.raises(ValueError):
+        ia.search_tensors(torch.zeros(2, 5, 3), torch.zeros(2, 5, 3))  # host tensors
