@@ -982,7 +982,8 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     r.b = b;
     r.use_mlp = use_mlp;
     r.Nmax = Nmax;
-    r.timing = opts && (opts->stage_ms || opts->kernel_ms);
+    const bool print_profile = (opts && opts->profile) || std::getenv("INDIALIGN_PROFILE");
+    r.timing = (opts && (opts->stage_ms || opts->kernel_ms)) || print_profile;
     r.stage_event(0);
     // ---- seeds ----
     launch_prep(b, cfg.use_frag, st);
@@ -1096,9 +1097,15 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
             CK(cudaEventElapsedTime(&ms, r.stage_ev.front().second, r.stage_ev.back().second));
             stage[INDIALIGN_STAGES - 1] = ms;
         }
-        if (opts->stage_ms)
+        if (opts && opts->stage_ms)
             for (int k = 0; k < INDIALIGN_STAGES; k++) opts->stage_ms[k] = stage[k];
-        if (opts->kernel_ms) {
+        if (print_profile) {  // per-stage device times, the reference's stage names
+            const char *tag = std::getenv("INDIALIGN_PROFILE_TAG");
+            for (int k = 0; k < INDIALIGN_STAGES - 1; k++)
+                std::fprintf(stderr, "[indialign]%s pairs=%d stage=%s ms=%.3f\n", tag ? tag : "", n,
+                             kStageNames[k], stage[k]);
+        }
+        if (opts && opts->kernel_ms) {
             double ch = 0, bk = 0;
             for (auto &x : r.chain_ev) { CK(cudaEventElapsedTime(&ms, x.first, x.second)); ch += ms; }
             for (auto &x : r.bank_ev) { CK(cudaEventElapsedTime(&ms, x.first, x.second)); bk += ms; }

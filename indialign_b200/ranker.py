@@ -1,13 +1,15 @@
-"""Window ranker of the learned dense rescue: parameter blob, training on the
-GPU through the library's BF16 tensor-core kernels, training-set assembly
-from COLLECT-mode searches, and the shipped weights.
+"""Candidate ranker of the learned search: parameter blob, training on the
+GPU through the library's BF16 tensor-core kernels, checkpoints, and the
+shipped weights.
 
-The network predicts, from 16 features of a dense local-fragment rescue
-window (indialign_c/rescue.h:50-117), the score that the window's
-2-iteration dp_refine chain reaches.  It is an MLP 16 -> 128 -> 128 -> 1 with
-GELU, BF16 weights and activations, FP32 accumulation.  Training minimises
-mean squared error plus a pairwise logistic ranking loss on row pairs drawn
-from the same structure pair, with Adam.
+The network predicts, from 16 features of a candidate start of a refinement
+loop -- a local-fragment or dense rescue window (indialign_c/rescue.h:50-117),
+a threading-DP offset (rescue.h:121-190), a detailed-search fragment seed
+(align.h:15-50) -- the score that refining it reaches.  It is an MLP
+16 -> 128 -> 128 -> 1 with GELU, BF16 weights and activations, FP32
+accumulation.  Training minimises mean squared error plus a pairwise
+logistic ranking loss on row pairs drawn from the same candidate list, with
+Adam.
 
 Blob layout (FP32, INDIALIGN_RANKER_FLOATS): mean[16] std[16] W1[16][128]
 b1[128] W2[128][128] b2[128] w3[128] b3, weights [in][out].
@@ -137,6 +139,40 @@ class Trainer:
 
     def numpy_blob(self) -> np.ndarray:
         return self.blob.detach().cpu().numpy().astype(np.float32)
+
+    def checkpoint(self, path: str) -> None:
+        """Save weights, Adam moments and step (resume with restore)."""
+        cpu = lambda t: t.detach().cpu().numpy()
+        save_checkpoint(path, cpu(self.blob), cpu(self.m), cpu(self.v), self.steps)
+
+    def restore(self, path: str) -> None:
+        blob, m, v, step = load_checkpoint(path)
+        for dst, src in ((self.blob, blob), (self.m, m), (self.v, v)):
+            dst.copy_(self.torch.from_numpy(src))
+        self.steps = step
+        self.pack()
+
+
+CHECKPOINT_MAGIC = "indialign-ranker-v1"
+
+
+def save_checkpoint(path: str, blob: np.ndarray, m: np.ndarray, v: np.ndarray, step: int) -> None:
+    """Weights and Adam state in one .npz (header string, blob, moments, step)."""
+    for a in (blob, m, v):
+        assert np.asarray(a).size == RANKER_FLOATS
+    np.savez(path, magic=np.array(CHECKPOINT_MAGIC), blob=np.asarray(blob, np.float32),
+             m=np.asarray(m, np.float32), v=np.asarray(v, np.float32), step=np.array(int(step)))
+
+
+def load_checkpoint(path: str):
+    """(blob, m, v, step) from save_checkpoint."""
+    z = np.load(path)
+    if str(z["magic"]) != CHECKPOINT_MAGIC:
+        raise IndialignError(f"{path}: not a ranker checkpoint")
+    out = tuple(np.ascontiguousarray(z[k], np.float32) for k in ("blob", "m", "v"))
+    if any(a.size != RANKER_FLOATS for a in out):
+        raise IndialignError(f"{path}: wrong parameter count")
+    return out + (int(z["step"]),)
 
 
 def pair_rows(group: np.ndarray, rng: np.random.Generator) -> np.ndarray:

@@ -341,3 +341,21 @@ def test_learned_mode_with_full_fallback_is_the_plain_search():
             assert st[:, 0].sum() > 0 and st[:, 3].sum() == 0  # ranked, never pruned
         else:
             assert st.sum() == 0
+
+
+def test_trainer_checkpoint_restores_state(torch_cuda, tmp_path):
+    torch = torch_cuda
+    rng = np.random.default_rng(8)
+    x = torch.tensor(_features(rng, 512), device="cuda")
+    t = torch.tensor(rng.uniform(0, 1, 512).astype(np.float32), device="cuda")
+    a = ranker.Trainer(_blob(5), batch=512)
+    for _ in range(5):
+        a.step(x, t)
+    path = str(tmp_path / "ck.npz")
+    a.checkpoint(path)
+    b = ranker.Trainer(_blob(6), batch=512)
+    b.restore(path)
+    a.step(x, t)
+    b.step(x, t)
+    assert b.steps == a.steps == 6
+    np.testing.assert_array_equal(a.numpy_blob(), b.numpy_blob())

@@ -218,3 +218,16 @@ def test_search_multi_matches_single_call():
     np.testing.assert_array_equal(s, s0)
     np.testing.assert_array_equal(R, R0)
     np.testing.assert_array_equal(t, t0)
+
+
+def test_profile_env_prints_every_stage(capfd, monkeypatch):
+    """INDIALIGN_PROFILE prints the per-stage device times under the
+    reference's stage names, tagged with INDIALIGN_PROFILE_TAG."""
+    monkeypatch.setenv("INDIALIGN_PROFILE", "1")
+    monkeypatch.setenv("INDIALIGN_PROFILE_TAG", "[t]")
+    ia.search(W.batch(3, 40, 80, seed=5))
+    err = capfd.readouterr().err
+    names = ["seed_build", "seed_bank", "ss", "gapless_threading", "local_fragment", "threading_dp",
+             "dense_local_fragment", "topk_seed", "dp_refine", "offset_dp", "weighted_refine", "total"]
+    for nm in names:
+        assert f"[indialign][t] pairs=3 stage={nm} ms=" in err, nm

@@ -143,3 +143,19 @@ def test_learned_mode_rejects_missing_ranker():
     opts.mode = 7
     rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
     assert rc == -4 and "mode" in ia.last_error()
+
+
+def test_checkpoint_roundtrip(tmp_path):
+    rng = np.random.default_rng(0)
+    blob = _blob(3)
+    m = rng.normal(0, 1e-3, blob.size).astype(np.float32)
+    v = rng.uniform(0, 1e-4, blob.size).astype(np.float32)
+    p = str(tmp_path / "ck.npz")
+    ranker.save_checkpoint(p, blob, m, v, 1234)
+    b2, m2, v2, step = ranker.load_checkpoint(p)
+    assert step == 1234
+    for a, b in ((blob, b2), (m, m2), (v, v2)):
+        assert np.array_equal(a, b)
+    np.savez(str(tmp_path / "bad.npz"), magic=np.array("other"))
+    with pytest.raises(ia.IndialignError):
+        ranker.load_checkpoint(str(tmp_path / "bad.npz"))
