@@ -296,3 +296,30 @@ def select(score: np.ndarray, k: int, margin: float, audit_rate: float, seed: in
     if float(np.float32(top1 - topk)) < np.float32(margin):
         return -1, lst
     return k, lst
+
+
+# ---- main seed-bank seeds ------------------------------------------------------
+def main_seed_features(P: np.ndarray, Q: np.ndarray, valid: np.ndarray, sel: np.ndarray, anchor: bool,
+                       d0: float, d0s: float, lnorm: float) -> np.ndarray:
+    """Features of one main seed-bank seed (seeds.h:41-283) given its
+    selection (seed & valid) on the full pair, FP64."""
+    v = np.asarray(valid) != 0
+    s = (np.asarray(sel) != 0) & v
+    cnt = int(s.sum())
+    if cnt >= 3:
+        R, t = kabsch(P[s], Q[s])
+    else:
+        R, t = np.eye(3), np.zeros(3)
+    d2 = (((P @ R.T + t) - Q) ** 2).sum(1)
+    d0sq = d0 * d0
+    term = 1.0 / (1.0 + d2 / d0sq)
+    N = P.shape[0]
+    vc = max(int(v.sum()), 1)
+    idx = np.flatnonzero(s)
+    first, span = (idx[0], idx[-1] - idx[0] + 1) if idx.size else (0, 0)
+    rmsd = np.sqrt(d2[s].sum() / max(cnt, 1))
+    f = [cnt / vc, first / max(N, 1), span / max(N, 1), 1.0 if anchor else 0.0, rmsd / 10.0,
+         term[v].sum() / lnorm, (d2[v] < d0sq).sum() / vc, (d2[v] < 4 * d0sq).sum() / vc,
+         term[s].sum() / max(cnt, 1), (d2[v] < d0s * d0s).sum() / vc, 0.0, np.log(max(N, 1)) / 7.0, 0.0,
+         2.0, min(rmsd / d0, 10.0) / 10.0, term[s].sum() / lnorm]
+    return np.array(f, np.float64)

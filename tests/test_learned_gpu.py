@@ -359,3 +359,46 @@ def test_trainer_checkpoint_restores_state(torch_cuda, tmp_path):
     b.step(x, t)
     assert b.steps == a.steps == 6
     np.testing.assert_array_equal(a.numpy_blob(), b.numpy_blob())
+
+
+def test_main_seed_features_match_oracle(oracle):
+    """COLLECT-mode features of the main seed bank's seeds (fragment windows
+    and anchors, from the oracle's own seed builder) vs the FP64
+    restatement."""
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    dp = ctypes.POINTER(ctypes.c_double)
+    oracle.ora_all_seeds.argtypes = [dp, dp, u8p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                     u8p, ctypes.c_int]
+    oracle.ora_all_seeds.restype = ctypes.c_int
+    oracle.ora_seed_masks.argtypes = [ctypes.c_int, u8p, ctypes.c_int, ctypes.c_int, u8p, ctypes.c_int]
+    oracle.ora_seed_masks.restype = ctypes.c_int
+    oracle.ora_d0.argtypes = [ctypes.c_double, dp, dp, dp]
+    pairs = W.batch(12, 40, 160, seed=13)
+    (_, _, _), feat, label, off = ia.collect_windows(pairs)
+    rng = np.random.default_rng(1)
+    checked = 0
+    for i, p in enumerate(pairs):
+        N = p.pred.shape[0]
+        P, Q = np.ascontiguousarray(p.pred), np.ascontiguousarray(p.native)
+        v = np.ascontiguousarray(p.valid, np.uint8)
+        d0, d0s, sd8 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        oracle.ora_d0(p.lnorm, ctypes.byref(d0), ctypes.byref(d0s), ctypes.byref(sd8))
+        masks = np.zeros((1024, N), np.uint8)
+        K = oracle.ora_all_seeds(P.ctypes.data_as(dp), Q.ctypes.data_as(dp), v.ctypes.data_as(u8p), N,
+                                 d0s.value, d0.value, 1, masks.ctypes.data_as(u8p), 1024)
+        lab = label[off[4, i]:off[4, i + 1]]
+        assert int(np.isfinite(lab).sum()) == K, (i, K)
+        for w in rng.choice(K, size=min(12, K), replace=False):
+            fo = ro.main_seed_features(P, Q, v, masks[w], w >= _frag_count(oracle, N, v), d0.value, d0s.value,
+                                       p.lnorm)
+            np.testing.assert_allclose(feat[off[4, i] + w].astype(np.float64), fo, rtol=1e-5, atol=2e-6,
+                                       err_msg=f"pair {i} seed {w}")
+            checked += 1
+    assert checked >= 60
+
+
+def _frag_count(oracle, N, v):
+    """Number of fragment-window seeds (the anchors follow them)."""
+    buf = np.zeros((1024, N), np.uint8)
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    return oracle.ora_seed_masks(N, v.ctypes.data_as(u8p), 1, 50, buf.ctypes.data_as(u8p), 1024)
