@@ -231,3 +231,44 @@ def test_profile_env_prints_every_stage(capfd, monkeypatch):
              "dense_local_fragment", "topk_seed", "dp_refine", "offset_dp", "weighted_refine", "total"]
     for nm in names:
         assert f"[indialign][t] pairs=3 stage={nm} ms=" in err, nm
+
+
+def _walk_chain(N, rng):
+    """Persistent random walk of 5.9 A steps (a crude C1' chain)."""
+    steps = np.empty((N, 3))
+    d = rng.normal(size=3)
+    for i in range(N):
+        d = d / np.linalg.norm(d) + 0.3 * rng.normal(size=3)
+        steps[i] = d / np.linalg.norm(d) * (5.9 + 0.5 * rng.normal())
+    x = np.cumsum(steps, 0)
+    return x - x.mean(0)
+
+
+@pytest.mark.parametrize("N,sigma,floor", [(50, 1.0, 0.5), (200, 3.0, 0.2), (6000, 2.0, 0.3),
+                                           (8192, 2.0, 0.3)])
+def test_long_chains_like_the_reference_smoke_cases(N, sigma, floor):
+    """The reference C path's own smoke cases (random-walk chains, rotated,
+    Gaussian noise; rc 0 and a score floor), including N = 6000 and 8192,
+    which run the kernels' global-memory variants (point sets and NW rows
+    beyond shared memory)."""
+    rng = np.random.default_rng(N)
+    nat = _walk_chain(N, rng)
+    pred = nat @ W.random_rotation(rng).T + rng.normal(0, sigma, (N, 3))
+    ones = np.ones(N, np.uint8)
+    p = W.Pair(np.ascontiguousarray(pred), np.ascontiguousarray(nat), ones, ones, ones, float(N), sigma, False)
+    s, R, t = ia.search([p])
+    assert s[0] > floor, s
+    # the returned transform reproduces the returned same-index score
+    moved = pred @ R[0].reshape(3, 3) + t[0]
+    d2 = ((moved - nat) ** 2).sum(1)
+    L = float(N)
+    d0 = max(0.6 * np.sqrt(L - 0.5) - 2.5, 0.3)
+    assert abs((1.0 / (1.0 + d2 / d0 ** 2)).sum() / L - s[0]) < 1e-9
+
+
+def test_identity_long_chain_scores_one():
+    rng = np.random.default_rng(3)
+    nat = _walk_chain(100, rng)
+    ones = np.ones(100, np.uint8)
+    s, _, _ = ia.search([W.Pair(nat.copy(), nat, ones, ones, ones, 100.0, 0.0, False)])
+    assert s[0] > 0.95
