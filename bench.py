@@ -408,6 +408,11 @@ def main():
                     "bank_visits_per_step": int(ctr[2]),
                     "warp_cycle_split": dict(zip(["nw_fill", "traceback", "detailed", "kabsch"],
                                                  [float(x) for x in cyc / max(1.0, cyc.sum())]))}
+        # the library counts its stage launches (counter 7); the device entry
+        # adds the input repack and the result export, the learned search the
+        # MLP weight pack
+        per_call = 2 + (1 if learned_mode else 0)
+        launches = int(sum(int(c[7]) + per_call for c in lrn["ctr"]))
         rst = np.sum(lrn["rst"], 0).reshape(ia.CAND_KINDS, 8)
         rank_info = {}
         for k, nm in enumerate(ia.CAND_NAMES):
@@ -440,7 +445,7 @@ def main():
                            "l2": "flushed by a 256 MB write before every step",
                            "parallelism": f"independent pairs per GPU x{world}"},
                 "plain": plain, "rank": rank_info, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(ctr[7]) + 2, "clocks": clocks,
+                "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps, "clocks": clocks,
                 "stage_ms": dict(zip(STAGES, [round(float(x), 2) for x in np.mean(lrn["stg"], 0)])),
                 "mean_tm": float(l_scores.mean())}
         print(json.dumps(line))
