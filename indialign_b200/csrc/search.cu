@@ -174,6 +174,9 @@ struct Plan {
 class Runner {
   public:
     Runner(Ctx *c, const Cfg &cfg, int n) : c_(c), cfg_(cfg), n_(n) {}
+    ~Runner() { recycle(); }  // events go back to the context's pool on every exit path
+    Runner(const Runner &) = delete;
+    Runner &operator=(const Runner &) = delete;
     long long windows() const { return koff_[kCandKinds]; }
     int *sel_out = nullptr;  // device copy of each pass's selection (LEARNED, win_select)
     long long cand_offset(int kind) const { return koff_[kind]; }
@@ -963,7 +966,14 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaGetLastError());
     }
     const bool prof = (opts && (opts->profile || opts->stage_ms)) || std::getenv("INDIALIGN_PROFILE");
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct EventPair {  // the call's total-time events, destroyed on every exit path
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~EventPair() {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } call_ev;
+    cudaEvent_t &e0 = call_ev.a, &e1 = call_ev.b;
     if (prof) {
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
@@ -1033,8 +1043,6 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
             std::fprintf(stderr, "[indialign]%s pairs=%d stage=%s ms=%.3f\n", tag ? tag : "", n,
                          kStageNames[INDIALIGN_STAGES - 1], ms);
         if (opts && opts->stage_ms) opts->stage_ms[INDIALIGN_STAGES - 1] = ms;
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
     }
     if (err) {
         g_last_error = "device error flag " + std::to_string(err);
