@@ -153,10 +153,52 @@ def cpu_baseline(pairs, n_sample=32, budget_s=25.0, seed=7):
         dt += time.perf_counter() - t0
         done.extend(chunk)
         scores.extend(list(s))
-    return {"value": len(done) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
-            "sample": f"{len(done)} pairs of a {len(sample)}-pair length-stratified sample of the timed "
-                      f"batches (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}, \
-        done, np.array(scores)
+    out = {"value": len(done) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
+           "sample": f"{len(done)} pairs of a {len(sample)}-pair length-stratified sample of the timed "
+                     f"batches (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}
+    single = single_thread_rate(done)
+    if single:
+        out["single_thread"] = single
+    return out, done, np.array(scores)
+
+
+def single_thread_rate(pairs, budget_s=8.0):
+    """The reference build on ONE host thread (a child process started with
+    OMP_NUM_THREADS=1: the reference's rescue passes are OpenMP-parallel
+    inside a single pair), pairs in the given order until `budget_s`."""
+    import tempfile
+    fd, path = tempfile.mkstemp(prefix="indialign_single_", suffix=".npz")
+    os.close(fd)
+    try:
+        np.savez(path, **{f"{k}_{i}": np.asarray(getattr(p, k)) for i, p in enumerate(pairs)
+                          for k in ("pred", "native", "valid", "pred_valid", "native_valid")},
+                 lnorm=np.array([p.lnorm for p in pairs]))
+        r = subprocess.run([sys.executable, "-c", f"import bench; bench._single_thread_worker({path!r}, {budget_s})"],
+                           cwd=ROOT, env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True, text=True,
+                           timeout=budget_s * 10 + 120)
+        if r.returncode != 0 or not r.stdout.strip():
+            return None
+        return json.loads(r.stdout.strip().splitlines()[-1])
+    finally:
+        os.remove(path)
+
+
+def _single_thread_worker(path, budget_s):
+    z = np.load(path)
+    lnorm = z["lnorm"]
+    ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
+    done, dt = 0, 0.0
+    for i in range(len(lnorm)):
+        p = W.Pair(*(z[f"{k}_{i}"] for k in ("pred", "native", "valid", "pred_valid", "native_valid")),
+                   float(lnorm[i]))
+        t0 = time.perf_counter()
+        abi.run_batch(ref, [p])
+        dt += time.perf_counter() - t0
+        done += 1
+        if dt >= budget_s:
+            break
+    print(json.dumps({"value": done / dt if dt > 0 else None, "unit": "pairs/s", "cores": 1,
+                      "sample": f"first {done} pairs of the multi-core sample, one thread, {dt:.1f} s"}))
 
 
 def run_reference_arm(args):

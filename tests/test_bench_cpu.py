@@ -77,3 +77,11 @@ def test_clock_summary_parsing():
 def test_whole_job_rate_and_reduce_without_group():
     assert bench.whole_job_rate(100, 4, 2000.0) == pytest.approx(200.0)
     assert bench.reduce_max(None, 3.5, "cpu") == 3.5
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SO), reason="reference build (oracle/_ref) not present")
+def test_single_thread_reference_rate():
+    from indialign_b200 import workloads
+    pairs = workloads.batch(3, 30, 50, seed=5)
+    r = bench.single_thread_rate(pairs, budget_s=0.5)
+    assert r["cores"] == 1 and r["unit"] == "pairs/s" and r["value"] > 0
