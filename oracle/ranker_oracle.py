@@ -17,7 +17,10 @@ infrastructure (tests/ import it as the checker; the product never does).
 The reference has no learned component: parity of this part is pinned by
 the FP64 finite-difference check of mlp_backward (tests/test_ranker.py) and
 by the window schedule, which restates the reference loop and is checked
-against the library's own count.
+against the library's own count.  The schedule functions it is built from
+(local_frag_lengths, local_jump, frag_lengths, start_positions) and the
+detailed-search seed list are checked against the reference's own functions
+(tests/test_oracle_stages.py).
 """
 from __future__ import annotations
 

@@ -163,6 +163,28 @@ void ref_weighted_refine(const double *p, const double *q, const uint8_t *v,
     weighted_tm_refine(p, q, v, d0, Lnorm, N, n_iters, R, t, score);
 }
 
+// Candidate schedules (seeds.h:15-37, rescue.h:12-46): each writes at most
+// cap entries and returns the count, or -1 when cap is too small.
+static int put_list(const std::vector<int> &v, int *out, int cap) {
+    if ((int)v.size() > cap) return -1;
+    std::copy(v.begin(), v.end(), out);
+    return (int)v.size();
+}
+
+int ref_fragment_lengths(int max_len, int *out, int cap) {
+    return put_list(fragment_lengths(max_len), out, cap);
+}
+
+int ref_start_positions(int n, int frag, int ms, int *out, int cap) {
+    return put_list(start_positions(n, frag, ms), out, cap);
+}
+
+int ref_local_frag_lengths(int plen, int nlen, int dense, int *out, int cap) {
+    return put_list(local_frag_lengths(plen, nlen, dense != 0), out, cap);
+}
+
+int ref_local_jump(int length, int dense) { return local_jump(length, dense != 0); }
+
 // Stage names in the order the search runs them; stage_best receives one
 // {score,R[9],t[3]} record per stage (13 doubles), taken after the stage.
 enum { ST_SEED_BANK, ST_SS, ST_GAPLESS, ST_LOCAL, ST_THREAD_DP, ST_DENSE,

@@ -315,3 +315,64 @@ def test_weighted_refine(ora, ref, pair):
         assert s1.value == pytest.approx(s2.value, abs=TOL)
         np.testing.assert_allclose(R1, R2, atol=1e-9, rtol=0)
         np.testing.assert_allclose(t1, t2, atol=1e-9, rtol=0)
+
+
+# ---- candidate schedules of the learned ranker's oracle ---------------------
+
+def _ranker_oracle():
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+    import ranker_oracle
+    return ranker_oracle
+
+
+def _ref_list(fn, *args, cap=4096):
+    out = np.zeros(cap, np.int32)
+    fn.restype = ctypes.c_int
+    k = fn(*[ctypes.c_int(a) for a in args], ctypes.c_void_p(out.ctypes.data), ctypes.c_int(cap))
+    assert k >= 0
+    return out[:k].tolist()
+
+
+SIZES = list(range(0, 80)) + [99, 100, 101, 149, 150, 151, 199, 200, 201, 249, 250, 251, 299, 300, 301,
+                              349, 350, 351, 512, 999, 1000, 1500, 8192]
+
+
+def test_ranker_schedules_match_reference(ref):
+    """local_frag_lengths / local_jump (rescue.h:12-46), fragment_lengths and
+    start_positions (seeds.h:15-37) as the ranker oracle restates them."""
+    ro = _ranker_oracle()
+    for L in SIZES:
+        for dense in (0, 1):
+            ref.ref_local_jump.restype = ctypes.c_int
+            assert ro.local_jump(L, bool(dense)) == ref.ref_local_jump(ctypes.c_int(L), ctypes.c_int(dense)), L
+        assert ro.frag_lengths(L) == _ref_list(ref.ref_fragment_lengths, L), L
+        for frag in sorted({1, 4, 8, max(1, L // 2), max(1, L)}):
+            for ms in (1, 5, 50):
+                assert ro.start_positions(L, frag, ms) == _ref_list(ref.ref_start_positions, L, frag, ms), \
+                    (L, frag, ms)
+    for plen in (3, 4, 12, 13, 40, 77, 150, 300, 1000):
+        for nlen in (3, 4, 12, 13, 40, 77, 150, 300, 1000):
+            for dense in (0, 1):
+                assert ro.local_frag_lengths(plen, nlen, bool(dense)) == \
+                    _ref_list(ref.ref_local_frag_lengths, plen, nlen, dense), (plen, nlen, dense)
+
+
+@pytest.mark.parametrize("na", [3, 4, 7, 16, 33, 64, 100, 257])
+def test_ranker_detailed_seeds_match_reference_masks(ref, na):
+    """The ranker oracle's detailed-search seeds (whole aligned set, then the
+    fragment windows) are the masks the reference's build_seed_masks makes on
+    an all-valid aligned set of na points (align.h:33-37)."""
+    ro = _ranker_oracle()
+    cap = 8192
+    masks = np.zeros(cap * na, np.uint8)
+    ones = np.ones(na, np.uint8)
+    K = call(ref.ref_seed_masks, na, ones, 1, 50, masks, cap, restype=ctypes.c_int)
+    masks = masks[:K * na].reshape(K, na)
+    want = []
+    for row in masks:
+        idx = np.flatnonzero(row)
+        assert idx.size and idx[-1] - idx[0] + 1 == idx.size  # one contiguous window
+        want.append((int(idx.size), int(idx[0]), int(idx[0])))
+    assert ro.det_seeds(na) == want
