@@ -156,31 +156,48 @@ def cpu_baseline(pairs, n_sample=32, budget_s=25.0, seed=7):
     out = {"value": len(done) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
            "sample": f"{len(done)} pairs of a {len(sample)}-pair length-stratified sample of the timed "
                      f"batches (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}
-    single = single_thread_rate(done)
+    single = single_thread_rate(done, ref)
     if single:
         out["single_thread"] = single
     return out, done, np.array(scores)
 
 
-def single_thread_rate(pairs, budget_s=8.0):
-    """The reference build on ONE host thread (a child process started with
-    OMP_NUM_THREADS=1: the reference's rescue passes are OpenMP-parallel
-    inside a single pair), pairs in the given order until `budget_s`."""
+def single_thread_rate(pairs, ref=None, budget_s=8.0):
+    """The reference build on ONE host thread: a child process started with
+    OMP_NUM_THREADS=1 (the reference's rescue passes are OpenMP-parallel
+    inside a single pair) runs the pairs shortest first until `budget_s`;
+    with `ref` (the reference library loaded with all cores) the same pairs
+    are then timed on all cores, for the parallel speed-up on equal work."""
     import tempfile
+    order = sorted(pairs, key=lambda p: p.pred.shape[0])
     fd, path = tempfile.mkstemp(prefix="indialign_single_", suffix=".npz")
     os.close(fd)
     try:
-        np.savez(path, **{f"{k}_{i}": np.asarray(getattr(p, k)) for i, p in enumerate(pairs)
+        np.savez(path, **{f"{k}_{i}": np.asarray(getattr(p, k)) for i, p in enumerate(order)
                           for k in ("pred", "native", "valid", "pred_valid", "native_valid")},
-                 lnorm=np.array([p.lnorm for p in pairs]))
-        r = subprocess.run([sys.executable, "-c", f"import bench; bench._single_thread_worker({path!r}, {budget_s})"],
-                           cwd=ROOT, env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True, text=True,
-                           timeout=budget_s * 10 + 120)
+                 lnorm=np.array([p.lnorm for p in order]))
+        try:
+            r = subprocess.run([sys.executable, "-c",
+                                f"import bench; bench._single_thread_worker({path!r}, {budget_s})"],
+                               cwd=ROOT, env=dict(os.environ, OMP_NUM_THREADS="1"), capture_output=True,
+                               text=True, timeout=budget_s + 90)
+        except subprocess.TimeoutExpired:
+            return {"value": None, "unit": "pairs/s", "cores": 1,
+                    "sample": f"the shortest pair did not finish within {budget_s + 90:.0f} s on one thread"}
         if r.returncode != 0 or not r.stdout.strip():
             return None
-        return json.loads(r.stdout.strip().splitlines()[-1])
+        out = json.loads(r.stdout.strip().splitlines()[-1])
     finally:
         os.remove(path)
+    n = out.pop("pairs")
+    lens = [p.pred.shape[0] for p in order[:n]]
+    out["sample"] = (f"the {n} shortest pairs (L {min(lens)}-{max(lens)}) of the multi-core sample, "
+                     f"one thread, {out.pop('seconds'):.1f} s")
+    if ref is not None and n > 0:
+        t0 = time.perf_counter()
+        abi.run_batch(ref, order[:n])
+        out["same_pairs_all_cores"] = n / (time.perf_counter() - t0)
+    return out
 
 
 def _single_thread_worker(path, budget_s):
@@ -198,7 +215,7 @@ def _single_thread_worker(path, budget_s):
         if dt >= budget_s:
             break
     print(json.dumps({"value": done / dt if dt > 0 else None, "unit": "pairs/s", "cores": 1,
-                      "sample": f"first {done} pairs of the multi-core sample, one thread, {dt:.1f} s"}))
+                      "pairs": done, "seconds": dt}))
 
 
 def run_reference_arm(args):

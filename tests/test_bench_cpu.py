@@ -83,5 +83,9 @@ def test_whole_job_rate_and_reduce_without_group():
 def test_single_thread_reference_rate():
     from indialign_b200 import workloads
     pairs = workloads.batch(3, 30, 50, seed=5)
-    r = bench.single_thread_rate(pairs, budget_s=0.5)
+    import ctypes
+    from indialign_b200 import abi
+    ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
+    r = bench.single_thread_rate(pairs, ref, budget_s=0.5)
     assert r["cores"] == 1 and r["unit"] == "pairs/s" and r["value"] > 0
+    assert r["same_pairs_all_cores"] > 0 and "shortest" in r["sample"]
