@@ -1,0 +1,275 @@
+"""Precision study of the search (design evidence; test infrastructure only).
+
+Rebuilds the C oracle (indialign_oracle.c) with its arithmetic lowered to
+FP32 in five ways, runs each variant's batch search beside the reference
+build (_ref/libindialign_ref.so), rescores every variant's final (R, t) in
+FP64 with the reference's own tm_score_no_d8 (_ref/libindialign_ref_stages.so)
+and prints the per-pair change of the final TM-score against the reference:
+
+  dist32      FP32 distances and inlier tests, FP64 moments and sums
+  kahan32     FP32 distances, TM terms, score-matrix entries and centred
+              covariances with Kahan sums; FP64 eigen-solve
+  plain32     the same with plain FP32 sums
+  raw32       plain FP32 one-pass raw moments about the origin
+  raw32c      the same about the mean of each point set
+
+Variant sources and libraries go to oracle/_variants/.  The variants are
+compiled without -ffast-math (it would fold the Kahan compensation away).
+
+    python oracle/precision_study.py --pairs 400 --seed 21 --hard 160 --hard-seed 22
+
+takes ~30 min on 8 host cores; every textual substitution is checked, so a
+changed oracle source fails loudly instead of measuring the wrong thing.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+sys.path.insert(0, ROOT)
+
+from indialign_b200 import abi, workloads as W  # noqa: E402
+
+OUT = os.path.join(HERE, "_variants")
+REF_SO = os.path.join(HERE, "_ref", "libindialign_ref.so")
+STAGES_SO = os.path.join(HERE, "_ref", "libindialign_ref_stages.so")
+
+
+def _sub(s: str, old: str, new: str) -> str:
+    if s.count(old) != 1:
+        raise SystemExit(f"substitution does not apply (found {s.count(old)}x): {old[:60]!r}")
+    return s.replace(old, new)
+
+
+DIST64 = '''static inline double dist2_at(const double *p, const double *q, const double *R,
+                              const double *t) {
+    double mx = p[0] * R[0] + p[1] * R[3] + p[2] * R[6] + t[0];
+    double my = p[0] * R[1] + p[1] * R[4] + p[2] * R[7] + t[1];
+    double mz = p[0] * R[2] + p[1] * R[5] + p[2] * R[8] + t[2];
+    double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+    return dx * dx + dy * dy + dz * dz;
+}'''
+DIST32 = '''static inline double dist2_at(const double *p, const double *q, const double *R,
+                              const double *t) {
+    float px = (float)p[0], py = (float)p[1], pz = (float)p[2];
+    float mx = px * (float)R[0] + py * (float)R[3] + pz * (float)R[6] + (float)t[0];
+    float my = px * (float)R[1] + py * (float)R[4] + pz * (float)R[7] + (float)t[1];
+    float mz = px * (float)R[2] + py * (float)R[5] + pz * (float)R[8] + (float)t[2];
+    float dx = mx - (float)q[0], dy = my - (float)q[1], dz = mz - (float)q[2];
+    return (double)(dx * dx + dy * dy + dz * dz);
+}
+static inline float tmterm(double d2, double d0sq) { return 1.0f / (1.0f + (float)d2 / (float)d0sq); }'''
+IMIN = 'static int imin(int a, int b) { return a < b ? a : b; }\n'
+KAHAN = '''typedef struct { float s, c; } kahan;
+static inline void kadd(kahan *k, float x) { float y = x - k->c; float t = k->s + y; k->c = (t - k->s) - y; k->s = t; }
+'''
+PLAIN = '''typedef struct { float s, c; } kahan;
+static inline void kadd(kahan *k, float x) { k->s += x; }
+'''
+
+KABSCH64 = '''    double w = 0, cP[3] = {0, 0, 0}, cQ[3] = {0, 0, 0}, H[3][3];
+    for (int i = 0; i < N; i++) {
+        if (!mask[i]) continue;
+        for (int d = 0; d < 3; d++) { cP[d] += P[i * 3 + d]; cQ[d] += Q[i * 3 + d]; }
+        w += 1.0;
+    }
+    if (w < 3.0) {
+        memcpy(R, IDENT, sizeof IDENT);
+        t[0] = t[1] = t[2] = 0;
+        return;
+    }
+    for (int d = 0; d < 3; d++) { cP[d] /= w; cQ[d] /= w; }
+    memset(H, 0, sizeof H);
+    for (int i = 0; i < N; i++) {
+        double dp[3], dq[3];
+        if (!mask[i]) continue;
+        for (int d = 0; d < 3; d++) { dp[d] = P[i * 3 + d] - cP[d]; dq[d] = Q[i * 3 + d] - cQ[d]; }
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) H[r][c] += dp[r] * dq[c];
+    }
+    cov_to_rotation((const double(*)[3])H, R);'''
+KABSCH_CENTRED32 = '''    double w = 0, cP[3] = {0, 0, 0}, cQ[3] = {0, 0, 0}, H[3][3];
+    kahan kP[3] = {{0, 0}}, kQ[3] = {{0, 0}}, kH[9] = {{0, 0}};
+    float fP[3], fQ[3];
+    for (int i = 0; i < N; i++) {
+        if (!mask[i]) continue;
+        for (int d = 0; d < 3; d++) { kadd(&kP[d], (float)P[i * 3 + d]); kadd(&kQ[d], (float)Q[i * 3 + d]); }
+        w += 1.0;
+    }
+    if (w < 3.0) {
+        memcpy(R, IDENT, sizeof IDENT);
+        t[0] = t[1] = t[2] = 0;
+        return;
+    }
+    for (int d = 0; d < 3; d++) { fP[d] = kP[d].s / (float)w; fQ[d] = kQ[d].s / (float)w; cP[d] = fP[d]; cQ[d] = fQ[d]; }
+    for (int i = 0; i < N; i++) {
+        float dp[3], dq[3];
+        if (!mask[i]) continue;
+        for (int d = 0; d < 3; d++) { dp[d] = (float)P[i * 3 + d] - fP[d]; dq[d] = (float)Q[i * 3 + d] - fQ[d]; }
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) kadd(&kH[r * 3 + c], dp[r] * dq[c]);
+    }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) H[r][c] = kH[r * 3 + c].s;
+    cov_to_rotation((const double(*)[3])H, R);'''
+KABSCH_RAW32 = '''    double oP[3] = {0, 0, 0}, oQ[3] = {0, 0, 0}, cP[3], cQ[3], H[3][3], w = 0;
+    kahan sp[3] = {{0, 0}}, sq[3] = {{0, 0}}, h[9] = {{0, 0}};
+    if (OFFSET_MEAN && N > 0) {
+        for (int i = 0; i < N; i++)
+            for (int d = 0; d < 3; d++) { oP[d] += P[i * 3 + d]; oQ[d] += Q[i * 3 + d]; }
+        for (int d = 0; d < 3; d++) { oP[d] /= N; oQ[d] /= N; }
+    }
+    for (int i = 0; i < N; i++) {
+        float p[3], q[3];
+        if (!mask[i]) continue;
+        for (int d = 0; d < 3; d++) { p[d] = (float)(P[i * 3 + d] - oP[d]); q[d] = (float)(Q[i * 3 + d] - oQ[d]); }
+        for (int d = 0; d < 3; d++) { kadd(&sp[d], p[d]); kadd(&sq[d], q[d]); }
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) kadd(&h[r * 3 + c], p[r] * q[c]);
+        w += 1.0;
+    }
+    if (w < 3.0) {
+        memcpy(R, IDENT, sizeof IDENT);
+        t[0] = t[1] = t[2] = 0;
+        return;
+    }
+    for (int d = 0; d < 3; d++) { cP[d] = sp[d].s / w; cQ[d] = sq[d].s / w; }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) H[r][c] = h[r * 3 + c].s - w * cP[r] * cQ[c];
+    cov_to_rotation((const double(*)[3])H, R);
+    for (int d = 0; d < 3; d++) { cP[d] += oP[d]; cQ[d] += oQ[d]; }'''
+
+
+def _fp32_sums(s: str) -> str:
+    """TM sums, weights and score-matrix entries in FP32 (needs kahan/kadd)."""
+    s = _sub(s, '''    double d0sq = dmax(d0 * d0, 1e-12), sd8sq = sd8 * sd8, sum = 0;
+    for (int i = 0; i < N; i++) {
+        double d2;
+        if (!v[i]) continue;
+        d2 = dist2_at(p + 3 * i, q + 3 * i, R, t);
+        if (!use_d8 || d2 <= sd8sq) sum += 1.0 / (1.0 + d2 / d0sq);
+    }
+    return sum / dmax(Lnorm, 1.0);''', '''    double d0sq = dmax(d0 * d0, 1e-12), sd8sq = sd8 * sd8;
+    kahan sum = {0, 0};
+    for (int i = 0; i < N; i++) {
+        double d2;
+        if (!v[i]) continue;
+        d2 = dist2_at(p + 3 * i, q + 3 * i, R, t);
+        if (!use_d8 || d2 <= (double)(float)sd8sq) kadd(&sum, tmterm(d2, d0sq));
+    }
+    return (double)sum.s / dmax(Lnorm, 1.0);''')
+    s = _sub(s, '''            w[i] = v[i] ? 1.0 / (1.0 + dist2_at(p + 3 * i, q + 3 * i, R, t) / d0sq) : 0.0;''',
+             '''            w[i] = v[i] ? (double)tmterm(dist2_at(p + 3 * i, q + 3 * i, R, t), d0sq) : 0.0;''')
+    s = _sub(s, '''                    double dx = m[0] - n[0], dy = m[1] - n[1], dz = m[2] - n[2];
+                    double d2 = dx * dx + dy * dy + dz * dz;
+                    smat[(size_t)a * nlen + b] = d2 <= sd8sq ? 1.0 / (1.0 + d2 / d0sq_dp) : 0.0;''',
+             '''                    float dx = (float)m[0] - (float)n[0], dy = (float)m[1] - (float)n[1],
+                          dz = (float)m[2] - (float)n[2];
+                    float d2 = dx * dx + dy * dy + dz * dz;
+                    smat[(size_t)a * nlen + b] = d2 <= (float)sd8sq ? (double)tmterm(d2, d0sq_dp) : 0.0;''')
+    s = _sub(s, '''            for (int i = 0; i < na; i++)
+                sc += 1.0 / (1.0 + dist2_at(Pa + 3 * i, Qa + 3 * i, nR, nt) / d0sq_s);
+            sc /= dmax(Lnorm, 1.0);''', '''            {
+                kahan ks = {0, 0};
+                for (int i = 0; i < na; i++) kadd(&ks, tmterm(dist2_at(Pa + 3 * i, Qa + 3 * i, nR, nt), d0sq_s));
+                sc = (double)ks.s / dmax(Lnorm, 1.0);
+            }''')
+    s = _sub(s, '''                    moved[i * 3 + d] = pred[i * 3] * cR[d] + pred[i * 3 + 1] * cR[3 + d] +
+                                       pred[i * 3 + 2] * cR[6 + d] + ct[d];''',
+             '''                    moved[i * 3 + d] = (float)pred[i * 3] * (float)cR[d] + (float)pred[i * 3 + 1] * (float)cR[3 + d] +
+                                       (float)pred[i * 3 + 2] * (float)cR[6 + d] + (float)ct[d];''')
+    s = _sub(s, '''                double dx = m[0] - n[0], dy = m[1] - n[1], dz = m[2] - n[2];
+                double sc = 1.0 / (1.0 + (dx * dx + dy * dy + dz * dz) / d01sq);''',
+             '''                float dx = (float)m[0] - (float)n[0], dy = (float)m[1] - (float)n[1], dz = (float)m[2] - (float)n[2];
+                double sc = (double)tmterm(dx * dx + dy * dy + dz * dz, d01sq);''')
+    return s
+
+
+def variant_sources(src: str) -> dict[str, str]:
+    base = _sub(src, DIST64, DIST32)
+    out = {"dist32": base}
+    for name, acc in (("kahan32", KAHAN), ("plain32", PLAIN)):
+        s = _sub(base, IMIN, IMIN + acc)
+        out[name] = _fp32_sums(_sub(s, KABSCH64, KABSCH_CENTRED32))
+    for name, mean in (("raw32", 0), ("raw32c", 1)):
+        s = _sub(base, IMIN, IMIN + PLAIN)
+        s = _fp32_sums(_sub(s, KABSCH64 + '''
+    for (int d = 0; d < 3; d++)
+        t[d] = cQ[d] - (cP[0] * R[0 * 3 + d] + cP[1] * R[1 * 3 + d] + cP[2] * R[2 * 3 + d]);''', KABSCH_RAW32 + '''
+    for (int d = 0; d < 3; d++)
+        t[d] = cQ[d] - (cP[0] * R[0 * 3 + d] + cP[1] * R[1 * 3 + d] + cP[2] * R[2 * 3 + d]);'''))
+        out[name] = f"#define OFFSET_MEAN {mean}\n" + s
+    return out
+
+
+def build(names):
+    os.makedirs(OUT, exist_ok=True)
+    src = open(os.path.join(HERE, "indialign_oracle.c")).read()
+    libs = {}
+    for name, s in variant_sources(src).items():
+        if names and name not in names:
+            continue
+        c = os.path.join(OUT, f"{name}.c")
+        so = os.path.join(OUT, f"lib{name}.so")
+        with open(c, "w") as f:
+            f.write(s)
+        subprocess.run(["gcc", "-O3", "-std=c11", "-fPIC", "-fopenmp", "-I", HERE, "-shared", "-o", so, c, "-lm"],
+                       check=True)
+        libs[name] = so
+    return libs
+
+
+def compare(pairs, libs, label):
+    ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
+    st = ctypes.CDLL(STAGES_SO)
+    st.ref_tm_score.restype = ctypes.c_double
+
+    def rescore(p, R, t):
+        d0, d0s, sd8 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        st.ref_d0(ctypes.c_double(p.lnorm), ctypes.byref(d0), ctypes.byref(d0s), ctypes.byref(sd8))
+        arrs = [np.ascontiguousarray(a) for a in (p.pred.reshape(-1), p.native.reshape(-1), p.valid, R, t)]
+        ptr = [ctypes.c_void_p(a.ctypes.data) for a in arrs]
+        return st.ref_tm_score(*ptr, d0, ctypes.c_double(p.lnorm), sd8, ctypes.c_int(len(p.valid)),
+                               ctypes.c_int(0))
+
+    t0 = time.time()
+    _, sref, _, _ = abi.run_batch(ref, pairs)
+    print(f"{label}: {len(pairs)} pairs, reference build {time.time() - t0:.0f} s", flush=True)
+    for name, so in libs.items():
+        lib = abi.bind_reference_abi(ctypes.CDLL(so), prefix="ora_")
+        t0 = time.time()
+        _, _, R, t = abi.run_batch(lib, pairs, prefix="ora_")
+        d = np.array([rescore(p, R[k], t[k]) for k, p in enumerate(pairs)]) - sref
+        print(f"  {name:8s} {time.time() - t0:4.0f} s  mean {d.mean():+.2e}  worst {d.min():+.2e}  "
+              f"best {d.max():+.2e}  below -1e-6: {int((d < -1e-6).sum())}  "
+              f"below -1e-4: {int((d < -1e-4).sum())}", flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--pairs", type=int, default=400, help="pairs of the 4096-pair shape (L 40-300)")
+    ap.add_argument("--seed", type=int, default=21)
+    ap.add_argument("--hard", type=int, default=160, help="hard pairs with L <= 400 (0: none)")
+    ap.add_argument("--hard-seed", type=int, default=22)
+    ap.add_argument("--variants", nargs="*", default=[])
+    a = ap.parse_args()
+    if not (os.path.exists(REF_SO) and os.path.exists(STAGES_SO)):
+        raise SystemExit("reference build missing: make -C oracle ref")
+    libs = build(a.variants)
+    if a.pairs:
+        compare(W.batch(a.pairs, 40, 300, seed=a.seed), libs, f"batch L 40-300 seed {a.seed}")
+    if a.hard:
+        hard = [p for p in W.hard(4 * a.hard, seed=a.hard_seed) if p.pred.shape[0] <= 400][:a.hard]
+        compare(hard, libs, f"hard L <= 400 seed {a.hard_seed}")
+
+
+if __name__ == "__main__":
+    main()
