@@ -20,9 +20,11 @@ batches).
            buffers: host->device copies of the inputs and the device->host
            read of the results inside the timed region.
   roofline the dominant kernel of the learned step (by summed device time):
-           algorithmic FP64 flops / its device time against the measured FP64
-           FMA peak of the GPU (indialign_fp64_peak); NW chains: 18 flop per
-           NW cell + 55 per refine residue visit, bank: 55 per residue visit.
+           algorithmic flops / its device time against the GPU's measured FMA
+           peak of the precision the kernel's work runs in -- NW chains: FP64
+           (indialign_fp64_peak), 18 flop per NW cell + 55 per refine residue
+           visit; seed bank: FP32 (indialign_fp32_peak), 55 per residue
+           visit.
   cpu_baseline  the reference's own build (oracle/_ref, OpenMP batch entry)
            on this host's cores over a stratified sample of the timed pairs,
            bounded to ~25 s.
@@ -446,21 +448,22 @@ def main():
                "d2h_bytes_per_step": 104 * n_timed // args.steps}
 
     if rank == 0:
-        peak = ia.fp64_peak_tflops(local)
         kern = np.mean(lrn["kern"], 0)
         ctr = np.mean(lrn["ctr"], 0)
         step_ms = l_ms / args.steps
         if kern[0] >= kern[1]:
             flops = FLOP_PER_CELL * ctr[0] + FLOP_PER_VISIT * ctr[1]
             kname, kms = "k_chain (NW chains: score matrix + NW + Kabsch + refine)", kern[0]
+            bound, peak, src = "fp64", ia.fp64_peak_tflops(local), "measured FP64 FMA rate (indialign_fp64_peak)"
         else:
             flops = FLOP_PER_VISIT * ctr[2]
             kname, kms = "k_bank (seed x cutoff refine items)", kern[1]
+            bound, peak, src = "fp32", ia.fp32_peak_tflops(local), "measured FP32 FMA rate (indialign_fp32_peak)"
         achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else None
         cyc = ctr[8:12]
-        roofline = {"kernel": kname, "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        roofline = {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak if achieved else None, "traffic": None,
-                    "peak_source": "measured FP64 FMA rate (indialign_fp64_peak) in this run",
+                    "peak_source": f"{src} in this run",
                     "kernel_ms_per_step": float(kms), "kernel_share": float(kms / step_ms),
                     "kernel_ms": {"k_chain": float(kern[0]), "k_bank": float(kern[1]), "k_rank": float(kern[4])},
                     "nw_cells_per_step": int(ctr[0]), "chain_visits_per_step": int(ctr[1]),
@@ -494,8 +497,8 @@ def main():
                                                      "pairs_below_ref_minus_1e-6": int(np.sum(d < -1e-6))}
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64+f32 (seed-bank residue visits f32)", "data": "synthetic",
                 "config": {"workload": desc, "step_pairs": args.step_pairs, "pairs_timed_per_gpu": n_timed,
                            "mode": (f"learned (top_k {args.top_k}, margin {args.margin}, audit {args.audit}, "
                                     f"rank_mask {args.rank_mask or 'default'})"

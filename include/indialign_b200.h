@@ -278,8 +278,12 @@ int indialign_mlp_adam(float *d_blob, const float *d_grad, float *d_m, float *d_
                        float lr, float beta1, float beta2, float eps, void *stream);
 
 /* Measured FP64 FMA throughput of the device in TFLOP/s (the roofline
- * denominator for the search kernels, which are FP64 SIMT work). */
+ * denominator for the FP64 SIMT kernels: NW chains, Kabsch). */
 int indialign_fp64_peak(int device, double *tflops);
+
+/* Measured FP32 FMA throughput of the device in TFLOP/s (the roofline
+ * denominator for the seed-bank kernel, whose residue visits run in FP32). */
+int indialign_fp32_peak(int device, double *tflops);
 
 /* Diagnostic: y[i] = the search kernels' Newton-Raphson reciprocal of x[i],
  * computed on the device (host arrays of n doubles). */

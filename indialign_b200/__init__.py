@@ -105,6 +105,8 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.indialign_tmscore_search_padded.restype = ctypes.c_int
     lib.indialign_fp64_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.indialign_fp64_peak.restype = ctypes.c_int
+    lib.indialign_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.indialign_fp32_peak.restype = ctypes.c_int
     lib.indialign_candidate_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.indialign_candidate_count.restype = ctypes.c_int
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
@@ -374,4 +376,13 @@ def fp64_peak_tflops(device: int = 0) -> float:
     rc = load().indialign_fp64_peak(device, ctypes.byref(v))
     if rc != 0:
         raise IndialignError(f"indialign_fp64_peak rc={rc}")
+    return v.value
+
+
+def fp32_peak_tflops(device: int = 0) -> float:
+    """Measured FP32 FMA throughput (TFLOP/s) of the device."""
+    v = ctypes.c_double(0.0)
+    rc = load().indialign_fp32_peak(device, ctypes.byref(v))
+    if rc != 0:
+        raise IndialignError(f"indialign_fp32_peak rc={rc}")
     return v.value

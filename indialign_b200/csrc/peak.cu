@@ -1,8 +1,9 @@
-// FP64 pipe throughput probe: the denominator of the search kernels'
-// roofline.  The search is FP64 SIMT work (score matrices, NW, Kabsch); it
-// uses neither HBM bandwidth nor tensor cores to any extent, so its ceiling
-// is the FP64 FMA rate of the SMs, measured here with independent FMA chains
-// (8 per thread, enough to hide FMA latency at full occupancy).
+// FP64 and FP32 pipe throughput probes: the denominators of the search
+// kernels' rooflines.  The search is SIMT work (FP64 score matrices, NW and
+// Kabsch; FP32 seed-bank residue visits); it uses neither HBM bandwidth nor
+// tensor cores to any extent, so its ceiling is the FMA rate of the SMs,
+// measured here with independent FMA chains (8 per thread, enough to hide
+// FMA latency at full occupancy).
 #include <cuda_runtime.h>
 
 #include "../../include/indialign_b200.h"
@@ -10,36 +11,38 @@
 
 namespace ia {
 
-__global__ void k_fp64_fma(double *out, int iters, double a, double b) {
-    double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
-    double x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+template <typename T>
+__global__ void k_fma_chains(T *out, int iters, T a, T b) {
+    T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3;
+    T x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
     for (int i = 0; i < iters; i++) {
         x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
         x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
     }
-    double s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
-    if (s == 12345.678) out[0] = s;  // keeps the chains live
+    T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == (T)12345.678) out[0] = s;  // keeps the chains live
 }
 
-}  // namespace ia
-
-extern "C" int indialign_fp64_peak(int device, double *tflops) {
+// Best of 5 timed launches of 8 independent FMA chains per thread.
+template <typename T>
+static int fma_peak(int device, double *tflops) {
     if (!tflops) return INDIALIGN_E_INPUT;
     if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return INDIALIGN_E_CUDA;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device < 0 ? 0 : device) != cudaSuccess)
         return INDIALIGN_E_CUDA;
-    double *d = nullptr;
+    T *d = nullptr;
     if (cudaMalloc(&d, 64) != cudaSuccess) return INDIALIGN_E_CUDA;
     const int blocks = sms * 8, threads = 256, iters = 1 << 14;
+    const T a = (T)0.999999, b = (T)1e-7;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    ia::k_fp64_fma<<<blocks, threads>>>(d, iters / 8, 0.999999, 1e-7);  // warm-up
+    k_fma_chains<T><<<blocks, threads>>>(d, iters / 8, a, b);  // warm-up
     float best = 1e30f;
     for (int r = 0; r < 5; r++) {
         cudaEventRecord(e0);
-        ia::k_fp64_fma<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+        k_fma_chains<T><<<blocks, threads>>>(d, iters, a, b);
         cudaEventRecord(e1);
         cudaEventSynchronize(e1);
         float ms = 0;
@@ -54,6 +57,12 @@ extern "C" int indialign_fp64_peak(int device, double *tflops) {
     *tflops = 2.0 * 8.0 * (double)iters * blocks * threads / (best * 1e-3) / 1e12;
     return INDIALIGN_OK;
 }
+
+}  // namespace ia
+
+extern "C" int indialign_fp64_peak(int device, double *tflops) { return ia::fma_peak<double>(device, tflops); }
+
+extern "C" int indialign_fp32_peak(int device, double *tflops) { return ia::fma_peak<float>(device, tflops); }
 
 namespace ia {
 __global__ void k_rcp_check(const double *x, double *y, int n) {
