@@ -1,7 +1,7 @@
 """Precision study of the search (design evidence; test infrastructure only).
 
 Rebuilds the C oracle (indialign_oracle.c) with its arithmetic lowered to
-FP32 in five ways, runs each variant's batch search beside the reference
+FP32 in six ways, runs each variant's batch search beside the reference
 build (_ref/libindialign_ref.so), rescores every variant's final (R, t) in
 FP64 with the reference's own tm_score_no_d8 (_ref/libindialign_ref_stages.so)
 and prints the per-pair change of the final TM-score against the reference:
@@ -12,6 +12,12 @@ and prints the per-pair change of the final TM-score against the reference:
   plain32     the same with plain FP32 sums
   raw32       plain FP32 one-pass raw moments about the origin
   raw32c      the same about the mean of each point set
+  bank32      only the seed banks (evaluate_seed_bank, the detailed searches'
+              banks, gapless threading) lowered, in the GPU seed-bank
+              kernel's form: point sets centred on their FP64 mean and
+              converted to FP32, FP32 distances / inlier tests / raw moments,
+              FP32 item scores with a compensated sum, FP64 eigen-solves, the
+              winner rescored in FP64; everything else FP64
 
 Variant sources and libraries go to oracle/_variants/.  The variants are
 compiled without -ffast-math (it would fold the Kahan compensation away).
@@ -193,6 +199,185 @@ def _fp32_sums(s: str) -> str:
     return s
 
 
+BANK32_HELPERS = r"""
+/* ---- bank32: the GPU seed bank's arithmetic ---- */
+static void mean3(const double *X, int N, double *o) {
+    o[0] = o[1] = o[2] = 0;
+    for (int i = 0; i < N; i++)
+        for (int d = 0; d < 3; d++) o[d] += X[3 * i + d];
+    for (int d = 0; d < 3; d++) o[d] = N > 0 ? o[d] / N : 0.0;
+}
+static float *centred32(const double *X, int N, const double *o) {
+    float *f = (float *)malloc(sizeof(float) * 3 * (size_t)(N > 0 ? N : 1));
+    for (int i = 0; i < N; i++)
+        for (int d = 0; d < 3; d++) f[3 * i + d] = (float)(X[3 * i + d] - o[d]);
+    return f;
+}
+typedef struct { float sp[3], sq[3], h[9]; int w; } mom32;
+static void m32_add(mom32 *m, const float *p, const float *q) {
+    for (int d = 0; d < 3; d++) { m->sp[d] += p[d]; m->sq[d] += q[d]; }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) m->h[3 * r + c] += p[r] * q[c];
+    m->w++;
+}
+static void m32_kabsch(const mom32 *m, double *R, double *t) {
+    double cP[3], cQ[3], H[3][3];
+    if (m->w < 3) { memcpy(R, IDENT, sizeof IDENT); t[0] = t[1] = t[2] = 0; return; }
+    for (int d = 0; d < 3; d++) { cP[d] = m->sp[d] / (double)m->w; cQ[d] = m->sq[d] / (double)m->w; }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) H[r][c] = m->h[3 * r + c] - m->sp[r] * cQ[c];
+    cov_to_rotation((const double(*)[3])H, R);
+    for (int d = 0; d < 3; d++) t[d] = cQ[d] - (cP[0] * R[d] + cP[1] * R[3 + d] + cP[2] * R[6 + d]);
+}
+static float d2_32(const float *p, const float *q, const float *Rf, const float *tf) {
+    float dx = p[0] * Rf[0] + p[1] * Rf[3] + p[2] * Rf[6] + tf[0] - q[0];
+    float dy = p[0] * Rf[1] + p[1] * Rf[4] + p[2] * Rf[7] + tf[1] - q[1];
+    float dz = p[0] * Rf[2] + p[1] * Rf[5] + p[2] * Rf[8] + tf[2] - q[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+static void rt32(const double *R, const double *t, float *Rf, float *tf) {
+    for (int a = 0; a < 9; a++) Rf[a] = (float)R[a];
+    for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
+}
+static void refine32(const float *P, const float *Q, const uint8_t *v, int N, float cut2, int max_iter,
+                     double *R, double *t) {
+    int prev = -1;
+    for (int it = 0; it < max_iter; it++) {
+        float Rf[9], tf[3];
+        mom32 m;
+        int c = 0;
+        memset(&m, 0, sizeof m);
+        rt32(R, t, Rf, tf);
+        for (int i = 0; i < N; i++) {
+            if (!v[i]) continue;
+            if (d2_32(P + 3 * i, Q + 3 * i, Rf, tf) <= cut2) { m32_add(&m, P + 3 * i, Q + 3 * i); c++; }
+        }
+        if (c >= 3) m32_kabsch(&m, R, t);
+        if (c == prev) break;
+        prev = c;
+    }
+}
+static double score32(const float *P, const float *Q, const uint8_t *v, int N, const double *R, const double *t,
+                      double d0, double sd8, double Lnorm, int use_d8) {
+    float Rf[9], tf[3], d0sq = (float)dmax(d0 * d0, 1e-12), sd8sq = (float)(sd8 * sd8), sum = 0.f, comp = 0.f;
+    rt32(R, t, Rf, tf);
+    for (int i = 0; i < N; i++) {
+        float d2;
+        if (!v[i]) continue;
+        d2 = d2_32(P + 3 * i, Q + 3 * i, Rf, tf);
+        if (!use_d8 || d2 <= sd8sq) {
+            float y = 1.0f / (1.0f + d2 / d0sq) - comp, s2 = sum + y;
+            comp = (s2 - sum) - y;
+            sum = s2;
+        }
+    }
+    return (double)sum / dmax(Lnorm, 1.0);
+}
+static void to_caller(const double *oP, const double *oQ, const double *R, double *t) {
+    for (int d = 0; d < 3; d++) t[d] += oQ[d] - (oP[0] * R[d] + oP[1] * R[3 + d] + oP[2] * R[6 + d]);
+}
+"""
+
+BANK32_SEED_BANK = r"""static OraSeed seed_bank(const double *p, const double *q, const uint8_t *valid,
+                         const uint8_t *seeds, int K, const double *cands,
+                         int C, double d0, double sd8, double Lnorm, int N,
+                         int max_iter, int use_d8, double early_term) {
+    OraSeed best;
+    double R[9], t[3], oP[3], oQ[3];
+    float *Pf, *Qf;
+    memset(&best, 0, sizeof best);
+    best.score = -1e30;
+    mean3(p, N, oP); mean3(q, N, oQ);
+    Pf = centred32(p, N, oP); Qf = centred32(q, N, oQ);
+    for (int k = 0; k < K; k++) {
+        if (best.score >= early_term) break;
+        for (int c = 0; c < C; c++) {
+            mom32 m;
+            double sc;
+            memset(&m, 0, sizeof m);
+            for (int i = 0; i < N; i++)
+                if (seeds[(size_t)k * N + i] & valid[i]) m32_add(&m, Pf + 3 * i, Qf + 3 * i);
+            m32_kabsch(&m, R, t);
+            refine32(Pf, Qf, valid, N, (float)(cands[c] * cands[c]), max_iter, R, t);
+            sc = score32(Pf, Qf, valid, N, R, t, d0, sd8, Lnorm, use_d8);
+            if (sc > best.score) {
+                best.score = sc;
+                memcpy(best.R, R, 72);
+                memcpy(best.t, t, 24);
+            }
+        }
+    }
+    if (best.score > -1e30) {
+        to_caller(oP, oQ, best.R, best.t);
+        best.score = ora_tm_score(p, q, valid, best.R, best.t, d0, Lnorm, sd8, N, use_d8);
+    }
+    free(Pf); free(Qf);
+    return best;
+}
+
+"""
+
+BANK32_GAPLESS_OLD = r"""    for (int k = -kr; k <= kr; k += stride) {
+        int na = 0;
+        double R[9], t[3], sc;
+        if (k == 0) continue;
+        for (int i = 0; i < N; i++) {
+            int j = i - k;
+            if (j < 0 || j >= N || !pv[i] || !nv[j]) continue;
+            memcpy(Pa + 3 * na, p + 3 * i, 24);
+            memcpy(Qa + 3 * na, q + 3 * j, 24);
+            pm[na++] = 1;
+        }
+        if (na < min_ali) continue;
+        ora_kabsch(Pa, Qa, pm, na, R, t);
+        refine_from_rt(p, q, v, d0s, N, 5, R, t, sel);
+        sc = ora_tm_score(p, q, v, R, t, d0, Lnorm, 0, N, 0);
+        if (sc > best.score) {
+            best.score = sc;
+            memcpy(best.R, R, 72); memcpy(best.t, t, 24);
+        }
+    }"""
+BANK32_GAPLESS_NEW = r"""    {
+        double oP[3], oQ[3];
+        float *Pf, *Qf;
+        mean3(p, N, oP); mean3(q, N, oQ);
+        Pf = centred32(p, N, oP); Qf = centred32(q, N, oQ);
+        for (int k = -kr; k <= kr; k += stride) {
+            mom32 m;
+            double R[9], t[3], sc;
+            if (k == 0) continue;
+            memset(&m, 0, sizeof m);
+            for (int i = 0; i < N; i++) {
+                int j = i - k;
+                if (j < 0 || j >= N || !pv[i] || !nv[j]) continue;
+                m32_add(&m, Pf + 3 * i, Qf + 3 * j);
+            }
+            if (m.w < min_ali) continue;
+            m32_kabsch(&m, R, t);
+            refine32(Pf, Qf, v, N, (float)(d0s * d0s), 5, R, t);
+            sc = score32(Pf, Qf, v, N, R, t, d0, 0.0, Lnorm, 0);
+            if (sc > best.score) {
+                best.score = sc;
+                memcpy(best.R, R, 72); memcpy(best.t, t, 24);
+            }
+        }
+        if (best.score > -1e30) {
+            to_caller(oP, oQ, best.R, best.t);
+            best.score = ora_tm_score(p, q, v, best.R, best.t, d0, Lnorm, 0, N, 0);
+        }
+        free(Pf); free(Qf);
+    }"""
+
+
+def _bank32(src: str) -> str:
+    """Only the seed banks lowered, in the GPU seed-bank kernel's form."""
+    marker = "/* ---- seeds (indialign_c/seeds.h)"
+    s = _sub(src, marker, BANK32_HELPERS + "\n" + marker)
+    a, b = s.index("static OraSeed seed_bank("), s.index("void ora_seed_bank(")
+    s = s[:a] + BANK32_SEED_BANK + s[b:]
+    return _sub(s, BANK32_GAPLESS_OLD, BANK32_GAPLESS_NEW)
+
+
 def variant_sources(src: str) -> dict[str, str]:
     base = _sub(src, DIST64, DIST32)
     out = {"dist32": base}
@@ -207,6 +392,7 @@ def variant_sources(src: str) -> dict[str, str]:
     for (int d = 0; d < 3; d++)
         t[d] = cQ[d] - (cP[0] * R[0 * 3 + d] + cP[1] * R[1 * 3 + d] + cP[2] * R[2 * 3 + d]);'''))
         out[name] = f"#define OFFSET_MEAN {mean}\n" + s
+    out["bank32"] = _bank32(src)
     return out
 
 
