@@ -396,15 +396,15 @@ def variant_sources(src: str) -> dict[str, str]:
     return out
 
 
-def build(names):
-    os.makedirs(OUT, exist_ok=True)
+def build(names, out_dir: str = OUT):
+    os.makedirs(out_dir, exist_ok=True)
     src = open(os.path.join(HERE, "indialign_oracle.c")).read()
     libs = {}
     for name, s in variant_sources(src).items():
         if names and name not in names:
             continue
-        c = os.path.join(OUT, f"{name}.c")
-        so = os.path.join(OUT, f"lib{name}.so")
+        c = os.path.join(out_dir, f"{name}.c")
+        so = os.path.join(out_dir, f"lib{name}.so")
         with open(c, "w") as f:
             f.write(s)
         subprocess.run(["gcc", "-O3", "-std=c11", "-fPIC", "-fopenmp", "-I", HERE, "-shared", "-o", so, c, "-lm"],
