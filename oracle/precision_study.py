@@ -1,10 +1,11 @@
 """Precision study of the search (design evidence; test infrastructure only).
 
 Rebuilds the C oracle (indialign_oracle.c) with its arithmetic lowered to
-FP32 in six ways, runs each variant's batch search beside the reference
-build (_ref/libindialign_ref.so), rescores every variant's final (R, t) in
-FP64 with the reference's own tm_score_no_d8 (_ref/libindialign_ref_stages.so)
-and prints the per-pair change of the final TM-score against the reference:
+FP32 in six ways, and once with its eigen-solve replaced; runs each
+variant's batch search beside the reference build (_ref/libindialign_ref.so),
+rescores every variant's final (R, t) in FP64 with the reference's own
+tm_score_no_d8 (_ref/libindialign_ref_stages.so) and prints the per-pair
+change of the final TM-score against the reference:
 
   dist32      FP32 distances and inlier tests, FP64 moments and sums
   kahan32     FP32 distances, TM terms, score-matrix entries and centred
@@ -18,6 +19,11 @@ and prints the per-pair change of the final TM-score against the reference:
               converted to FP32, FP32 distances / inlier tests / raw moments,
               FP32 item scores with a compensated sum, FP64 eigen-solves, the
               winner rescored in FP64; everything else FP64
+  qcp64       all FP64, every Kabsch eigen-solve by the characteristic
+              polynomial of Horn's key matrix (Newton for its top roots,
+              eigenvector from an adjugate column) instead of Jacobi sweeps,
+              Jacobi kept where the top two eigenvalues lie within 1e-4 of
+              the spectrum's scale; prints the fallback rate
 
 Variant sources and libraries go to oracle/_variants/.  The variants are
 compiled without -ffast-math (it would fold the Kahan compensation away).
@@ -369,6 +375,105 @@ BANK32_GAPLESS_NEW = r"""    {
     }"""
 
 
+QCP64 = r"""
+/* ---- qcp64: the dominant eigenvector of Horn's key matrix F from its
+ * characteristic polynomial (Theobald 2005, "Rapid calculation of RMSDs using
+ * a quaternion-based characteristic polynomial"): P(x) = x^4 - tr(F^2)/2 x^2
+ * - tr(F^3)/3 x + det F (F is traceless), its largest root by Newton from the
+ * upper bound sqrt(tr(F^2)), the second root the same way on P(x)/(x - l1),
+ * the eigenvector from the largest column of adj(F - l1 I).  When
+ * l1 - l2 < 1e-4 sqrt(tr(F^2)) the reference's Jacobi sequence runs instead. */
+long qcp_calls = 0, qcp_fallbacks = 0;
+static double qdet3(double a, double b, double c, double d, double e, double f, double g, double h, double i) {
+    return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+}
+static double qminor(const double A[4][4], int row, int col) {
+    double m[9];
+    int k = 0;
+    for (int i = 0; i < 4; i++) {
+        if (i == row) continue;
+        for (int j = 0; j < 4; j++)
+            if (j != col) m[k++] = A[i][j];
+    }
+    return qdet3(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], m[8]);
+}
+static double qcp_newton_top(double b3, double b2, double b1, double b0, double x, double scale) {
+    /* largest root of x^4 + b3 x^3 + b2 x^2 + b1 x + b0 (b3 = 0) or of the
+     * cubic x^3 + b2 x^2 + b1 x + b0 (b3 < 0 marks the cubic), from above */
+    for (int it = 0; it < 200; it++) {
+        double g, dg, nx;
+        if (b3 >= 0) { g = ((x * x + b2) * x + b1) * x + b0; dg = (4 * x * x + 2 * b2) * x + b1; }
+        else { g = ((x + b2) * x + b1) * x + b0; dg = (3 * x + 2 * b2) * x + b1; }
+        if (!(dg > 0)) break;
+        nx = x - g / dg;
+        if (!(nx < x)) break;
+        if (x - nx <= 1e-16 * scale) return nx;
+        x = nx;
+    }
+    return x;
+}
+static int qcp_rotation(const double F[4][4], double *R) {
+    double F2[4][4], p2 = 0, p3 = 0, dt, c2, c1, scale, l1, l2, A[4][4], q[4] = {1, 0, 0, 0}, best = -1, qn;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            double s = 0;
+            for (int k = 0; k < 4; k++) s += F[i][k] * F[k][j];
+            F2[i][j] = s;
+        }
+    for (int i = 0; i < 4; i++) {
+        p2 += F2[i][i];
+        for (int k = 0; k < 4; k++) p3 += F2[i][k] * F[k][i];
+    }
+    dt = 0;
+    for (int j = 0; j < 4; j++) dt += ((j & 1) ? -1.0 : 1.0) * F[0][j] * qminor(F, 0, j);
+    c2 = -0.5 * p2; c1 = -p3 / 3.0; scale = sqrt(p2);
+    if (!(scale > 0)) return 1;
+    l1 = qcp_newton_top(0.0, c2, c1, dt, scale, scale);
+    l2 = qcp_newton_top(-1.0, l1, c2 + l1 * l1, c1 + l1 * c2 + l1 * l1 * l1, l1, scale);
+    if (l1 - l2 < 1e-4 * scale) return 1;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) A[i][j] = F[i][j] - (i == j ? l1 : 0.0);
+    for (int c = 0; c < 4; c++) {
+        double v[4], n;
+        for (int r = 0; r < 4; r++) v[r] = (((r + c) & 1) ? -1.0 : 1.0) * qminor(A, c, r);
+        n = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+        if (n > best) { best = n; memcpy(q, v, sizeof q); }
+    }
+    if (!(best > 0)) return 1;
+    qn = sqrt(best);
+    for (int i = 0; i < 4; i++) q[i] /= qn;
+    R[0] = q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3];
+    R[1] = 2 * (q[1] * q[2] + q[0] * q[3]);
+    R[2] = 2 * (q[1] * q[3] - q[0] * q[2]);
+    R[3] = 2 * (q[1] * q[2] - q[0] * q[3]);
+    R[4] = q[0] * q[0] - q[1] * q[1] + q[2] * q[2] - q[3] * q[3];
+    R[5] = 2 * (q[2] * q[3] + q[0] * q[1]);
+    R[6] = 2 * (q[1] * q[3] + q[0] * q[2]);
+    R[7] = 2 * (q[2] * q[3] - q[0] * q[1]);
+    R[8] = q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3];
+    return 0;
+}
+"""
+QCP64_CALL_OLD = """    jacobi4(F, V);"""
+QCP64_CALL_NEW = """    {
+        int fb;
+#pragma omp atomic
+        qcp_calls++;
+        fb = qcp_rotation((const double(*)[4])F, R);
+        if (!fb) return;
+#pragma omp atomic
+        qcp_fallbacks++;
+    }
+    jacobi4(F, V);"""
+
+
+def _qcp64(src: str) -> str:
+    """The eigen-solve of every Kabsch by the characteristic polynomial."""
+    marker = "/* Horn's quaternion matrix from the 3x3 covariance"
+    s = _sub(src, marker, QCP64 + "\n" + marker)
+    return _sub(s, QCP64_CALL_OLD, QCP64_CALL_NEW)
+
+
 def _bank32(src: str) -> str:
     """Only the seed banks lowered, in the GPU seed-bank kernel's form."""
     marker = "/* ---- seeds (indialign_c/seeds.h)"
@@ -393,6 +498,7 @@ def variant_sources(src: str) -> dict[str, str]:
         t[d] = cQ[d] - (cP[0] * R[0 * 3 + d] + cP[1] * R[1 * 3 + d] + cP[2] * R[2 * 3 + d]);'''))
         out[name] = f"#define OFFSET_MEAN {mean}\n" + s
     out["bank32"] = _bank32(src)
+    out["qcp64"] = _qcp64(src)
     return out
 
 
@@ -434,9 +540,14 @@ def compare(pairs, libs, label):
         t0 = time.time()
         _, _, R, t = abi.run_batch(lib, pairs, prefix="ora_")
         d = np.array([rescore(p, R[k], t[k]) for k, p in enumerate(pairs)]) - sref
+        extra = ""
+        if hasattr(lib, "qcp_calls"):
+            calls = ctypes.c_long.in_dll(lib, "qcp_calls").value
+            fb = ctypes.c_long.in_dll(lib, "qcp_fallbacks").value
+            extra = f"  eigen-solves {calls}, Jacobi fallbacks {fb} ({fb / max(calls, 1):.1e})"
         print(f"  {name:8s} {time.time() - t0:4.0f} s  mean {d.mean():+.2e}  worst {d.min():+.2e}  "
               f"best {d.max():+.2e}  below -1e-6: {int((d < -1e-6).sum())}  "
-              f"below -1e-4: {int((d < -1e-4).sum())}", flush=True)
+              f"below -1e-4: {int((d < -1e-4).sum())}{extra}", flush=True)
 
 
 def main():
