@@ -289,6 +289,12 @@ int indialign_fp32_peak(int device, double *tflops);
  * computed on the device (host arrays of n doubles). */
 int indialign_selftest_rcp(int n, const double *x, double *y);
 
+/* Diagnostic: R[9i..9i+8] = the search kernels' rotation (Horn quaternion,
+ * aligned_d = sum_k p_k R[3k+d]) for the 3x3 covariance H[9i..9i+8] (row
+ * major, sum of p q^T), computed on the device (host arrays of n matrices);
+ * the counterpart of the reference's cov_to_rotation (indialign_c/core.h:64-90). */
+int indialign_selftest_rotation(int n, const double *H, double *R);
+
 /* Text of the last error on this thread ("" if none). */
 const char *indialign_last_error(void);
 

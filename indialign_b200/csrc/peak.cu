@@ -83,3 +83,33 @@ extern "C" int indialign_selftest_rcp(int n, const double *x, double *y) {
     cudaFree(d);
     return e == cudaSuccess ? INDIALIGN_OK : INDIALIGN_E_CUDA;
 }
+
+namespace ia {
+__global__ void k_rotation_check(const double *H9, double *R9, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double H[3][3];
+#pragma unroll
+    for (int a = 0; a < 9; a++) H[a / 3][a % 3] = H9[9 * (size_t)i + a];
+    double R[9];
+    cov_to_rotation(H, R);
+#pragma unroll
+    for (int a = 0; a < 9; a++) R9[9 * (size_t)i + a] = R[a];
+}
+}  // namespace ia
+
+// Diagnostic: the search's eigen-solve on the device for n host covariances
+// (tests compare it with the reference's rotation).
+extern "C" int indialign_selftest_rotation(int n, const double *H, double *R) {
+    if (n <= 0 || !H || !R) return INDIALIGN_E_INPUT;
+    double *d = nullptr;
+    const size_t bytes = 9 * sizeof(double) * (size_t)n;
+    if (cudaMalloc(&d, 2 * bytes) != cudaSuccess) return INDIALIGN_E_CUDA;
+    cudaError_t e = cudaMemcpy(d, H, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        ia::k_rotation_check<<<(n + 127) / 128, 128>>>(d, d + 9 * (size_t)n, n);
+        e = cudaMemcpy(R, d + 9 * (size_t)n, bytes, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d);
+    return e == cudaSuccess ? INDIALIGN_OK : INDIALIGN_E_CUDA;
+}
