@@ -76,6 +76,37 @@ def test_oracle_length_zero(oracle):
     assert out.score == 7.0
 
 
+def test_oracle_non_finite_coordinates_vs_reference(oracle, ref):
+    """NaN and Inf coordinates: the same final scores as the reference build.
+    A NaN reaches every candidate score, nothing beats the initial -1e30, and
+    the reference then returns an uninitialised (R, t) (indialign_c/search.h:
+    69-70 sets only best.score), so (R, t) are compared only where a
+    candidate was accepted."""
+    rng = np.random.default_rng(3)
+    pairs = []
+    for k in range(5):
+        p = W.make_pair(50, 2.0, rng)
+        if k == 0:
+            p.pred[7, 1] = np.nan
+        elif k == 1:
+            p.native[20, 0] = np.nan
+        elif k == 2:
+            p.pred[:, :] = np.nan
+        elif k == 3:
+            p.native[5, 2] = np.inf
+        else:
+            p.pred[3, 0] = -np.inf
+        pairs.append(p)
+    rc, so, Ro, to = abi.run_batch(oracle, pairs, prefix="ora_")
+    rc2, sr, Rr, tr = abi.run_batch(ref, pairs)
+    assert rc == 0 and rc2 == 0
+    np.testing.assert_allclose(so, sr, atol=1e-12, rtol=0)
+    assert np.all(so[:3] == -1e30) and np.all(sr[:3] == -1e30)
+    ok = so > -1e29
+    np.testing.assert_allclose(Ro[ok], Rr[ok], atol=1e-9)
+    np.testing.assert_allclose(to[ok], tr[ok], atol=1e-7)
+
+
 def _nw_cases():
     import os
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_nw.npz"))
