@@ -143,6 +143,16 @@ def test_learned_mode_rejects_missing_ranker():
     opts.mode = 7
     rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
     assert rc == -4 and "mode" in ia.last_error()
+    blob = np.zeros(ia.RANKER_FLOATS, np.float32)
+    for k in (-1, 33):  # top_k outside 1..32 (0 means the default 8)
+        ia.learned_options(opts, blob, k, 0.02, 0.02, 0, None)
+        rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
+        assert rc == -4 and "top_k" in ia.last_error(), (k, rc, ia.last_error())
+    opts2 = ia.BatchOptions()
+    opts2.device = -1
+    opts2.mode = ia.MODE_COLLECT  # no feature / label buffers
+    rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts2), res)
+    assert rc == -4 and "collect" in ia.last_error()
 
 
 def test_checkpoint_roundtrip(tmp_path):
