@@ -26,7 +26,10 @@ def _atom_c1(line: str):
 
 
 def c1_models(text: str) -> list[np.ndarray]:
-    """C1' coordinates of every model, in file order ([N, 3] each)."""
+    """C1' coordinates of every model closed by ENDMDL, in file order
+    ([N, 3] each); a file without any closed model gives its C1' atoms as
+    one model (benchmark/pdb_hard_benchmark.py:134-150: atoms after the last
+    ENDMDL of a multi-model file are dropped)."""
     models, cur = [], []
     for line in text.splitlines():
         rec = line[:6].strip()
@@ -40,13 +43,28 @@ def c1_models(text: str) -> list[np.ndarray]:
             a = _atom_c1(line)
             if a is not None:
                 cur.append(a[2])
-    if cur:  # a file without MODEL records, or a last model without ENDMDL
+    if not models and cur:
         models.append(np.array(cur))
     return models
 
 
+def c1_chains(text: str) -> dict[str, np.ndarray]:
+    """{chain: C1' coordinates [N, 3] in file order} of the first model
+    (benchmark/pdb_hard_benchmark.py:152-166)."""
+    chains: dict[str, list] = {}
+    for line in text.splitlines():
+        if line[:6].strip() == "ENDMDL":
+            break
+        a = _atom_c1(line)
+        if a is not None:
+            chains.setdefault(a[0], []).append(a[2])
+    return {ch: np.array(v) for ch, v in chains.items()}
+
+
 def c1_by_chain(text: str) -> dict[str, dict[int, np.ndarray]]:
-    """{chain: {residue number: C1' xyz}} of the first model."""
+    """{chain: {residue number: C1' xyz}} of the first model; a repeated
+    residue number keeps its last atom (benchmark/pdb_hard_benchmark.py:
+    168-183)."""
     chains: dict[str, dict[int, np.ndarray]] = {}
     for line in text.splitlines():
         if line[:6].strip() == "ENDMDL":

@@ -31,6 +31,26 @@ def test_c1_roundtrip_and_models():
     assert [m.shape for m in pdb.c1_models(txt)] == [(27, 3)]
 
 
+def test_extraction_rules_follow_the_reference_benchmark():
+    """Records other than ATOM, other atom names and models after the first
+    are ignored where the reference's extraction ignores them; atoms after
+    the last ENDMDL of a multi-model file are dropped."""
+    x = _trace(6, 3)
+    a = pdb.c1_pdb_text(x, chain="A").replace("END\n", "")
+    b = pdb.c1_pdb_text(x[:4] + 1.0, chain="B", first_resnum=20).replace("END\n", "")
+    het = "HETATM    1  C1'   A A  99       1.000   2.000   3.000  1.00  0.00           C\n"
+    other = a.splitlines()[0].replace(" C1' ", " C2' ") + "\n"
+    text = "MODEL        1\n" + a + het + other + b + "ENDMDL\nMODEL        2\n" + a + "ENDMDL\n" + a
+    models = pdb.c1_models(text)
+    assert [m.shape for m in models] == [(10, 3), (6, 3)]  # trailing atoms dropped
+    ch = pdb.c1_chains(text)
+    assert sorted(ch) == ["A", "B"] and ch["A"].shape == (6, 3) and ch["B"].shape == (4, 3)
+    np.testing.assert_allclose(ch["B"], x[:4] + 1.0, atol=5e-4)
+    by = pdb.c1_by_chain(text)
+    assert sorted(by["B"]) == [20, 21, 22, 23] and 99 not in by["A"]
+    assert [m.shape for m in pdb.c1_models(a)] == [(6, 3)]  # no MODEL records: one model
+
+
 def test_pair_by_resnum_marks_each_side():
     a = {1: np.zeros(3), 2: np.ones(3), 5: np.full(3, 2.0)}
     b = {2: np.ones(3), 3: np.zeros(3), 5: np.zeros(3)}
