@@ -75,6 +75,24 @@ def c1_by_chain(text: str) -> dict[str, dict[int, np.ndarray]]:
     return chains
 
 
+def most_divergent_pair(models: list[np.ndarray]) -> tuple[int, int, float]:
+    """(i, j, rmsd) of the two equal-length models with the largest C1' RMSD,
+    the first such pair in scan order; ensembles of more than 20 models are
+    scanned on model 0 and 19 models spread evenly over the rest
+    (benchmark/pdb_hard_benchmark.py:195-207)."""
+    n = len(models)
+    idx = list(range(n))
+    if n > 20:
+        idx = [0] + [int(v) for v in np.linspace(1, n - 1, 19).astype(int)]
+    best = (0, 1, -1.0)
+    for a, i in enumerate(idx):
+        for j in idx[a + 1:]:
+            r = float(np.sqrt(np.mean(np.sum((models[i] - models[j]) ** 2, axis=1))))
+            if r > best[2]:
+                best = (i, j, r)
+    return best
+
+
 def pair_by_resnum(pred: dict[int, np.ndarray], native: dict[int, np.ndarray]) -> Pair:
     """One padded pair over the union of residue numbers (ascending)."""
     res = sorted(set(pred) | set(native))

@@ -51,6 +51,22 @@ def test_extraction_rules_follow_the_reference_benchmark():
     assert [m.shape for m in pdb.c1_models(a)] == [(6, 3)]  # no MODEL records: one model
 
 
+def test_most_divergent_pair():
+    rng = np.random.default_rng(4)
+    base = _trace(20, 5)
+    models = [base + rng.normal(0, 0.2, base.shape) for _ in range(6)]
+    models[4] = base + 5.0  # far from every other model
+    i, j, r = pdb.most_divergent_pair(models)
+    assert 4 in (i, j) and r > 4.0
+    # a large ensemble is scanned on model 0 and 19 evenly spread models
+    many = [base + rng.normal(0, 0.1, base.shape) for _ in range(41)]
+    many[8] = base + 9.0  # not among the scanned models (1, 3, 5, 7, 9, ...)
+    many[40] = base + 3.0  # the last model is always scanned
+    i, j, _ = pdb.most_divergent_pair(many)
+    assert 40 in (i, j) and 8 not in (i, j)
+    assert pdb.most_divergent_pair([base]) == (0, 1, -1.0)
+
+
 def test_pair_by_resnum_marks_each_side():
     a = {1: np.zeros(3), 2: np.ones(3), 5: np.full(3, 2.0)}
     b = {2: np.ones(3), 3: np.zeros(3), 5: np.zeros(3)}
