@@ -4,7 +4,10 @@ formula with the same d0, so differences in the tools' own scoring conventions
 drop out.
 
 * `common_tm`: sum over all residues of 1 / (1 + d^2 / d0^2) after moving pred
-  by (R, t), divided by lnorm -- no d8 cutoff (fair_benchmark.py:57-61).
+  by (R, t), divided by lnorm -- no d8 cutoff (fair_benchmark.py:57-61);
+  `common_tm_masked` counts only residues valid on both sides and divides by
+  their number (pdb_hard_benchmark.py:114-120), the form `compare` uses, so
+  padded PDB pairs (`pdb.ensemble_pair`, `pdb.family_pairs`) compare too.
 * `d0_rna`: the RNA d0 both tools use (fair_benchmark.py:48-55).
 * USalign (`run_usalign`): C1' PDB files in, `-atom " C1'" -TMscore 1 -m
   <file>` (sequence-dependent superposition), the second "TM-score=" of its
@@ -58,6 +61,18 @@ def common_tm(pred: np.ndarray, native: np.ndarray, M: np.ndarray, t: np.ndarray
     moved = pred @ np.asarray(M).T + np.asarray(t)
     d2 = np.sum((moved - native) ** 2, axis=1)
     return float(np.sum(1.0 / (1.0 + d2 / (d0 * d0))) / lnorm)
+
+
+def common_tm_masked(pred: np.ndarray, native: np.ndarray, valid: np.ndarray, M: np.ndarray, t: np.ndarray,
+                     d0: float) -> float:
+    """common_tm over the residues valid on both sides, normalised by their
+    count (benchmark/pdb_hard_benchmark.py:114-120); 0 when none is."""
+    v = np.asarray(valid) != 0
+    if not v.any():
+        return 0.0
+    moved = pred @ np.asarray(M).T + np.asarray(t)
+    d2 = np.sum((moved - native) ** 2, axis=1)
+    return float(np.sum(v / (1.0 + d2 / (d0 * d0))) / v.sum())
 
 
 def matrix_from_result(R9: np.ndarray) -> np.ndarray:
@@ -123,13 +138,16 @@ def parse_usalign_matrix(text: str) -> tuple[np.ndarray, np.ndarray]:
     return M, t
 
 
-def run_usalign(pred: np.ndarray, native: np.ndarray, usalign: str, timeout: float = 30.0):
-    """(score, M, t, seconds) of one USalign run on C1' traces."""
+def run_usalign(pred: np.ndarray, native: np.ndarray, usalign: str, timeout: float = 30.0,
+                pred_valid: np.ndarray | None = None, native_valid: np.ndarray | None = None):
+    """(score, M, t, seconds) of one USalign run on C1' traces (residues
+    invalid on a side are left out of that side's file, with their residue
+    numbers kept)."""
     with tempfile.TemporaryDirectory() as d:
         pp, pn, pm = (os.path.join(d, f) for f in ("pred.pdb", "native.pdb", "matrix.txt"))
-        for path, xyz in ((pp, pred), (pn, native)):
+        for path, xyz, v in ((pp, pred, pred_valid), (pn, native, native_valid)):
             with open(path, "w") as f:
-                f.write(pdb.c1_pdb_text(xyz))
+                f.write(pdb.c1_pdb_text(xyz, v))
         t0 = time.perf_counter()
         out = subprocess.run([usalign, pp, pn, "-atom", " C1'", "-TMscore", "1", "-m", pm],
                              capture_output=True, text=True, timeout=timeout)
@@ -191,15 +209,20 @@ def compare(pairs: list[Pair], usalign: str | None = None, search=None) -> Repor
     t0 = time.perf_counter()
     s, R, t = search(pairs)
     secs = time.perf_counter() - t0
-    common = np.array([common_tm(p.pred, p.native, matrix_from_result(R[k]), t[k], d0_rna(p.lnorm), p.lnorm)
-                       for k, p in enumerate(pairs)])
-    rep = Report(np.asarray(s), common, secs)
+
+    def common(p, M, tt):  # residues valid on both sides, d0 of their count
+        n = int(np.sum(p.valid != 0))
+        return common_tm_masked(p.pred, p.native, p.valid, M, tt, d0_rna(max(n, 1)))
+
+    rep = Report(np.asarray(s), np.array([common(p, matrix_from_result(R[k]), t[k]) for k, p in enumerate(pairs)]),
+                 secs)
     if usalign:
         su, cu, du = [], [], []
         for p in pairs:
-            sc, M, tu, dt = run_usalign(p.pred, p.native, usalign)
+            sc, M, tu, dt = run_usalign(p.pred, p.native, usalign, pred_valid=p.pred_valid,
+                                        native_valid=p.native_valid)
             su.append(sc)
-            cu.append(common_tm(p.pred, p.native, M, tu, d0_rna(p.lnorm), p.lnorm))
+            cu.append(common(p, M, tu))
             du.append(dt)
         rep.self_usalign, rep.common_usalign, rep.seconds_usalign = np.array(su), np.array(cu), np.array(du)
         rep.stats = _stats(rep.common_ours, rep.common_usalign)
@@ -231,13 +254,32 @@ def format_report(rep: Report) -> str:
     return "\n".join(lines)
 
 
+def pdb_pairs(ensembles: list[str], family: list[str]) -> list[Pair]:
+    """Pairs from local PDB files: each ensemble file's most divergent model
+    pair, and a family's later structures against its first."""
+    out = []
+    for path in ensembles:
+        r = pdb.ensemble_pair(open(path).read())
+        if r is not None:
+            out.append(r[0])
+    if family:
+        out += pdb.family_pairs([open(p).read() for p in family])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--pairs", type=int, default=50)
+    ap.add_argument("--pairs", type=int, default=50, help="synthetic random-walk pairs (without PDB input)")
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--usalign", default=None, help="path of a USalign binary")
+    ap.add_argument("--pdb-ensemble", nargs="*", default=[], help="multi-model PDB files")
+    ap.add_argument("--pdb-family", nargs="*", default=[], help="PDB files of one family (first = native)")
     a = ap.parse_args()
-    print(format_report(compare(fair_pairs(a.pairs, a.seed), a.usalign)))
+    pairs = pdb_pairs(a.pdb_ensemble, a.pdb_family) if (a.pdb_ensemble or a.pdb_family) \
+        else fair_pairs(a.pairs, a.seed)
+    if not pairs:
+        raise SystemExit("no pairs")
+    print(format_report(compare(pairs, a.usalign)))
 
 
 if __name__ == "__main__":

@@ -110,6 +110,52 @@ def pair_by_resnum(pred: dict[int, np.ndarray], native: dict[int, np.ndarray]) -
     return Pair(P, Q, v, pv, nv, float(max(int(v.sum()), 1)), 0.0, False)
 
 
+def ensemble_pair(text: str, min_len: int = 30, max_len: int = 4096):
+    """(pair, (i, j, rmsd)) of an NMR-style ensemble's most divergent models,
+    or None when it has fewer than two models, models of different lengths,
+    or a length outside [min_len, max_len] (benchmark/pdb_hard_benchmark.py:
+    257-272).  All residues valid, lnorm = length."""
+    models = c1_models(text)
+    if len(models) < 2 or len({len(m) for m in models}) != 1:
+        return None
+    n = len(models[0])
+    if n < min_len or n > max_len:
+        return None
+    i, j, r = most_divergent_pair(models)
+    ones = np.ones(n, np.uint8)
+    return Pair(np.ascontiguousarray(models[i]), np.ascontiguousarray(models[j]), ones, ones.copy(),
+                ones.copy(), float(n), 0.0, False), (i, j, r)
+
+
+def longest_chain(text: str, min_len: int = 30):
+    """(chain id, {residue number: xyz}) of the first model's longest chain
+    (the first of equal length), or None below min_len residues."""
+    chains = c1_by_chain(text)
+    if not chains:
+        return None
+    best = max(chains, key=lambda c: len(chains[c]))
+    return (best, chains[best]) if len(chains[best]) >= min_len else None
+
+
+def family_pairs(texts: list[str], min_shared: int = 20, max_len: int = 4096) -> list[Pair]:
+    """Structures of one family: the longest chain of the first structure is
+    the native, the longest chain of each later one a prediction, paired by
+    residue number; pairs with fewer than min_shared residues on both sides
+    or more than max_len slots are left out (benchmark/pdb_hard_benchmark.py:
+    355-385)."""
+    chains = [c for c in (longest_chain(t) for t in texts) if c is not None]
+    if len(chains) < 2:
+        return []
+    native = chains[0][1]
+    out = []
+    for _, pred in chains[1:]:
+        p = pair_by_resnum(pred, native)
+        if int(p.valid.sum()) < min_shared or len(p.valid) > max_len:
+            continue
+        out.append(p)
+    return out
+
+
 def pair_padded(pred: np.ndarray, native: np.ndarray, lnorm: float | None = None) -> Pair:
     """Two traces of possibly different lengths, without residue numbers:
     both padded to the longer one with invalid slots.  lnorm defaults to the

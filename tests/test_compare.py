@@ -112,3 +112,51 @@ def test_whole_comparison_with_the_oracle_as_search(oracle, tmp_path):
     text = C.format_report(rep)
     assert "wins" in text and "USalign" in text
     assert "not run" in C.format_report(C.compare(pairs[:2], None, search=search))
+
+
+def test_masked_common_scorer():
+    rng = np.random.default_rng(9)
+    p = C.fair_pairs(1, seed=4)[0]
+    M, t = W.random_rotation(rng), rng.normal(0, 3, 3)
+    v = (rng.uniform(size=len(p.valid)) < 0.7).astype(np.uint8)
+    d0 = C.d0_rna(int(v.sum()))
+    full = C.common_tm(p.pred[v != 0], p.native[v != 0], M, t, d0, float(v.sum()))
+    assert C.common_tm_masked(p.pred, p.native, v, M, t, d0) == pytest.approx(full, abs=1e-14)
+    assert C.common_tm_masked(p.pred, p.native, np.zeros_like(v), M, t, d0) == 0.0
+
+
+@needs_ref
+def test_comparison_on_padded_pdb_pairs(oracle, tmp_path):
+    """Family pairs with residues missing on either side: the search's own
+    score is the masked common score (same d0 of the shared count)."""
+    from indialign_b200 import pdb
+    rng = np.random.default_rng(12)
+    x = C.random_walk_trace(70, rng)
+    keep = np.ones(70, bool)
+    keep[[2, 3, 40]] = False
+    texts = [pdb.c1_pdb_text(x), pdb.c1_pdb_text(x @ W.random_rotation(rng).T + rng.normal(0, 2, x.shape), keep),
+             pdb.c1_pdb_text(x[10:] + rng.normal(0, 3, (60, 3)), first_resnum=11)]
+    pairs = pdb.family_pairs(texts)
+    assert len(pairs) == 2
+
+    def search(ps):
+        rc, s, R, t = abi.run_batch(oracle, ps, prefix="ora_")
+        assert rc == 0
+        return s, R, t
+
+    rep = C.compare(pairs, _fake_usalign(tmp_path), search=search)
+    np.testing.assert_allclose(rep.self_ours, rep.common_ours, atol=1e-12)
+
+
+def test_pdb_pairs_from_files(tmp_path):
+    from indialign_b200 import pdb
+    rng = np.random.default_rng(13)
+    x = C.random_walk_trace(40, rng)
+    ens = tmp_path / "ens.pdb"
+    ens.write_text("".join(f"MODEL     {k + 1:>4d}\n" + pdb.c1_pdb_text(x + rng.normal(0, 1 + 2 * k, x.shape))
+                           .replace("END\n", "") + "ENDMDL\n" for k in range(3)) + "END\n")
+    fam = [tmp_path / f"f{k}.pdb" for k in range(3)]
+    for k, f in enumerate(fam):
+        f.write_text(pdb.c1_pdb_text(x + rng.normal(0, 1, x.shape)))
+    pairs = C.pdb_pairs([str(ens)], [str(f) for f in fam])
+    assert len(pairs) == 3 and all(p.valid.sum() == 40 for p in pairs)

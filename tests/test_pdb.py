@@ -67,6 +67,45 @@ def test_most_divergent_pair():
     assert pdb.most_divergent_pair([base]) == (0, 1, -1.0)
 
 
+def _ensemble_text(models, chain="A"):
+    body = ""
+    for k, m in enumerate(models):
+        body += f"MODEL     {k + 1:>4d}\n" + pdb.c1_pdb_text(m, chain=chain).replace("END\n", "") + "ENDMDL\n"
+    return body + "END\n"
+
+
+def test_ensemble_pair_picks_the_most_divergent_models():
+    base = _trace(40, 6)
+    rng = np.random.default_rng(1)
+    models = [base + rng.normal(0, 0.3, base.shape) for _ in range(5)]
+    models[2] = base + rng.normal(0, 4.0, base.shape)
+    pair, (i, j, r) = pdb.ensemble_pair(_ensemble_text(models))
+    assert 2 in (i, j) and r > 3.0
+    np.testing.assert_allclose(pair.pred, models[i], atol=5e-4)
+    np.testing.assert_allclose(pair.native, models[j], atol=5e-4)
+    assert pair.lnorm == 40.0 and pair.valid.all()
+    assert pdb.ensemble_pair(_ensemble_text(models[:1])) is None           # one model
+    assert pdb.ensemble_pair(_ensemble_text([base, base[:30]])) is None    # unequal lengths
+    assert pdb.ensemble_pair(_ensemble_text([base[:20], base[:20]])) is None  # too short
+
+
+def test_family_pairs_by_residue_number():
+    base = _trace(60, 7)
+    native = pdb.c1_pdb_text(base, chain="A") + pdb.c1_pdb_text(base[:10], chain="B")
+    keep = np.ones(60, bool)
+    keep[:5] = False
+    pred1 = pdb.c1_pdb_text(base + 0.5, keep, chain="C")
+    pred2 = pdb.c1_pdb_text(base[40:], chain="A", first_resnum=41)   # 20 residues: too short a chain
+    pred3 = pdb.c1_pdb_text(base[:45], chain="D", first_resnum=30)   # 30..74: 31 shared with the native
+    assert pdb.longest_chain(native)[0] == "A" and pdb.longest_chain(pred2) is None
+    pairs = pdb.family_pairs([native, pred1, pred2, pred3], min_shared=20)
+    assert len(pairs) == 2
+    p1, p3 = pairs
+    assert int(p1.valid.sum()) == 55 and p1.lnorm == 55.0 and len(p1.valid) == 60
+    assert int(p3.valid.sum()) == 31 and len(p3.valid) == 74
+    assert pdb.family_pairs([native, pred3], min_shared=40) == []
+
+
 def test_pair_by_resnum_marks_each_side():
     a = {1: np.zeros(3), 2: np.ones(3), 5: np.full(3, 2.0)}
     b = {2: np.ones(3), 3: np.zeros(3), 5: np.zeros(3)}
