@@ -12,7 +12,8 @@
 //
 // Precision: the residue visits -- transform, distance, inlier test, raw
 // moment sums and the item's TM sum -- run in FP32 (the point set is staged
-// as FP64 and converted in shared memory; the TM sum is compensated); each
+// as FP64, centred on its FP64 mean and converted to FP32 in shared memory;
+// the TM sum is compensated); each
 // Kabsch eigen-solve runs in FP64 from the FP32 moments, and reduce_bank
 // rescores the task's winning item in FP64, so every reported score is an
 // FP64 TM-score of the returned (R, t).  The oracle rebuilt with this
