@@ -26,13 +26,19 @@ batches).
            visit; seed bank: FP32 (indialign_fp32_peak), 55 per residue
            visit.
   cpu_baseline  the reference's own build (oracle/_ref, OpenMP batch entry)
-           on this host's cores over a stratified sample of the timed pairs,
-           bounded to ~25 s.
+           on this host's cores: one batch call over a length-stratified
+           sample of the timed pairs, two pairs per host thread.
+
+stdout carries one short JSON line (key figures); the full record (ranker
+statistics per candidate kind, stage and kernel times, work counters) goes
+to stderr and, with --detail-out, to a file.
 
 Multi-GPU (torchrun): pairs are independent, so each rank searches its own
 batches of the same shape (weak scaling, no data-path collective); value =
 all ranks' pairs / max rank time.  --impl reference: the reference build on
-the host cores, rank 0 only.
+the host cores, rank 0 only: per step one batch call over a stratified
+sample of that step's batch, two pairs per host thread and at least 256
+timed pairs in all.
 """
 from __future__ import annotations
 
@@ -61,13 +67,16 @@ STAGES = ["seeds", "seed_bank", "ss", "gapless", "local_fragment", "threading_dp
 
 
 def workload(name: str, step_pairs: int, n_steps: int, rank: int = 0):
-    """The pairs of n_steps consecutive batches of `name` for this rank."""
+    """The pairs of n_steps consecutive batches of `name` for this rank; the
+    batches cycle through the workload's pairs (every rank has its own
+    workload of the same shape)."""
     if name == "learned16384":
         total = 16384
-        n = min(total, step_pairs * n_steps) if rank == 0 else step_pairs * n_steps
+        n = min(total, step_pairs * n_steps)
         pairs = W.parallel_batch(n, 40, 1000, seed=4 + 1000 * rank)
         desc = ("learned16384: 16384 pairs, L~U(40,1000), sigma~U(0.5,14) A, random rigid transform, "
-                "5% invalid per mask, lnorm=L")
+                f"5% invalid per mask, lnorm=L; a step is one {step_pairs}-pair search call, the steps "
+                "cycle through the workload's consecutive batches")
     elif name == "batch4096":
         pairs = W.parallel_batch(min(4096, step_pairs * n_steps), 40, 300, seed=1 + 1000 * rank)
         desc = "batch4096: 4096 pairs, L~U(40,300), sigma~U(0.5,14), 5% invalid per mask"
@@ -135,29 +144,40 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_baseline(pairs, n_sample=32, budget_s=25.0, seed=7):
-    """The reference build on this host's cores over a stratified sample of
-    `pairs`, in chunks of one pair per core until `budget_s` is spent."""
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def ref_pairs_per_call(cores: int) -> int:
+    """The reference batch entry parallelises over pairs only (one pair per
+    OpenMP thread, inner loops serial), so a call needs at least two pairs
+    per host thread to keep every core busy until its end."""
+    return 2 * cores
+
+
+def cpu_baseline(pairs, n_sample=0, seed=7):
+    """The reference build on this host's cores: one batch call over a
+    length-stratified sample of `pairs` with two pairs per host thread."""
     if not os.path.exists(REF_SO):
         return None
-    sample = W.subsample(pairs, n_sample, seed=seed)
     cores = os.cpu_count() or 1
+    sample = W.subsample(pairs, n_sample or ref_pairs_per_call(cores), seed=seed)
     os.environ["OMP_NUM_THREADS"] = str(cores)
     ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
-    rng = np.random.default_rng(seed)
-    order = list(rng.permutation(len(sample)))
-    done, scores, dt = [], [], 0.0
-    while order and dt < budget_s:
-        chunk = [sample[i] for i in order[:cores]]
-        order = order[cores:]
-        t0 = time.perf_counter()
-        _, s, _, _ = abi.run_batch(ref, chunk)
-        dt += time.perf_counter() - t0
-        done.extend(chunk)
-        scores.extend(list(s))
+    t0 = time.perf_counter()
+    _, s, _, _ = abi.run_batch(ref, sample)
+    dt = time.perf_counter() - t0
+    done, scores = sample, list(s)
     out = {"value": len(done) / dt, "unit": "pairs/s", "cores": cores, "kind": "reference",
-           "sample": f"{len(done)} pairs of a {len(sample)}-pair length-stratified sample of the timed "
-                     f"batches (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}
+           "cpu": cpu_model(),
+           "sample": f"one batch call over a {len(sample)}-pair length-stratified sample of the timed "
+                     f"pairs (seed {seed}), reference build, OpenMP batch entry, {dt:.1f} s"}
     single = single_thread_rate(done, ref)
     if single:
         out["single_thread"] = single
@@ -230,12 +250,14 @@ def run_reference_arm(args):
     batches, desc = workload(args.workload, args.step_pairs, args.warmup + args.steps)
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
+    # two pairs per host thread per call, and at least 256 timed pairs in all
+    per_step = args.ref_pairs or max(ref_pairs_per_call(cores), -(-256 // max(args.steps, 1)))
     ref = abi.bind_reference_abi(ctypes.CDLL(REF_SO))
     for k in range(args.warmup):
         abi.run_batch(ref, sorted(batches[k], key=lambda p: p.pred.shape[0])[:1])  # shortest pair
     times, n_done = [], 0
     for k in range(args.steps):
-        sample = W.subsample(batches[args.warmup + k], args.ref_pairs, seed=100 + k)
+        sample = W.subsample(batches[args.warmup + k], per_step, seed=100 + k)
         t0 = time.perf_counter()
         abi.run_batch(ref, sample)
         times.append(time.perf_counter() - t0)
@@ -246,10 +268,12 @@ def run_reference_arm(args):
             "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": desc,
-                       "step": f"{args.ref_pairs}-pair stratified sample of one {args.step_pairs}-pair batch",
-                       "host_threads": cores},
+                       "step": (f"one reference batch call over a {per_step}-pair length-stratified sample "
+                                f"of one {args.step_pairs}-pair batch"),
+                       "host_threads": cores, "cpu": cpu_model()},
             "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": cores, "kind": "reference",
-                             "sample": f"{args.ref_pairs} pairs per step x {args.steps} steps"},
+                             "cpu": cpu_model(),
+                             "sample": f"{per_step} pairs per step x {args.steps} steps = {n_done} pairs"},
             "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -304,8 +328,11 @@ def main():
     ap.add_argument("--audit", type=float, default=0.02)
     ap.add_argument("--rank-mask", type=int, default=0, help="INDIALIGN_RANK_* bits (0: library default)")
     ap.add_argument("--weights", default=None, help="ranker blob (.npy; default the shipped weights)")
-    ap.add_argument("--ref-pairs", type=int, default=8)
-    ap.add_argument("--cpu-sample", type=int, default=32)
+    ap.add_argument("--ref-pairs", type=int, default=0,
+                    help="pairs per reference-arm step (0: two per host thread, >= 256 timed in all)")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="pairs of the cpu_baseline call (0: two per host thread)")
+    ap.add_argument("--detail-out", default=None, help="also write the full record (JSON) here")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -510,9 +537,47 @@ def main():
                 "gpu_launches": launches, "gpu_launches_per_step": launches / args.steps, "clocks": clocks,
                 "stage_ms": dict(zip(STAGES, [round(float(x), 2) for x in np.mean(lrn["stg"], 0)])),
                 "mean_tm": float(l_scores.mean())}
-        print(json.dumps(line))
+        # the full record goes to stderr (and --detail-out); stdout gets one
+        # short line whose every key survives a few-KB tail of the output
+        print(json.dumps(line), file=sys.stderr)
+        if args.detail_out:
+            with open(args.detail_out, "w") as f:
+                json.dump(line, f, indent=1)
+        print(json.dumps(compact_line(line)))
     if dist:
         dist.destroy_process_group()
+
+
+def compact_line(line: dict) -> dict:
+    """The bench line without the per-kind ranker statistics, stage and
+    kernel breakdowns (those stay in the full record): key figures first."""
+    keep = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+            "scaling", "vs_baseline", "dtype", "data"]
+    out = {k: line[k] for k in keep}
+    pl = line.get("plain")
+    if pl:
+        out["plain"] = {k: pl[k] for k in ("value", "unit", "ms_per_step", "learned_over_plain", "delta_tm")}
+    if line.get("rank"):
+        r = line["rank"]
+        lists = sum(v["pairs"] for v in r.values())
+        out["rank"] = {"lists": lists,
+                       "fallback_rate": sum(v["fallback_rate"] * v["pairs"] for v in r.values()) / max(lists, 1),
+                       "audit_misses": sum(v["audit_misses"] for v in r.values())}
+    rf = line.get("roofline")
+    if rf:
+        out["roofline"] = {k: rf[k] for k in ("kernel", "bound", "achieved", "peak", "unit", "frac", "traffic",
+                                              "peak_source", "kernel_share") if k in rf}
+    cpu = line.get("cpu_baseline")
+    if cpu:
+        out["cpu_baseline"] = {k: v for k, v in cpu.items() if k != "single_thread"}
+        st = cpu.get("single_thread")
+        if st:
+            out["cpu_baseline"]["single_thread"] = {"value": st.get("value"), "cores": 1}
+    for k in ("e2e", "gpu_launches", "mean_tm", "config"):
+        out[k] = line.get(k)
+    c = line.get("clocks")
+    out["clocks"] = {k: c[k] for k in ("sm_mhz", "sm_max_mhz", "reasons")} if c else None
+    return out
 
 
 class _Null:

@@ -231,9 +231,9 @@ int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_
                        int *d_na, void *stream);
 
 /* indialign_nw_align without any device allocation (no counterpart in the
- * reference).  For callers that cannot call cudaMalloc when they align: code
- * running under another component's CUDA graph capture, or hosts whose device
- * memory belongs to a framework's pool.  Same arguments, kernel and outputs
+ * reference).  For callers that cannot call cudaMalloc when they align: hosts
+ * whose device memory belongs to a framework's pool allocator, or paths that
+ * forbid driver allocations.  Same arguments, kernel and outputs
  * as indialign_nw_align; the caller passes device inputs and outputs, the
  * scratch lives in a fixed device array of about 1.1 MB that every GPU using
  * the library keeps until exit.  Limit: 1 <= np, nn <= 2048, else
@@ -243,6 +243,35 @@ int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_
  * legacy default stream; the call returns after the stream synchronizes. */
 int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap, int *d_ap,
                                int *d_an, int *d_na, void *stream);
+
+/* ---- one batch over several GPUs of this process (no counterpart in the
+ * reference, which parallelises over pairs with OpenMP only,
+ * indialign_c/indialign.cpp:305-313).  Pairs are independent, so the split
+ * needs no collective. */
+
+/* Estimated device work of every pair (NW-cell units): the always-run passes
+ * and the seed bank, plus the rescue passes' NW cells (windows and offsets
+ * from rescue.h:12-46, 136-142) weighted by how likely they run, judged from
+ * the pair's TM-score under one Kabsch superposition of all valid residues
+ * (written to tm0[n] when tm0 is not NULL).  Host only, no device work. */
+int indialign_pair_costs(int n_pairs, const NativePairInput *inputs, double *cost, double *tm0);
+
+/* shard_of[p] in 0..n_shards-1: longest-processing-time split of the batch
+ * by indialign_pair_costs (costliest pair first onto the least-loaded shard;
+ * ties to the lower index).  Deterministic, so every rank of a multi-process
+ * job computes the same split.  Host only. */
+int indialign_shard_pairs(int n_pairs, const NativePairInput *inputs, int n_shards, int *shard_of);
+
+/* indialign_tmscore_search_batch_ex over devices[0..n_devices-1] (a device
+ * may be listed more than once): indialign_shard_pairs split, one host thread
+ * and library context per shard, results in batch order.  opts may carry the
+ * search mode and the aggregate outputs (stage_ms: the slowest shard's;
+ * counters, kernel_ms, rank_stats: summed); a caller stream and the
+ * per-pair outputs (stage_best, win_*) are per-device and rejected with
+ * INDIALIGN_E_INPUT.  The first failing shard's code is returned. */
+int indialign_tmscore_search_multi(int n_pairs, const NativePairInput *inputs, const NativeConfig *cfg,
+                                   const IndialignBatchOptions *opts, const int *devices, int n_devices,
+                                   NativePairResult *outputs);
 
 /* Candidates of kind INDIALIGN_CAND_* of a pair with plen / nlen valid pred /
  * native residues (the schedules of rescue.h:12-46 and :136-142; for

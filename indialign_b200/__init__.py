@@ -109,6 +109,17 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.indialign_fp32_peak.restype = ctypes.c_int
     lib.indialign_candidate_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.indialign_candidate_count.restype = ctypes.c_int
+    lib.indialign_pair_costs.argtypes = [ctypes.c_int, ctypes.POINTER(NativePairInput),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.indialign_pair_costs.restype = ctypes.c_int
+    lib.indialign_shard_pairs.argtypes = [ctypes.c_int, ctypes.POINTER(NativePairInput), ctypes.c_int,
+                                          ctypes.POINTER(ctypes.c_int)]
+    lib.indialign_shard_pairs.restype = ctypes.c_int
+    lib.indialign_tmscore_search_multi.argtypes = [
+        ctypes.c_int, ctypes.POINTER(NativePairInput), ctypes.POINTER(NativeConfig),
+        ctypes.POINTER(BatchOptions), ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+        ctypes.POINTER(NativePairResult)]
+    lib.indialign_tmscore_search_multi.restype = ctypes.c_int
     vp, sz = ctypes.c_void_p, ctypes.c_size_t
     for name, args, res in (
             ("indialign_mlp_packed_bytes", [], sz),
@@ -310,64 +321,56 @@ def search_tensors(pred, native, valid=None, pred_valid=None, native_valid=None,
     return out[:, 0], out[:, 1:10], out[:, 10:13]
 
 
+def pair_costs(pairs: Sequence) -> tuple[np.ndarray, np.ndarray]:
+    """(cost, tm0) per pair from the library's work estimate
+    (indialign_pair_costs): NW-cell units, the rescue passes weighted by
+    their likelihood judged from tm0, the TM-score under one Kabsch of all
+    valid residues.  Host only."""
+    lib = load()
+    pk = abi.PackedInputs(list(pairs))
+    cost = np.zeros(pk.n)
+    tm0 = np.zeros(pk.n)
+    rc = lib.indialign_pair_costs(pk.n, pk.arr, cost.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                  tm0.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if rc != 0:
+        raise IndialignError(f"indialign_pair_costs rc={rc}")
+    return cost, tm0
+
+
 def shard_pairs(pairs: Sequence, n_shards: int) -> list[list[int]]:
-    """Length-balanced split of a batch over n_shards devices: pairs sorted by
-    an L^3 work estimate (the rescue passes' NW work grows as windows x L^2),
-    each placed on the least-loaded shard (longest-processing-time greedy).
+    """Work-balanced split of a batch over n_shards devices or ranks
+    (indialign_shard_pairs: longest-processing-time greedy over
+    pair_costs()).  Deterministic, so every rank computes the same split.
     Returns the pair indices of every shard, ascending."""
     n_shards = max(1, int(n_shards))
-    cost = [float(p.pred.shape[0]) ** 3 for p in pairs]
-    order = sorted(range(len(pairs)), key=lambda i: (-cost[i], i))
-    load = [0.0] * n_shards
-    out: list[list[int]] = [[] for _ in range(n_shards)]
-    for i in order:
-        k = min(range(n_shards), key=lambda j: (load[j], j))
-        out[k].append(i)
-        load[k] += cost[i]
-    return [sorted(o) for o in out]
+    lib = load()
+    pk = abi.PackedInputs(list(pairs))
+    shard = np.zeros(max(pk.n, 1), np.int32)
+    rc = lib.indialign_shard_pairs(pk.n, pk.arr, n_shards, shard.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != 0:
+        raise IndialignError(f"indialign_shard_pairs rc={rc}")
+    return [[i for i in range(pk.n) if shard[i] == k] for k in range(n_shards)]
 
 
 def search_multi(pairs: Sequence, devices: Sequence[int], cfg: NativeConfig | None = None,
-                 ranker: np.ndarray | None = None, **learned):
-    """Search a batch over several GPUs of this process: shard_pairs() split,
-    one host thread per device (each call has its own device context and
-    stream), results gathered in the batch's order.  No collective: pairs
+                 ranker: np.ndarray | None = None, rank_stats: np.ndarray | None = None, **learned):
+    """Search a batch over several GPUs of this process through
+    indialign_tmscore_search_multi: shard_pairs() split, one host thread and
+    context per device, results in the batch's order.  No collective: pairs
     are independent."""
-    import threading
     lib = load()
     cfg = cfg or default_config()
-    shards = shard_pairs(pairs, len(devices))
-    n = len(pairs)
-    score = np.zeros(n)
-    R = np.zeros((n, 9))
-    t = np.zeros((n, 3))
-    errors: list[str] = []
-
-    def work(dev: int, idx: list[int]):
-        if not idx:
-            return
-        sub = [pairs[i] for i in idx]
-        pk = abi.PackedInputs(sub)
-        res = (NativePairResult * pk.n)()
-        opts = BatchOptions()
-        opts.device = int(dev)
-        if ranker is not None:
-            learned_options(opts, ranker, **learned)
-        rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
-        if rc != 0:
-            errors.append(f"device {dev}: rc={rc} {last_error()}")
-            return
-        s_, R_, t_ = abi.results_to_numpy(res, pk.n)
-        score[idx], R[idx], t[idx] = s_, R_, t_
-
-    threads = [threading.Thread(target=work, args=(d, ix)) for d, ix in zip(devices, shards)]
-    for th in threads:
-        th.start()
-    for th in threads:
-        th.join()
-    if errors:
-        raise IndialignError("; ".join(errors))
-    return score, R, t
+    pk = abi.PackedInputs(list(pairs))
+    res = (NativePairResult * max(pk.n, 1))()
+    opts = BatchOptions()
+    if ranker is not None:
+        learned_options(opts, ranker, rank_stats=rank_stats, **learned)
+    devs = np.ascontiguousarray(devices, np.int32)
+    rc = lib.indialign_tmscore_search_multi(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts),
+                                            devs.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(devs), res)
+    if rc != 0:
+        raise IndialignError(f"indialign_tmscore_search_multi rc={rc}: {last_error()}")
+    return abi.results_to_numpy(res, pk.n)
 
 
 def fp64_peak_tflops(device: int = 0) -> float:

@@ -85,27 +85,46 @@ IA_DEV float coord(const float *f, const double *d, const double *off, int k) {
     else return (float)(d[k] - off[k % 3]);
 }
 
-// CTA-wide FP64 mean of n points into out[3] (shared); red holds 3 doubles
-// per warp.  The summation order depends only on n, so both kernel paths
-// get the same mean.
+// CTA-wide FP64 mean of the finite values of n points, per axis, into
+// out[3] (shared); red holds 6 doubles per warp.  The summation order
+// depends only on n, so both kernel paths get the same mean.  Non-finite
+// coordinates are left out: the mean is only the frame the FP32 work runs
+// in, and one Inf must not turn every centred point into NaN (the
+// reference's FP64 seeds that avoid such a residue still score finitely).
+// With all values finite this is the plain mean.
 IA_DEV void points_mean(const double *src, int n, double *out, double *red) {
-    double a[3] = {0.0, 0.0, 0.0};
+    double a[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
     for (int i = threadIdx.x; i < n; i += kBankChunk) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) a[d] += src[3 * i + d];
+        for (int d = 0; d < 3; d++) {
+            const double x = src[3 * i + d];
+            if (isfinite(x)) {
+                a[d] += x;
+                c[d] += 1.0;
+            }
+        }
     }
 #pragma unroll
-    for (int d = 0; d < 3; d++) a[d] = warp_sum(a[d]);
+    for (int d = 0; d < 3; d++) {
+        a[d] = warp_sum(a[d]);
+        c[d] = warp_sum(c[d]);
+    }
     const int w = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int d = 0; d < 3; d++) red[3 * w + d] = a[d];
+        for (int d = 0; d < 3; d++) {
+            red[6 * w + d] = a[d];
+            red[6 * w + 3 + d] = c[d];
+        }
     }
     __syncthreads();
     if (threadIdx.x < 3) {
-        double v = 0.0;
-        for (int k = 0; k < kBankChunk / 32; k++) v += red[3 * k + threadIdx.x];
-        out[threadIdx.x] = n > 0 ? v / n : 0.0;
+        double v = 0.0, m = 0.0;
+        for (int k = 0; k < kBankChunk / 32; k++) {
+            v += red[6 * k + threadIdx.x];
+            m += red[6 * k + 3 + threadIdx.x];
+        }
+        out[threadIdx.x] = m > 0.0 ? v / m : 0.0;
     }
     __syncthreads();
 }
@@ -141,7 +160,7 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
     extern __shared__ __align__(16) char smem[];
     __shared__ BankSmem ctl;
     __shared__ uint64_t bar;
-    __shared__ double oP[3], oQ[3], red[3 * (kBankChunk / 32)];  // point-set means
+    __shared__ double oP[3], oQ[3], red[6 * (kBankChunk / 32)];  // point-set means
     // layout: P[nmax*3] Q[nmax*3] (each +16 B lead room), V, PV, NV bytes
     // room for a 15-byte lead and the rounded-up tail of a bulk copy
     const uint32_t coord_bytes = ((uint32_t)nmax * 24u + 47u) & ~15u;

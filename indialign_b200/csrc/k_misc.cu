@@ -203,7 +203,13 @@ IA_DEV uint64_t fnv_bits(const uint32_t *bits, int N, const uint64_t *pw) {
 // equal counts keep the order its introsort leaves them in.  This is the same
 // sequence of element moves (libstdc++ introsort: median-of-three to the
 // front, unguarded partition, depth 2*floor(log2 n) then heapsort, runs <= 16
-// finished by insertion sort), so ties resolve identically.
+// finished by insertion sort), so ties resolve identically.  The move
+// sequence follows GCC's libstdc++ (bits/stl_algo.h: __introsort_loop,
+// __unguarded_partition_pivot, __final_insertion_sort; bits/stl_heap.h:
+// __adjust_heap, __push_heap), which is licensed under GPLv3 with the GCC
+// Runtime Library Exception; it is restated here only so that tie order
+// matches the reference build's std::sort, and is pinned against that build
+// by a golden fixture of sort orders.
 struct KV { int key, idx; };
 #define KVL(x, y) ((x).key > (y).key)
 IA_DEV void kv_swap(KV *a, KV *b) { KV t = *a; *a = *b; *b = t; }

@@ -1,12 +1,12 @@
 // Allocation-free NW alignment entry point.
 //
 // Some callers cannot call cudaMalloc at the moment they need an alignment:
-// code running while another component captures a CUDA graph (cudaMalloc is
-// illegal during capture), hosts whose device memory is owned entirely by a
-// framework's pool allocator, or latency-critical paths that forbid driver
-// allocations.  indialign_nw_align allocates its trace scratch on first use;
-// this variant runs the same kernel (k_nw_explicit) with its scratch in a
-// fixed file-scope device array instead, so it allocates nothing.
+// hosts whose device memory is handed out entirely by a framework's pool
+// allocator (a cudaMalloc beside the pool fails or fragments it), or
+// latency-critical paths that forbid driver allocations.  indialign_nw_align
+// allocates its trace scratch on first use; this variant runs the same kernel
+// (k_nw_explicit) with its scratch in a fixed file-scope device array
+// instead, so it allocates nothing.
 //
 // The array holds the NW trace, the stripe boundary row, the reversed
 // alignment and the kernel's work counters for one problem of at most
@@ -14,7 +14,10 @@
 // this library until the process exits).  All calls share it: two calls whose
 // kernels overlap on the GPU race on it.  The kernel zeroes the boundary row
 // itself and writes every trace word it later reads, so no state carries over
-// from the previous call; the counters are never read.
+// from the previous call; the counters are never read.  The first call on a
+// device looks up the array's device address (cudaGetSymbolAddress) with
+// that device current; make that first call before any stream capture.  The
+// call returns after `stream` synchronizes.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -18,11 +18,14 @@ from .workloads import Pair
 
 
 def _atom_c1(line: str):
-    """(chain, resnum, xyz) of a C1' ATOM record, else None."""
+    """(chain, xyz) of a C1' ATOM record, else None.  The residue number is
+    not parsed here: the model and chain extractors of the reference
+    benchmark never read it, so a blank or non-numeric resSeq (hybrid-36)
+    must not stop them."""
     if not line.startswith("ATOM") or line[12:16].strip() != "C1'":
         return None
     xyz = (float(line[30:38]), float(line[38:46]), float(line[46:54]))
-    return line[21], int(line[22:26]), np.array(xyz, np.float64)
+    return line[21], np.array(xyz, np.float64)
 
 
 def c1_models(text: str) -> list[np.ndarray]:
@@ -42,7 +45,7 @@ def c1_models(text: str) -> list[np.ndarray]:
         else:
             a = _atom_c1(line)
             if a is not None:
-                cur.append(a[2])
+                cur.append(a[1])
     if not models and cur:
         models.append(np.array(cur))
     return models
@@ -57,7 +60,7 @@ def c1_chains(text: str) -> dict[str, np.ndarray]:
             break
         a = _atom_c1(line)
         if a is not None:
-            chains.setdefault(a[0], []).append(a[2])
+            chains.setdefault(a[0], []).append(a[1])
     return {ch: np.array(v) for ch, v in chains.items()}
 
 
@@ -71,7 +74,7 @@ def c1_by_chain(text: str) -> dict[str, dict[int, np.ndarray]]:
             break
         a = _atom_c1(line)
         if a is not None:
-            chains.setdefault(a[0], {})[a[1]] = a[2]
+            chains.setdefault(a[0], {})[int(line[22:26])] = a[1]
     return chains
 
 

@@ -66,6 +66,12 @@ class GoldenPairs:
                 z["v"][a:b], z["pv"][a:b], z["nv"][a:b], float(z["lnorm"][k]),
                 float(z["sigma"][k])))
         self.score, self.R, self.t, self.trace = z["score"], z["R"], z["t"], z["trace"]
+        self.hard = z["hard"] if "hard" in z else np.zeros(len(self.pairs), bool)
+
+    def shortest(self, k):
+        """Indices of the k shortest pairs (for checks that must stay fast on
+        the CPU)."""
+        return sorted(range(len(self.pairs)), key=lambda i: self.pairs[i].pred.shape[0])[:k]
 
 
 GOLDEN_SETS = ["single", "batch", "hard", "edge"]

@@ -2,13 +2,23 @@
 
 Runs here, where the reference sources exist:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py          # small sets
+    python tests/golden/make_golden.py shapes                       # cfg1 / cfg2
 
 oracle/_ref/libindialign_ref.so is the reference's `make cpu` build compiled
 from its sources (oracle/Makefile); ref_trace_search (oracle/ref_stages.cpp)
 replays its stage order through the reference's own stage functions to record
 the running best after every stage.  Outputs are small .npz files: the packed
 inputs of each case group and the reference's results.
+
+`shapes` writes the stratified samples of the two batch workloads the search
+is quoted on (golden_cfg1.npz: 48 pairs of the 4096-pair shape, L 40-300,
+5 % invalid per mask; golden_cfg2.npz: 18 pairs of the uneven hard shape,
+L 30-1500, 10 of them hard, spread over every rescue stride branch of
+rescue.h:30-46).  Every pair runs in its own single-threaded process
+(OMP_NUM_THREADS=1, so the reference's inner loops take their serial,
+deterministic path, as inside its batch entry); the longest hard pairs take
+tens of minutes each.
 """
 from __future__ import annotations
 
@@ -92,6 +102,64 @@ def edge_pairs():
     return out
 
 
+# (L, hard) of the uneven-shape sample: hard pairs whose valid counts fall in
+# every stride bracket of local_jump (rescue.h:30-46: <=150, <=200, <=250,
+# <=300, <=350, >350 residues) up to 1500, easy pairs spread log-uniformly
+CFG2_SHAPES = [(60, True), (140, True), (190, True), (240, True), (290, True), (340, True),
+               (420, True), (750, True), (1100, True), (1480, True),
+               (30, False), (55, False), (120, False), (210, False), (330, False), (560, False),
+               (900, False), (1350, False)]
+
+
+def cfg1_pairs():
+    """48 pairs stratified by length from 480 pairs of the 4096-pair shape."""
+    return W.subsample(W.batch(480, 40, 300, seed=111), 48, seed=3)
+
+
+def cfg2_pairs():
+    rng = np.random.default_rng(222)
+    out = []
+    for L, hard in CFG2_SHAPES:
+        sigma = float(rng.uniform(4, 14)) if hard else float(rng.uniform(0.5, 14))
+        out.append(W.make_pair(L, sigma, rng, 0.05, hard=hard))
+    return out
+
+
+def _serial_init():
+    os.environ["OMP_NUM_THREADS"] = "1"
+
+
+def _ref_one(arg):
+    """Reference batch entry and stage replay of one pair, single-threaded."""
+    k, pair = arg
+    s, R, t, trace = run_ref([pair])
+    return k, s[0], R[0], t[0], trace[0]
+
+
+def run_ref_serial(pairs, procs=8):
+    """run_ref over `pairs`, one single-threaded process per pair, longest first."""
+    import multiprocessing as mp
+    order = sorted(range(len(pairs)), key=lambda i: -pairs[i].pred.shape[0])
+    s = np.zeros(len(pairs))
+    R = np.zeros((len(pairs), 9))
+    t = np.zeros((len(pairs), 3))
+    trace = np.zeros((len(pairs), N_STAGES, 13))
+    with mp.get_context("spawn").Pool(procs, initializer=_serial_init) as pool:
+        for k, sk, Rk, tk, trk in pool.imap_unordered(_ref_one, [(i, pairs[i]) for i in order]):
+            s[k], R[k], t[k], trace[k] = sk, Rk, tk, trk
+            print(f"  pair {k} L={pairs[k].pred.shape[0]} score={sk:.6f}", flush=True)
+    return s, R, t, trace
+
+
+def main_shapes():
+    for name, pairs in (("cfg1", cfg1_pairs()), ("cfg2", cfg2_pairs())):
+        s, R, t, trace = run_ref_serial(pairs)
+        np.savez_compressed(os.path.join(OUT, f"golden_{name}.npz"), score=s, R=R, t=t, trace=trace,
+                            sigma=np.array([p.sigma for p in pairs]),
+                            hard=np.array([p.hard for p in pairs]), **pack(pairs))
+        print(name, len(pairs), np.round(s, 4), flush=True)
+
+
 def main():
     groups = {
         "single": W.single(0),
@@ -162,4 +230,7 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["shapes"]:
+        main_shapes()
+    else:
+        main()

@@ -89,3 +89,44 @@ def test_single_thread_reference_rate():
     r = bench.single_thread_rate(pairs, ref, budget_s=0.5)
     assert r["cores"] == 1 and r["unit"] == "pairs/s" and r["value"] > 0
     assert r["same_pairs_all_cores"] > 0 and "shortest" in r["sample"]
+
+
+def test_compact_line_keeps_the_verdict_fields_in_a_short_line():
+    """stdout's line keeps the learned-vs-plain ratio and the per-pair TM
+    change, the roofline, the CPU baseline, e2e and clocks, and stays well
+    under a few-KB output tail even with the full record's breakdowns."""
+    kinds = {nm: {"pairs": 1000 + k, "fallback_rate": 0.1, "audit_rate": 0.02, "pruned_rate": 0.8,
+                  "refined_fraction": 0.2, "audit_misses": 7} for k, nm in enumerate("abcde")}
+    full = {"metric": bench.METRIC, "value": 1786.0, "unit": "pairs/s", "n_gpus": 1, "steps": 20, "warmup": 5,
+            "ms_per_step": 1146.6, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32", "data": "synthetic",
+            "config": {"workload": "learned16384: " + "x" * 200, "step_pairs": 2048},
+            "plain": {"value": 405.0, "unit": "pairs/s", "ms_per_step": 5059.0, "learned_over_plain": 4.41,
+                      "delta_tm": {"mean": 4e-8, "worst": -5e-7, "best": 1e-3, "pairs_below_-1e-4": 0,
+                                   "pairs_below_-1e-3": 0, "pairs": 40960},
+                      "stage_ms": {s: 1.0 for s in bench.STAGES}, "kernel_ms": {"k_chain": 1.0}},
+            "rank": kinds,
+            "roofline": {"kernel": "k_bank", "bound": "fp32", "achieved": 12.0, "peak": 67.7, "unit": "TFLOP/s",
+                         "frac": 0.18, "traffic": 1.0e9, "peak_source": "measured", "kernel_share": 0.55,
+                         "warp_cycle_split": {"nw_fill": 0.8}, "kernel_ms": {"k_bank": 1.0}},
+            "cpu_baseline": {"value": 0.9, "unit": "pairs/s", "cores": 16, "kind": "reference", "cpu": "Xeon",
+                             "sample": "s" * 150, "single_thread": {"value": 0.45, "sample": "t" * 100},
+                             "plain_parity_on_sample": {"min_dTM": -1e-8}},
+            "e2e": {"value": 1733.0, "unit": "pairs/s", "h2d_bytes_per_step": 54540422,
+                    "d2h_bytes_per_step": 212992},
+            "gpu_launches": 3140, "gpu_launches_per_step": 157.0,
+            "clocks": {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": [], "samples": 108},
+            "stage_ms": {s: 1.0 for s in bench.STAGES}, "mean_tm": 0.48}
+    c = bench.compact_line(full)
+    text = json.dumps(c)
+    assert len(text) < 2000
+    assert c["plain"]["delta_tm"]["worst"] == -5e-7 and c["plain"]["learned_over_plain"] == 4.41
+    assert c["roofline"]["frac"] == 0.18 and c["roofline"]["traffic"] == 1.0e9
+    assert c["cpu_baseline"]["cpu"] == "Xeon" and c["e2e"]["value"] == 1733.0
+    assert c["rank"]["lists"] == sum(v["pairs"] for v in kinds.values())
+    assert list(c)[:3] == ["metric", "value", "unit"]
+
+
+def test_reference_arm_fills_the_host():
+    """Two pairs per host thread per reference call."""
+    assert bench.ref_pairs_per_call(16) == 32

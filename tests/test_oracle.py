@@ -41,6 +41,26 @@ def test_oracle_stage_trace_matches_golden(oracle, golden):
         np.testing.assert_allclose(tr[ran, 0], ref[ran, 0], rtol=0, atol=1e-9)
 
 
+@pytest.mark.parametrize("name,k", [("cfg1", 10), ("cfg2", 4)])
+def test_oracle_matches_golden_workload_shapes(oracle, name, k):
+    """The oracle on the shortest pairs of the workload-shape samples (the
+    long ones are checked on the GPU against the same fixtures)."""
+    g = GoldenPairs(name)
+    idx = g.shortest(k)
+    rc, s, R, t = abi.run_batch(oracle, [g.pairs[i] for i in idx], prefix="ora_")
+    assert rc == 0
+    np.testing.assert_allclose(s, g.score[idx], rtol=0, atol=1e-9)
+
+
+def test_cfg2_sample_reaches_the_dense_rescue():
+    """The hard pairs of the uneven sample fall below 0.3 before the dense
+    local-fragment pass (so it runs) at every rescue stride bracket."""
+    g = GoldenPairs("cfg2")
+    # trace stage 5 = dense_local_fragment: recorded only when the pass ran
+    gated = [g.pairs[k].pred.shape[0] for k in range(len(g.pairs)) if g.hard[k] and g.trace[k, 5, 0] > -1e30]
+    assert len(gated) >= 6 and max(gated) >= 1000, gated
+
+
 def test_sort_tie_order_matches_std_sort(oracle):
     """The anchor candidates' tie order (count-only std::sort) is reproduced."""
     import os

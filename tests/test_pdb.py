@@ -51,6 +51,21 @@ def test_extraction_rules_follow_the_reference_benchmark():
     assert [m.shape for m in pdb.c1_models(a)] == [(6, 3)]  # no MODEL records: one model
 
 
+def test_model_and_chain_extraction_ignore_the_residue_number_field():
+    """A blank or non-numeric resSeq (hybrid-36 style) does not stop the model
+    and chain extractors, which, like the reference benchmark's, never read
+    the residue number."""
+    x = _trace(5, 7)
+    lines = pdb.c1_pdb_text(x, chain="A").splitlines()
+    odd = [l[:22] + ("    " if k % 2 else "A0B1") + l[26:] if l.startswith("ATOM") else l
+           for k, l in enumerate(lines)]
+    text = "\n".join(odd) + "\n"
+    models = pdb.c1_models(text)
+    assert [m.shape for m in models] == [(5, 3)]
+    np.testing.assert_allclose(models[0], x, atol=5e-4)
+    assert pdb.c1_chains(text)["A"].shape == (5, 3)
+
+
 def test_most_divergent_pair():
     rng = np.random.default_rng(4)
     base = _trace(20, 5)
