@@ -14,9 +14,13 @@
 // the sign bit of H (H >= 0 always; -0.0 encodes a diagonal zero).  Score
 // entries are computed on the fly from the transformed pred row held in
 // registers and the native column in shared memory, never stored.  Trace
-// directions (2 bits/cell) go to a per-warp global scratch block, which stays
-// L2-resident for the sizes of interest, and the traceback walks 32x16-cell
-// tiles held in registers (one coalesced load per tile, shuffles inside).
+// directions (2 bits/cell) go to a per-warp global scratch block in a
+// stripe-major layout: for every 16 steps the warp's 64 rows store one
+// contiguous 256-byte line (one 8-byte store per lane), so the stores are
+// full-sector writes; the traceback walks 32-row tiles held in registers
+// (coalesced loads, shuffles inside).
+#include <type_traits>
+
 #include "dmath.cuh"
 #include "stage.cuh"
 #include "pipeline.h"
@@ -46,6 +50,20 @@ IA_DEV void al_get(const uint32_t *al, int na, int k, int &pi, int &ni) {
     ni = (int)(e & 0xffffu);
 }
 
+// Value type of the NW fill of the search's score matrices (dp_refine and
+// the SS + distance NW): FP32 by default (1), FP64 like the reference (0).
+// Measured on the CPU (the oracle rebuilt with FP32 score entries, and with
+// FP32 entries and DP values, against the reference build on 240 pairs of
+// the 4096-pair shape and 96 hard pairs): every final TM-score within
+// 5.6e-16 of the reference's, for either choice.  The SS-identity
+// NW (entries 0/1, gap -1) runs in FP32, where its integer-valued DP is
+// exact; the explicit-matrix NW entry stays FP64 (bit-exact with the
+// reference's nw_dp on the same matrix).
+#ifndef IA_CHAIN_DP32
+#define IA_CHAIN_DP32 1
+#endif
+using ChainDP = std::conditional_t<IA_CHAIN_DP32 != 0, float, double>;
+
 struct NWParams {
     int plen, nlen;
     int smode;
@@ -54,58 +72,77 @@ struct NWParams {
     double cut2;      // SMAT_DP: score only if d2 <= cut2
     const uint8_t *Lp, *Ln;  // SS labels (compact order)
     const double *smat;      // SMAT_EXPLICIT: plen x nlen row-major
+    const float4 *Qf;        // native column as FP32 (shared memory), or null
 };
 
-// One score-matrix entry (indialign_c/align.h:86-98; ss.h:69-72, 118-131).
-// 1/(1 + d2/d0^2) uses the Newton reciprocal (<= 1 ulp); arguments past the
-// float range (d > ~1e19 d0) contribute nothing representable to H.
-template <int SMODE>
-IA_DEV double smat_entry(const NWParams &pr, double mx, double my, double mz, uint8_t lp,
-                         double qx, double qy, double qz, uint8_t ln) {
-    if (SMODE == SMAT_SS2) return (lp == ln) ? 1.0 : 0.0;
-    const double dx = mx - qx, dy = my - qy, dz = mz - qz;
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    const double r = rcp_nr(fmin(fma(d2, pr.inv_d0sq, 1.0), 1e30));
-    if (SMODE == SMAT_DP) return d2 <= pr.cut2 ? r : 0.0;
-    return (lp == ln) ? r + 0.5 : r;
+// One score-matrix entry (indialign_c/align.h:86-98; ss.h:69-72, 118-131)
+// in FP32: the moved pred point (FP64 transform, rounded to FP32) minus the
+// native point rounded to FP32, FP32 d2 and cutoff test, and the term
+// 1/(1 + d2 * (1/d0^2)) with a correctly rounded FP32 reciprocal; the SS
+// bonus 0.5 is added in the DP's type.  A NaN distance gives 0 in the DP
+// mode (the cutoff test fails) and NaN in the SS4 mode, an infinite one 0,
+// as in the reference's FP64 arithmetic.
+template <int SMODE, typename T>
+IA_DEV T smat_entry(float inv_d0sq, float cut2, float mx, float my, float mz, uint8_t lp, float qx,
+                    float qy, float qz, uint8_t ln) {
+    if (SMODE == SMAT_SS2) return (lp == ln) ? T(1) : T(0);
+    const float dx = mx - qx, dy = my - qy, dz = mz - qz;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    const float r = __frcp_rn(1.0f + d2 * inv_d0sq);
+    if (SMODE == SMAT_DP) return d2 <= cut2 ? T(r) : T(0);
+    return (lp == ln) ? T(r) + T(0.5) : T(r);
 }
 
 // One NW cell (indialign_c/nw.h:20-35).  With a gap penalty the "reached
-// diagonally" bit of a cell travels in the sign of its H (H >= 0; -0.0 is a
+// diagonally" bit of a cell travels in the sign of its H (H >= 0; -0 is a
 // diagonal zero) and a gap move out of a diagonal cell pays the penalty;
 // without one the bit is irrelevant and H is kept plain.  Ties prefer diag,
 // then left, then up.  Selects only, so a step is one basic block.
-template <bool GAPZ>
-IA_DEV double nw_cell(double diag_src, double sc, double up_enc, double left_enc, double gap,
-                      uint32_t &dir) {
-    const double diag = diag_src + sc;
-    double up, left;
+template <bool GAPZ, typename T>
+IA_DEV T nw_cell(T diag_src, T sc, T up_enc, T left_enc, T gap, uint32_t &dir) {
+    const T diag = diag_src + sc;
+    T up, left;
     if (GAPZ) {
         up = up_enc;
         left = left_enc;
     } else {
-        up = fabs(up_enc) + (signbit(up_enc) ? gap : 0.0);
-        left = fabs(left_enc) + (signbit(left_enc) ? gap : 0.0);
+        up = fabs(up_enc) + (signbit(up_enc) ? gap : T(0));
+        left = fabs(left_enc) + (signbit(left_enc) ? gap : T(0));
     }
     const bool is_diag = diag >= up && diag >= left;
     const bool l_ge_u = left >= up;
     dir = is_diag ? 0u : (l_ge_u ? 2u : 1u);
-    const double nh = is_diag ? diag : (l_ge_u ? left : up);
+    const T nh = is_diag ? diag : (l_ge_u ? left : up);
     return (GAPZ || !is_diag) ? nh : -nh;
 }
 
 // Plain value of an encoded H.
-template <bool GAPZ>
-IA_DEV double hval(double h) { return GAPZ ? h : fabs(h); }
+template <bool GAPZ, typename T>
+IA_DEV T hval(T h) { return GAPZ ? h : fabs(h); }
 
-// Trace layout: cell (i, j) of stripe k = (i-1)/64, lane l = ((i-1)%64)/2,
-// row r = (i-1)%2 is computed at step t = base(i) + j - 1 with
-// base(i) = k*P + 2l + r.  Its 2 direction bits sit at bit 2*(t%16) of word
-// t/16 - base(i)/16 of row i's block of `wpr` words, so every lane fills and
-// stores its words on the same steps.
-IA_DEV int trace_base(int i, int P) {
-    const int rem = (i - 1) & 63;
-    return ((i - 1) >> 6) * P + (rem & ~1) + (rem & 1);
+// Native point jc of the score matrix as FP32: the staged shared copy, or the
+// FP64 global array rounded on load.
+IA_DEV float4 native_f32(const NWParams &pr, const Pts &x, int jc) {
+    if (pr.Qf) return pr.Qf[jc];
+    const double *q = x.Q + 3 * jc;
+    return make_float4((float)q[0], (float)q[1], (float)q[2], 0.f);
+}
+
+// Trace layout: cell (i, j) of stripe k = (i-1)/64, row ri = (i-1)%64 of it
+// (lane ri/2, row ri%2 of the lane) is computed at step t = base(i) + j - 1
+// with base(i) = k*P + ri.  Its 2 direction bits sit at bit 2*(t%16) of the
+// word at ((k*G + g) * 64 + ri), g = t/16 - (k*P)/16 the step word within
+// the stripe, G = (P + 127) / 16 words per stripe (a lane stays in stripe k
+// for steps below (k+1)*P + 64, so g < G).  Every lane fills and stores its
+// two rows' words on the same steps, at adjacent addresses.
+IA_DEV int trace_base(int i, int P) { return ((i - 1) >> 6) * P + ((i - 1) & 63); }
+IA_DEV int trace_G(int P) { return (P + 127) / 16; }
+// Word of row i (1-based) whose row-relative index is w (w = t/16 -
+// base(i)/16), as an offset from the trace block.
+IA_DEV size_t trace_word(int i, int w, int P, int G) {
+    const int k = (i - 1) >> 6, ri = (i - 1) & 63;
+    const int g = w + ((k * P + ri) >> 4) - ((k * P) >> 4);
+    return ((size_t)k * G + g) * 64 + ri;
 }
 
 // Fill the trace of the NW DP for (R,t) and return the aligned pair count;
@@ -125,58 +162,61 @@ IA_DEV int trace_base(int i, int P) {
 // inlined: measured faster than out-of-line calls (the call frame costs more
 // than the registers it frees)
 #define IA_NW_ATTR IA_DEV
-template <int SMODE, bool GAPZ>
+template <int SMODE, bool GAPZ, typename T>
 IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
-                          double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
+                          double *bH_, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     const int lane = threadIdx.x & 31;
     const int plen = pr.plen, nlen = pr.nlen;
     if (lane == 0) atomicAdd(ctr + CTR_NW_CELLS, (unsigned long long)plen * (unsigned long long)nlen);
     const long long clk0 = clock64();
-    const int wpr = (nlen + 15) / 16 + 1;
     const int P = max(nlen + 1, 64);
+    const int G = trace_G(P);
     const int S = (plen + 63) >> 6;  // stripes
-    const double gap = pr.gap;
-    for (int j = lane; j <= nlen; j += 32) bH[j] = 0.0;
+    const T gap = (T)pr.gap;
+    const float inv_d0sq = (float)pr.inv_d0sq, cut2 = (float)pr.cut2;
+    T *bH = reinterpret_cast<T *>(bH_);  // stripe boundary row (nlen + 1 values)
+    for (int j = lane; j <= nlen; j += 32) bH[j] = T(0);
     __syncwarp();
     int k = 0, j0 = 1 - 2 * lane;  // stripe and row-0 column of this lane
     int i0 = 2 * lane + 1;         // 1-based row of row 0
-    double m0x = 0, m0y = 0, m0z = 0, m1x = 0, m1y = 0, m1z = 0;
+    float m0x = 0, m0y = 0, m0z = 0, m1x = 0, m1y = 0, m1z = 0;
     uint8_t l0 = 0, l1 = 0, ln1 = 0;
-    double h0 = 0.0, h1 = 0.0, h0prev = 0.0, up0prev = 0.0;
-    double q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
+    T h0 = 0, h1 = 0, h0prev = 0, up0prev = 0;
+    float q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
     uint32_t acc0 = 0, acc1 = 0;
     bool r0ok = false, r1ok = false;
-    uint32_t *row0 = trace, *row1 = trace;  // this lane's two trace rows
-    int wb0 = 0, wb1 = 0;                   // their first word index (base/16)
+    // this lane's two rows in the current stripe's block: word g of them at
+    // blk[g * 64 + 2 * lane], blk[g * 64 + 2 * lane + 1]; g0 = (k*P)/16
+    uint2 *blk = reinterpret_cast<uint2 *>(trace) + lane;
+    int g0 = 0;
     const int last_lane = ((plen - 1) & 63) >> 1;
     const int total_steps = (S - 1) * P + 2 * last_lane + 1 + nlen + 1;
 #pragma unroll kNwUnroll
     for (int step = 0; step < total_steps; step++) {
-        double up0 = __shfl_up_sync(kFull, h1, 1);
+        T up0 = __shfl_up_sync(kFull, h1, 1);
         if (j0 > P) {  // next stripe (rare): flush the finished rows' last words
             const int w = (step - 1) >> 4;
-            if (((step - 1) & 15) != 15) {  // else stored (and cleared) last step
-                if (r0ok && w - wb0 < wpr) row0[w - wb0] = acc0;
-                if (r1ok && w - wb1 < wpr) row1[w - wb1] = acc1;
-            }
+            if (((step - 1) & 15) != 15 && k < S)  // else stored (and cleared) last step
+                blk[(size_t)(w - g0) * 32] = make_uint2(acc0, acc1);
             j0 -= P;
             k++;
             i0 += 64;
+            blk = reinterpret_cast<uint2 *>(trace + (size_t)k * G * 64) + lane;
+            g0 = (k * P) >> 4;
         }
         if (j0 == 1) {  // entering a stripe (rare): set up its two rows
-            h0 = h1 = h0prev = up0prev = 0.0;
+            h0 = h1 = h0prev = up0prev = T(0);
             acc0 = acc1 = 0;
             r0ok = k < S && i0 <= plen;
             r1ok = k < S && i0 + 1 <= plen;
             const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
-            row0 = trace + (size_t)a0 * wpr;
-            row1 = trace + (size_t)a1 * wpr;
-            wb0 = step >> 4;
-            wb1 = (step + 1) >> 4;
             const double *p0 = x.P + 3 * a0, *p1 = x.P + 3 * a1;
             if (SMODE != SMAT_SS2 && SMODE != SMAT_EXPLICIT) {
-                xform(R, t, p0[0], p0[1], p0[2], m0x, m0y, m0z);
-                xform(R, t, p1[0], p1[1], p1[2], m1x, m1y, m1z);
+                double ax, ay, az, bx, by, bz;
+                xform(R, t, p0[0], p0[1], p0[2], ax, ay, az);
+                xform(R, t, p1[0], p1[1], p1[2], bx, by, bz);
+                m0x = (float)ax; m0y = (float)ay; m0z = (float)az;
+                m1x = (float)bx; m1y = (float)by; m1z = (float)bz;
             }
             if (SMODE == SMAT_SS2 || SMODE == SMAT_SS4) {
                 l0 = pr.Lp[a0];
@@ -184,50 +224,45 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
             }
         }
         const int jc = min(max(j0, 1), nlen) - 1;  // clamped 0-based column
-        double q0x = 0, q0y = 0, q0z = 0;
-        if (SMODE != SMAT_EXPLICIT) {
-            const double *q = x.Q + 3 * jc;
-            q0x = q[0]; q0y = q[1]; q0z = q[2];
+        float q0x = 0, q0y = 0, q0z = 0;
+        if (SMODE == SMAT_DP || SMODE == SMAT_SS4) {
+            const float4 q = native_f32(pr, x, jc);
+            q0x = q.x; q0y = q.y; q0z = q.z;
         }
         const uint8_t ln0 = (SMODE == SMAT_SS2 || SMODE == SMAT_SS4) ? pr.Ln[jc] : (uint8_t)0;
         const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;
-        if (lane == 0) up0 = (k > 0 && v0) ? bH[j0] : 0.0;
+        if (lane == 0) up0 = (k > 0 && v0) ? bH[j0] : T(0);
         uint32_t d0, d1;
-        double sc0, sc1;
+        T sc0, sc1;
         if (SMODE == SMAT_EXPLICIT) {
             const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
             const int jc1 = min(max(j0 - 1, 1), nlen) - 1;
-            sc0 = pr.smat[(size_t)a0 * nlen + jc];
-            sc1 = pr.smat[(size_t)a1 * nlen + jc1];
+            sc0 = (T)pr.smat[(size_t)a0 * nlen + jc];
+            sc1 = (T)pr.smat[(size_t)a1 * nlen + jc1];
         } else {
-            sc1 = smat_entry<SMODE>(pr, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
-            sc0 = smat_entry<SMODE>(pr, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
+            sc1 = smat_entry<SMODE, T>(inv_d0sq, cut2, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
+            sc0 = smat_entry<SMODE, T>(inv_d0sq, cut2, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
         }
-        const double n1 = nw_cell<GAPZ>(h0prev, sc1, h0, h1, gap, d1);
-        const double n0 = nw_cell<GAPZ>(up0prev, sc0, up0, h0, gap, d0);
+        const T n1 = nw_cell<GAPZ, T>(h0prev, sc1, h0, h1, gap, d1);
+        const T n0 = nw_cell<GAPZ, T>(up0prev, sc0, up0, h0, gap, d0);
         const int sh = 2 * (step & 15);
         acc0 |= d0 << sh;
         acc1 |= d1 << sh;
         if (lane == 31 && k + 1 < S && r1ok && j0 >= 2 && j0 <= nlen + 1) bH[j0 - 1] = n1;
-        if ((step & 15) == 15) {  // uniform: every lane stores its two words
-            const int w = step >> 4;
-            if (r0ok && w - wb0 < wpr) row0[w - wb0] = acc0;
-            if (r1ok && w - wb1 < wpr) row1[w - wb1] = acc1;
+        if ((step & 15) == 15) {  // uniform: the warp stores one 256-byte line
+            if (k < S) blk[(size_t)((step >> 4) - g0) * 32] = make_uint2(acc0, acc1);
             acc0 = acc1 = 0;
         }
-        h0prev = hval<GAPZ>(h0);
-        up0prev = hval<GAPZ>(up0);
+        h0prev = hval<GAPZ, T>(h0);
+        up0prev = hval<GAPZ, T>(up0);
         h1 = n1;
         h0 = n0;
         q1x = q0x; q1y = q0y; q1z = q0z;
         ln1 = ln0;
         j0++;
     }
-    if (((total_steps - 1) & 15) != 15) {  // flush the last rows' pending words
-        const int w = (total_steps - 1) >> 4;
-        if (r0ok && w - wb0 < wpr && w >= wb0) row0[w - wb0] = acc0;
-        if (r1ok && w - wb1 < wpr && w >= wb1) row1[w - wb1] = acc1;
-    }
+    if (((total_steps - 1) & 15) != 15 && k < S)  // flush the last rows' pending words
+        blk[(size_t)(((total_steps - 1) >> 4) - g0) * 32] = make_uint2(acc0, acc1);
     __syncwarp();
     const long long clk1 = clock64();
     // traceback from (plen, nlen): diag emits a pair, up steps i, else j.
@@ -247,11 +282,10 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
             if (r >= 1) {
                 const int br = trace_base(r, P);
                 const int wr = ((br + j - 1) >> 4) - (br >> 4);
-                const uint32_t *rowp = trace + (size_t)(r - 1) * wpr;
-                t3 = rowp[wr];
-                t2 = wr >= 1 ? rowp[wr - 1] : 0u;
-                t1 = wr >= 2 ? rowp[wr - 2] : 0u;
-                t0 = wr >= 3 ? rowp[wr - 3] : 0u;
+                t3 = trace[trace_word(r, wr, P, G)];
+                t2 = wr >= 1 ? trace[trace_word(r, wr - 1, P, G)] : 0u;
+                t1 = wr >= 2 ? trace[trace_word(r, wr - 2, P, G)] : 0u;
+                t0 = wr >= 3 ? trace[trace_word(r, wr - 3, P, G)] : 0u;
             }
         }
         const int wk = wi - (((bi + jl - 1) >> 4) - (bi >> 4)) + 3;  // 0..3 within the tile
@@ -281,11 +315,11 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
 IA_DEV int nw_align(const Pts &x, const NWParams &pr, const double *R, const double *t,
                     double *bH, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
     if (pr.smode == SMAT_DP) {
-        if (pr.gap == 0.0) return nw_align_t<SMAT_DP, true>(x, pr, R, t, bH, trace, al, ctr);
-        return nw_align_t<SMAT_DP, false>(x, pr, R, t, bH, trace, al, ctr);
+        if (pr.gap == 0.0) return nw_align_t<SMAT_DP, true, ChainDP>(x, pr, R, t, bH, trace, al, ctr);
+        return nw_align_t<SMAT_DP, false, ChainDP>(x, pr, R, t, bH, trace, al, ctr);
     }
-    if (pr.smode == SMAT_SS4) return nw_align_t<SMAT_SS4, false>(x, pr, R, t, bH, trace, al, ctr);
-    return nw_align_t<SMAT_SS2, false>(x, pr, R, t, bH, trace, al, ctr);
+    if (pr.smode == SMAT_SS4) return nw_align_t<SMAT_SS4, false, ChainDP>(x, pr, R, t, bH, trace, al, ctr);
+    return nw_align_t<SMAT_SS2, false, float>(x, pr, R, t, bH, trace, al, ctr);
 }
 
 // Kabsch on the aligned pairs + their compact TM (no d8)
@@ -406,12 +440,14 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
     __shared__ ChainCtl ctl;
     __shared__ uint64_t bar;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // shared layout: [native points as float4][pred labels][native labels]
+    // (flag 1), then per warp the NW boundary row (flag 2) and the alignment
+    // (flag 4); the FP64 point sets are read from global memory (L1)
     const bool coord_smem = flags & 1, bh_smem = flags & 2, al_smem = flags & 4;
-    const uint32_t pbytes = ((uint32_t)pmax * 24u + 47u) & ~15u;
-    const uint32_t nbytes = ((uint32_t)nmax * 24u + 47u) & ~15u;
+    const uint32_t qfbytes = (uint32_t)nmax * 16u;
     const uint32_t plb = ((uint32_t)pmax + 47u) & ~15u, nlb = ((uint32_t)nmax + 47u) & ~15u;
-    char *sP = smem, *sQ = sP + (coord_smem ? pbytes : 0);
-    char *sLp = sQ + (coord_smem ? nbytes : 0), *sLn = sLp + (coord_smem ? plb : 0);
+    char *sQf = smem;
+    char *sLp = sQf + (coord_smem ? qfbytes : 0), *sLn = sLp + (coord_smem ? plb : 0);
     char *wbase = sLn + (coord_smem ? nlb : 0);
     const uint32_t bh_bytes = (((uint32_t)nmax + 1u) * 8u + 15u) & ~15u;
     const uint32_t al_bytes = ((uint32_t)min(pmax, nmax) * 4u + 15u) & ~15u;
@@ -429,6 +465,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
     int staged = -1;
     Pts x = {nullptr, nullptr};
     const uint8_t *Lp = nullptr, *Ln = nullptr;
+    const float4 *Qf = nullptr;
     for (;;) {
         if (threadIdx.x == 0) {
             int c = atomicAdd(counter, 1);
@@ -455,20 +492,23 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             const double *gP = b.predc + 3 * (size_t)off, *gQ = b.natc + 3 * (size_t)off;
             const uint8_t *gLp = reinterpret_cast<const uint8_t *>(b.sspc + off);
             const uint8_t *gLn = reinterpret_cast<const uint8_t *>(b.ssnc + off);
+            x.P = gP;
+            x.Q = gQ;
             if (coord_smem) {
-                Copy cp[4];
-                char *dst[4] = {sP, sQ, sLp, sLn};
-                cp[0] = plan_copy(gP, (uint32_t)plen * 24u);
-                cp[1] = plan_copy(gQ, (uint32_t)nlen * 24u);
-                cp[2] = plan_copy(gLp, (uint32_t)plen);
-                cp[3] = plan_copy(gLn, (uint32_t)nlen);
-                stage_copies(cp, dst, 4, &bar, phase, b.err);
-                x.P = reinterpret_cast<const double *>(sP + cp[0].lead);
-                x.Q = reinterpret_cast<const double *>(sQ + cp[1].lead);
-                Lp = reinterpret_cast<const uint8_t *>(sLp + cp[2].lead);
-                Ln = reinterpret_cast<const uint8_t *>(sLn + cp[3].lead);
+                Copy cp[2];
+                char *dst[2] = {sLp, sLn};
+                cp[0] = plan_copy(gLp, (uint32_t)plen);
+                cp[1] = plan_copy(gLn, (uint32_t)nlen);
+                stage_copies(cp, dst, 2, &bar, phase, b.err);
+                float4 *qf = reinterpret_cast<float4 *>(sQf);
+                for (int i = threadIdx.x; i < nlen; i += blockDim.x)
+                    qf[i] = make_float4((float)gQ[3 * i], (float)gQ[3 * i + 1], (float)gQ[3 * i + 2], 0.f);
+                __syncthreads();
+                Qf = qf;
+                Lp = reinterpret_cast<const uint8_t *>(sLp + cp[0].lead);
+                Ln = reinterpret_cast<const uint8_t *>(sLn + cp[1].lead);
             } else {
-                x.P = gP; x.Q = gQ; Lp = gLp; Ln = gLn;
+                Qf = nullptr; Lp = gLp; Ln = gLn;
             }
             staged = T.pair;
         }
@@ -505,6 +545,7 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             pr.gap = gap;
             pr.Lp = Lp;
             pr.Ln = Ln;
+            pr.Qf = Qf;
             if (T.smode == SMAT_SS4) {
                 double d01 = fmax(I.d0 + 1.5, I.d0s);
                 pr.inv_d0sq = 1.0 / (d01 * d01);
@@ -549,8 +590,9 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                 // >= 3 valid residues (indialign_c/align.h:141)
                 const bool sized = plen >= 3 && nlen >= 3;
                 for (int it = 0; live && sized && it < T.max_iter; it++) {
-                    const int na = pr.gap == 0.0 ? nw_align_t<SMAT_DP, true>(x, pr, R, t, bH, trace, al, b.ctr)
-                                                 : nw_align_t<SMAT_DP, false>(x, pr, R, t, bH, trace, al, b.ctr);
+                    const int na = pr.gap == 0.0
+                                       ? nw_align_t<SMAT_DP, true, ChainDP>(x, pr, R, t, bH, trace, al, b.ctr)
+                                       : nw_align_t<SMAT_DP, false, ChainDP>(x, pr, R, t, bH, trace, al, b.ctr);
                     if (na < 3) break;  // same transform -> same alignment next time
                     double nR[9], nt[3], dR[9], dt[3];
                     const long long ck0 = clock64();
@@ -605,12 +647,13 @@ __global__ void k_nw_explicit(const double *__restrict__ smat, int np, int nn, d
     pr.cut2 = 0.0;
     pr.Lp = pr.Ln = nullptr;
     pr.smat = smat;
+    pr.Qf = nullptr;
     Pts x = {nullptr, nullptr};
     const double I[12] = {1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0};
     int na = 0;
     if (np >= 1 && nn >= 1) {
-        if (gap == 0.0) na = nw_align_t<SMAT_EXPLICIT, true>(x, pr, I, I + 9, bH, trace, al, ctr);
-        else na = nw_align_t<SMAT_EXPLICIT, false>(x, pr, I, I + 9, bH, trace, al, ctr);
+        if (gap == 0.0) na = nw_align_t<SMAT_EXPLICIT, true, double>(x, pr, I, I + 9, bH, trace, al, ctr);
+        else na = nw_align_t<SMAT_EXPLICIT, false, double>(x, pr, I, I + 9, bH, trace, al, ctr);
     }
     for (int k = threadIdx.x; k < na; k += 32) {
         const uint32_t e = al[na - 1 - k];
@@ -620,7 +663,7 @@ __global__ void k_nw_explicit(const double *__restrict__ smat, int np, int nn, d
     if (threadIdx.x == 0) *na_out = na;
 }
 
-size_t nw_trace_words(int np, int nn) { return (size_t)np * ((nn + 15) / 16 + 1); }
+size_t nw_trace_words(int np, int nn) { return nw_trace_words_for(np, nn); }
 
 void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t *trace,
                         double *bH, uint32_t *al, int *ap, int *an, int *na,
@@ -631,7 +674,7 @@ void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t
 size_t chain_smem_bytes(int pmax, int nmax, int flags) {
     size_t s = 0;
     if (flags & 1) {
-        s += (((size_t)pmax * 24 + 47) & ~size_t(15)) + (((size_t)nmax * 24 + 47) & ~size_t(15));
+        s += (size_t)nmax * 16;
         s += (((size_t)pmax + 47) & ~size_t(15)) + (((size_t)nmax + 47) & ~size_t(15));
     }
     if (flags & 2) s += kChainWarps * ((((size_t)nmax + 1) * 8 + 15) & ~size_t(15));

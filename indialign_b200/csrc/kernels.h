@@ -93,6 +93,12 @@ void launch_chain(const DevBatch &b, const ChainTask *tasks, const int *chunk_be
 cudaError_t chain_set_attributes();
 const void *chain_kernel_ptr();
 size_t nw_trace_words(int np, int nn);
+// NW trace words of an np x nn problem in k_chain.cu's layout: per 64-row
+// stripe a block of G step words x 64 rows, G = (P + 127) / 16 with period
+// P = max(nn + 1, 64).
+constexpr size_t nw_trace_words_for(int np, int nn) {
+    return (size_t)((np + 63) / 64) * 64 * (size_t)(((nn + 1 > 64 ? nn + 1 : 64) + 127) / 16);
+}
 void launch_nw_explicit(const double *smat, int np, int nn, double gap, uint32_t *trace,
                         double *bH, uint32_t *al, int *ap, int *an, int *na,
                         unsigned long long *ctr, cudaStream_t st);

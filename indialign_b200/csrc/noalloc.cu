@@ -29,7 +29,7 @@
 namespace ia {
 
 constexpr int kNoAllocMaxLen = 2048;
-constexpr size_t kNATraceWords = (size_t)kNoAllocMaxLen * ((kNoAllocMaxLen + 15) / 16 + 1);
+constexpr size_t kNATraceWords = nw_trace_words_for(kNoAllocMaxLen, kNoAllocMaxLen);
 constexpr size_t kNABhOff = ((kNATraceWords * 4 + 255) / 256) * 256;
 constexpr size_t kNAAlOff = kNABhOff + (((kNoAllocMaxLen + 1) * 8 + 255) / 256) * 256;
 constexpr size_t kNACtrOff = kNAAlOff + ((kNoAllocMaxLen * 4 + 255) / 256) * 256;

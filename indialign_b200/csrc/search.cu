@@ -424,7 +424,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
         if (I.nlen > nmax) nmax = I.nlen;
     }
     chain_flags_ = 0;
-    if ((size_t)(pmax + nmax) * 25 + 256 <= 96 * 1024) chain_flags_ |= 1;
+    if ((size_t)nmax * 17 + pmax + 256 <= 96 * 1024) chain_flags_ |= 1;
     if (nmax <= 512) chain_flags_ |= 2;
     if ((pmax < nmax ? pmax : nmax) <= 2048) chain_flags_ |= 4;
     size_t smem = chain_smem_bytes(pmax, nmax, chain_flags_);
@@ -432,7 +432,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, chain_kernel_ptr(), 32 * kChainWarps,
                                                      smem));
     if (per_sm < 1) per_sm = 1;
-    trace_words_ = (size_t)pmax * ((nmax + 15) / 16 + 1);  // NW trace rows (k_chain.cu)
+    trace_words_ = nw_trace_words_for(pmax, nmax);  // NW trace block per warp (k_chain.cu)
     long long warps = (long long)c_->sms * per_sm * kChainWarps;
     const size_t budget = (size_t)4 << 30;  // trace scratch budget
     long long cap = (long long)(budget / (trace_words_ * 4 + 1));

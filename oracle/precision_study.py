@@ -19,6 +19,12 @@ change of the final TM-score against the reference:
               converted to FP32, FP32 distances / inlier tests / raw moments,
               FP32 item scores with a compensated sum, FP64 eigen-solves, the
               winner rescored in FP64; everything else FP64
+  smat32      only the score-matrix entries of dp_refine and of the SS +
+              distance NW lowered, in the NW-chain kernel's form: the moved
+              pred point rounded to FP32, FP32 difference, d2, cutoff test and
+              term 1/(1 + d2 * (1/d0^2)), widened to FP64 for the DP
+  dp32        smat32 plus the NW fill's values (H, diagonal and gap moves)
+              in FP32
   qcp64       all FP64, every Kabsch eigen-solve by the characteristic
               polynomial of Horn's key matrix (Newton for its top roots,
               eigenvector from an adjugate column) instead of Jacobi sweeps,
@@ -483,6 +489,37 @@ def _bank32(src: str) -> str:
     return _sub(s, BANK32_GAPLESS_OLD, BANK32_GAPLESS_NEW)
 
 
+def _smat32(s: str) -> str:
+    """Score-matrix entries (dp_refine and the SS+distance NW) in FP32, in the
+    NW-chain kernel's form: the pred point moved in FP64 and rounded to FP32,
+    FP32 difference / d2 / cutoff test, the term 1/(1 + d2 * (1/d0^2)) in
+    FP32, widened to FP64 for the DP."""
+    s = _sub(s, '''                    double dx = m[0] - n[0], dy = m[1] - n[1], dz = m[2] - n[2];
+                    double d2 = dx * dx + dy * dy + dz * dz;
+                    smat[(size_t)a * nlen + b] = d2 <= sd8sq ? 1.0 / (1.0 + d2 / d0sq_dp) : 0.0;''',
+             '''                    float dx = (float)m[0] - (float)n[0], dy = (float)m[1] - (float)n[1],
+                          dz = (float)m[2] - (float)n[2];
+                    float d2 = dx * dx + dy * dy + dz * dz;
+                    smat[(size_t)a * nlen + b] =
+                        d2 <= (float)sd8sq ? (double)(1.0f / (1.0f + d2 * (float)(1.0 / d0sq_dp))) : 0.0;''')
+    s = _sub(s, '''                double dx = m[0] - n[0], dy = m[1] - n[1], dz = m[2] - n[2];
+                double sc = 1.0 / (1.0 + (dx * dx + dy * dy + dz * dz) / d01sq);''',
+             '''                float dx = (float)m[0] - (float)n[0], dy = (float)m[1] - (float)n[1], dz = (float)m[2] - (float)n[2];
+                double sc = (double)(1.0f / (1.0f + (dx * dx + dy * dy + dz * dz) * (float)(1.0 / d01sq)));''')
+    return s
+
+
+def _dp32(s: str) -> str:
+    """The NW fill's values (H, the diagonal, gap moves) in FP32 as well."""
+    return _sub(_smat32(s), '''            double diag = H[(i - 1) * Hn + (j - 1)] + smat[(i - 1) * Nn + (j - 1)];
+            double up = H[(i - 1) * Hn + j], left = H[i * Hn + (j - 1)];
+            if (tr[(i - 1) * Hn + j] == 0) up += gap;
+            if (tr[i * Hn + (j - 1)] == 0) left += gap;''', '''            float diag = (float)H[(i - 1) * Hn + (j - 1)] + (float)smat[(i - 1) * Nn + (j - 1)];
+            float up = (float)H[(i - 1) * Hn + j], left = (float)H[i * Hn + (j - 1)];
+            if (tr[(i - 1) * Hn + j] == 0) up += (float)gap;
+            if (tr[i * Hn + (j - 1)] == 0) left += (float)gap;''')
+
+
 def variant_sources(src: str) -> dict[str, str]:
     base = _sub(src, DIST64, DIST32)
     out = {"dist32": base}
@@ -499,6 +536,8 @@ def variant_sources(src: str) -> dict[str, str]:
         out[name] = f"#define OFFSET_MEAN {mean}\n" + s
     out["bank32"] = _bank32(src)
     out["qcp64"] = _qcp64(src)
+    out["smat32"] = _smat32(src)
+    out["dp32"] = _dp32(src)
     return out
 
 

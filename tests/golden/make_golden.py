@@ -3,7 +3,7 @@
 Runs here, where the reference sources exist:
 
     make -C oracle && python tests/golden/make_golden.py          # small sets
-    python tests/golden/make_golden.py shapes                       # cfg1 / cfg2
+    python tests/golden/make_golden.py shapes [cfg1] [cfg2]         # workload shapes
 
 oracle/_ref/libindialign_ref.so is the reference's `make cpu` build compiled
 from its sources (oracle/Makefile); ref_trace_search (oracle/ref_stages.cpp)
@@ -151,8 +151,10 @@ def run_ref_serial(pairs, procs=8):
     return s, R, t, trace
 
 
-def main_shapes():
+def main_shapes(only=()):
     for name, pairs in (("cfg1", cfg1_pairs()), ("cfg2", cfg2_pairs())):
+        if only and name not in only:
+            continue
         s, R, t, trace = run_ref_serial(pairs)
         np.savez_compressed(os.path.join(OUT, f"golden_{name}.npz"), score=s, R=R, t=t, trace=trace,
                             sigma=np.array([p.sigma for p in pairs]),
@@ -230,7 +232,7 @@ def main():
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["shapes"]:
-        main_shapes()
+    if sys.argv[1:2] == ["shapes"]:
+        main_shapes(tuple(sys.argv[2:]))
     else:
         main()
