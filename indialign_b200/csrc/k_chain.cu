@@ -32,11 +32,13 @@ namespace ia {
 constexpr unsigned kFull = 0xffffffffu;
 
 // build-time tuning knobs: minimum resident CTAs per SM for k_chain (caps
-// registers; 4 -> 128 registers measured best) and the NW step-loop unroll
-// factor (1 measured best: the rare stripe branches make unrolled copies
-// larger without shortening the dependency chain)
+// registers; 5 -> 96 registers measured best with the NW fill out of line,
+// 8% faster than 4 -> 128, while 6 and 8 were slower) and the NW step-loop
+// unroll factor (1 measured best: the rare stripe branches make unrolled
+// copies larger without shortening the dependency chain; a 16-step unrolled
+// block without those branches measured 2x slower)
 #ifndef IA_CHAIN_MINB
-#define IA_CHAIN_MINB 4
+#define IA_CHAIN_MINB 5
 #endif
 #ifndef IA_NW_UNROLL
 #define IA_NW_UNROLL 1
@@ -159,9 +161,12 @@ IA_DEV size_t trace_word(int i, int w, int P, int G) {
 // the matrix are computed on clamped indices and never read by a valid one
 // (a row's state is reset when it enters a stripe, and its neighbours only
 // read its in-range cells), so the step has no per-cell branches.
-// inlined: measured faster than out-of-line calls (the call frame costs more
-// than the registers it frees)
-#define IA_NW_ATTR IA_DEV
+// Out of line: inside the chain kernel (register-capped) an inlined fill
+// shares the register budget with the caller's live state and spilled inside
+// its step loop (measured: ~4 local loads per step); as a call it has the
+// whole budget and no spills, and the caller's state is saved once per
+// alignment.
+#define IA_NW_ATTR __device__ __noinline__
 template <int SMODE, bool GAPZ, typename T>
 IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, const double *t,
                           double *bH_, uint32_t *trace, uint32_t *al, unsigned long long *ctr) {
@@ -428,6 +433,23 @@ struct ChainCtl {
     int chunk, task, next;
 };
 
+// Element `lane` of a result record {score, R[9], t[3]} by unrolled selects
+// (a dynamic index into R or t would move them to local memory).
+IA_DEV double rec_elem(int lane, double score, const double *R, const double *t) {
+    double v = score;
+#pragma unroll
+    for (int a = 0; a < 9; a++) v = lane == 1 + a ? R[a] : v;
+#pragma unroll
+    for (int a = 0; a < 3; a++) v = lane == 10 + a ? t[a] : v;
+    return v;
+}
+
+// dst[0..11] = {R[9], t[3]} written by lanes 0..11 of the warp.
+IA_DEV void put_rt(double *dst, const double *R, const double *t, int lane) {
+    const double v = rec_elem(lane + 1, 0.0, R, t);
+    if (lane < 12) dst[lane] = v;
+}
+
 // EMIT = false: LITE dp_refine chains only (the hot rescue kernel, DP score
 // mode only); EMIT = true: single NW alignments for SS seeds / full dp_refine.
 // Two instantiations keep the hot kernel's code small.
@@ -439,6 +461,10 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
     extern __shared__ __align__(16) char smem[];
     __shared__ ChainCtl ctl;
     __shared__ uint64_t bar;
+    // per warp: the LITE chain's current (R, t) and its best (R, t), kept in
+    // shared memory so that no transform stays live in registers across the
+    // NW fill
+    __shared__ double s_rt[kChainWarps][24];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // shared layout: [native points as float4][pred labels][native labels]
     // (flag 1), then per warp the NW boundary row (flag 2) and the alignment
@@ -579,20 +605,28 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
                     double nR[9], nt[3];
                     double s = aligned_kabsch(x, al, na, I.d0, I.lnorm, nR, nt, b.ctr);
                     double *o = T.res + (size_t)si * kRec;
-                    if (lane < kRec) o[lane] = lane == 0 ? s : (lane < 10 ? nR[lane - 1] : nt[lane - 10]);
+                    const double v = rec_elem(lane, s, nR, nt);
+                    if (lane < kRec) o[lane] = v;
                 }
             } else {
                 // LITE dp_refine chain (indialign_c/align.h:54-145,
                 // d0_search_lite): best starts at score 0 / identity.
-                double bs = 0.0, bR[9], bt[3];
-                set_identity(bR, bt);
+                double *rt = s_rt[warp];  // [current R, t][best R, t]
+                double bs = 0.0;
+                {
+                    double iR[9], it_[3];
+                    set_identity(iR, it_);
+                    put_rt(rt, R, t, lane);
+                    put_rt(rt + 12, iR, it_, lane);
+                }
+                __syncwarp();
                 // dp_refine_chunk returns 0 / identity unless both sides have
                 // >= 3 valid residues (indialign_c/align.h:141)
                 const bool sized = plen >= 3 && nlen >= 3;
                 for (int it = 0; live && sized && it < T.max_iter; it++) {
                     const int na = pr.gap == 0.0
-                                       ? nw_align_t<SMAT_DP, true, ChainDP>(x, pr, R, t, bH, trace, al, b.ctr)
-                                       : nw_align_t<SMAT_DP, false, ChainDP>(x, pr, R, t, bH, trace, al, b.ctr);
+                                       ? nw_align_t<SMAT_DP, true, ChainDP>(x, pr, rt, rt + 9, bH, trace, al, b.ctr)
+                                       : nw_align_t<SMAT_DP, false, ChainDP>(x, pr, rt, rt + 9, bH, trace, al, b.ctr);
                     if (na < 3) break;  // same transform -> same alignment next time
                     double nR[9], nt[3], dR[9], dt[3];
                     const long long ck0 = clock64();
@@ -610,21 +644,17 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
 #pragma unroll
                         for (int a = 0; a < 3; a++) nt[a] = dt[a];
                     }
-#pragma unroll
-                    for (int a = 0; a < 9; a++) R[a] = nR[a];
-#pragma unroll
-                    for (int a = 0; a < 3; a++) t[a] = nt[a];
+                    __syncwarp();  // every lane's NW reads of the current (R, t) are done
+                    put_rt(rt, nR, nt, lane);
                     if (s > bs) {
                         bs = s;
-#pragma unroll
-                        for (int a = 0; a < 9; a++) bR[a] = nR[a];
-#pragma unroll
-                        for (int a = 0; a < 3; a++) bt[a] = nt[a];
+                        put_rt(rt + 12, nR, nt, lane);
                     }
+                    __syncwarp();
                 }
                 double *o = T.res + (size_t)chain * kRec;
-                if (lane < kRec) o[lane] = lane == 0 ? (live ? bs : kNegInf)
-                                                     : (lane < 10 ? bR[lane - 1] : bt[lane - 10]);
+                if (lane < kRec) o[lane] = lane == 0 ? (live ? bs : kNegInf) : rt[12 + lane - 1];
+                __syncwarp();  // the slot is reused by this warp's next chain
             }
         }
         __syncthreads();

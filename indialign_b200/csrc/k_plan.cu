@@ -149,7 +149,7 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
     }
     T.n_items = on ? T.K * T.C : 0;
     c.btasks[s] = T;
-    c.counts[s] = (T.n_items + kBankChunk - 1) / kBankChunk;
+    c.counts[s] = (T.n_items + kBankChunkItems - 1) / kBankChunkItems;
 }
 
 // ---- chain plans ------------------------------------------------------------

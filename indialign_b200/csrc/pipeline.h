@@ -22,7 +22,11 @@ constexpr int kDetC = 6;           // cutoffs of the detailed searches
 constexpr int kMaxSeeds = 1024;    // fragment windows (<= 1+9*101) + anchors
 constexpr int kMaxBitSeeds = 32;   // anchor masks (<= 6 radii x 5) + top-k mask
 constexpr int kRec = 13;           // {score, R[9], t[3]}
-constexpr int kBankChunk = 128;    // bank items per CTA chunk (4 warps x 32)
+constexpr int kBankChunk = 128;    // threads of a bank CTA (4 warps x 32)
+#ifndef IA_BANK_CHUNK_ITEMS
+#define IA_BANK_CHUNK_ITEMS 256
+#endif
+constexpr int kBankChunkItems = IA_BANK_CHUNK_ITEMS;  // bank items per CTA chunk
 constexpr int kChainWarps = 4;     // warps per NW-chain CTA
 constexpr int kChainChunk = 16;    // chains per CTA chunk, pulled by the warps
 constexpr double kNegInf = -1e300; // "no candidate" marker
