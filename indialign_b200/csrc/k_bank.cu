@@ -13,7 +13,8 @@
 // Precision: the residue visits -- transform, distance, inlier test, raw
 // moment sums and the item's TM sum -- run in FP32 (the point set is staged
 // as FP64, centred on its FP64 mean and converted to FP32 in shared memory;
-// the TM sum is compensated); each
+// the TM sum is compensated; the operation order is fixed with explicit
+// fused multiply-adds, as restated by the oracle's FP32 study build); each
 // Kabsch eigen-solve runs in FP64 from the FP32 moments, and reduce_bank
 // rescores the task's winning item in FP64, so every reported score is an
 // FP64 TM-score of the returned (R, t).  The oracle rebuilt with this
@@ -59,9 +60,9 @@ struct MomentsF {
     IA_DEV void add(float px, float py, float pz, float qx, float qy, float qz) {
         sp[0] += px; sp[1] += py; sp[2] += pz;
         sq[0] += qx; sq[1] += qy; sq[2] += qz;
-        h[0] += px * qx; h[1] += px * qy; h[2] += px * qz;
-        h[3] += py * qx; h[4] += py * qy; h[5] += py * qz;
-        h[6] += pz * qx; h[7] += pz * qy; h[8] += pz * qz;
+        h[0] = fmaf(px, qx, h[0]); h[1] = fmaf(px, qy, h[1]); h[2] = fmaf(px, qz, h[2]);
+        h[3] = fmaf(py, qx, h[3]); h[4] = fmaf(py, qy, h[4]); h[5] = fmaf(py, qz, h[5]);
+        h[6] = fmaf(pz, qx, h[6]); h[7] = fmaf(pz, qy, h[7]); h[8] = fmaf(pz, qz, h[8]);
         w++;
     }
     // Kabsch in FP64 from these sums (identity below 3 pairs)
@@ -81,16 +82,29 @@ struct MomentsF {
 
 // The FP32 work runs on coordinates centred on their point set's FP64 mean
 // (so the raw moments do not cancel against a large offset); the kernel's
-// (R, t) live in that frame until an item is written out.
+// (R, t) live in that frame until an item is written out.  A point is a
+// float4 (x, y, z, w) with w = 1 for a valid residue of the cutoff and score
+// passes (V[i] != 0, or no mask) and 0 otherwise.
 //
-// Point coordinate k (3*i + axis) in the centred frame as FP32: from the
-// converted shared copy, or converted on load from the FP64 global arrays
-// (point sets too large for shared memory).  Both give the same float, so a
-// pair's results do not depend on which path its batch takes.
+// Point i of a set in the centred FP32 frame: the converted shared copy, or
+// converted on load from the FP64 global array (point sets too large for
+// shared memory).  Both give the same floats, so a pair's results do not
+// depend on which path its batch takes.
 template <bool SMEM>
-IA_DEV float coord(const float *f, const double *d, const double *off, int k) {
-    if constexpr (SMEM) return f[k];
-    else return (float)(d[k] - off[k % 3]);
+IA_DEV float4 point(const float4 *f, const double *d, const double *off, const uint8_t *V, int i) {
+    if constexpr (SMEM) return f[i];
+    else return make_float4((float)(d[3 * i] - off[0]), (float)(d[3 * i + 1] - off[1]),
+                            (float)(d[3 * i + 2] - off[2]), (V == nullptr || V[i] != 0) ? 1.f : 0.f);
+}
+
+// Squared distance of p moved by (Rf, tf) from q, in a fixed FP32 operation
+// order (the order the oracle's FP32 study build restates):
+// d = ((t - q) + p_z R + p_y R) + p_x R per axis, d2 = (dx^2 + dy^2) + dz^2.
+IA_DEV float dist2_f32(const float4 &p, const float4 &q, const float *Rf, const float *tf) {
+    const float dx = fmaf(p.x, Rf[0], fmaf(p.y, Rf[3], fmaf(p.z, Rf[6], tf[0] - q.x)));
+    const float dy = fmaf(p.x, Rf[1], fmaf(p.y, Rf[4], fmaf(p.z, Rf[7], tf[1] - q.y)));
+    const float dz = fmaf(p.x, Rf[2], fmaf(p.y, Rf[5], fmaf(p.z, Rf[8], tf[2] - q.z)));
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
 }
 
 // CTA-wide FP64 mean of the finite values of n points, per axis, into
@@ -138,24 +152,23 @@ IA_DEV void points_mean(const double *src, int n, double *out, double *red) {
 }
 
 // CTA-wide in-place conversion of n staged FP64 points (at src, inside the
-// region that starts at dst) to centred FP32 at dst.  Round r reads points
-// [128r, 128r+128) before any thread writes them; its writes end at byte
-// 12*128(r+1), below the first byte (24*128(r+1)) that a later round reads.
-IA_DEV void points_to_f32(const double *src, float *dst, int n, const double *off) {
+// region that starts at dst) to centred FP32 float4 at dst, w from the
+// validity bytes V (null: all valid).  Round r reads points [128r, 128r+128)
+// before any thread writes them; its writes end at byte 16*128(r+1), at or
+// below the first byte (24*128(r+1)) that a later round reads.
+IA_DEV void points_to_f32(const double *src, float4 *dst, int n, const double *off, const uint8_t *V) {
     for (int base = 0; base < n; base += kBankChunk) {
         const int i = base + (int)threadIdx.x;
         double x = 0.0, y = 0.0, z = 0.0;
+        float w = 0.f;
         if (i < n) {
             x = src[3 * i] - off[0];
             y = src[3 * i + 1] - off[1];
             z = src[3 * i + 2] - off[2];
+            w = (V == nullptr || V[i] != 0) ? 1.f : 0.f;
         }
         __syncthreads();
-        if (i < n) {
-            dst[3 * i] = (float)x;
-            dst[3 * i + 1] = (float)y;
-            dst[3 * i + 2] = (float)z;
-        }
+        if (i < n) dst[i] = make_float4((float)x, (float)y, (float)z, w);
     }
     __syncthreads();
 }
@@ -181,7 +194,7 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
     __syncthreads();
     const int total = scan->total_chunks;
     int staged = -1;
-    const float *Pf = nullptr, *Qf = nullptr;   // shared FP32 copies (SMEM)
+    const float4 *Pf = nullptr, *Qf = nullptr;  // shared FP32 copies (SMEM)
     const double *Pd = nullptr, *Qd = nullptr;  // global FP64 arrays (!SMEM)
     const uint8_t *V = nullptr, *PV = nullptr, *NV = nullptr;
     for (;;) {
@@ -220,12 +233,12 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 const double *dQ = reinterpret_cast<const double *>(sQ + cp[1].lead);
                 points_mean(dP, n, oP, red);
                 points_mean(dQ, n, oQ, red);
-                points_to_f32(dP, reinterpret_cast<float *>(sP), n, oP);
-                points_to_f32(dQ, reinterpret_cast<float *>(sQ), n, oQ);
-                Pf = reinterpret_cast<const float *>(sP);
-                Qf = reinterpret_cast<const float *>(sQ);
                 int k = 2;
                 V = T.V ? reinterpret_cast<const uint8_t *>(sV + cp[k++].lead) : nullptr;
+                points_to_f32(dP, reinterpret_cast<float4 *>(sP), n, oP, V);
+                points_to_f32(dQ, reinterpret_cast<float4 *>(sQ), n, oQ, nullptr);
+                Pf = reinterpret_cast<const float4 *>(sP);
+                Qf = reinterpret_cast<const float4 *>(sQ);
                 PV = T.PV ? reinterpret_cast<const uint8_t *>(sPV + cp[k++].lead) : nullptr;
                 NV = T.NV ? reinterpret_cast<const uint8_t *>(sNV + cp[k++].lead) : nullptr;
             } else {
@@ -277,9 +290,10 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             for (int i = 0; i < n; i++) {
                 int j = i - o;
                 bool sel = active && j >= 0 && j < n && PV[i] != 0 && NV[j] != 0;
-                if (sel)
-                    m.add(coord<SMEM>(Pf, Pd, oP, 3 * i), coord<SMEM>(Pf, Pd, oP, 3 * i + 1), coord<SMEM>(Pf, Pd, oP, 3 * i + 2),
-                          coord<SMEM>(Qf, Qd, oQ, 3 * j), coord<SMEM>(Qf, Qd, oQ, 3 * j + 1), coord<SMEM>(Qf, Qd, oQ, 3 * j + 2));
+                if (sel) {
+                    const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, j);
+                    m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
+                }
             }
             skip = m.w < T.shift_min;
         } else {
@@ -299,9 +313,10 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                 bool sel;
                 if (brow) sel = ((brow[i >> 5] >> (i & 31)) & 1u) && (v & 1u);  // 1 & valid
                 else sel = i >= s && i < s + len && v != 0;                    // valid & valid
-                if (active && sel)
-                    m.add(coord<SMEM>(Pf, Pd, oP, 3 * i), coord<SMEM>(Pf, Pd, oP, 3 * i + 1), coord<SMEM>(Pf, Pd, oP, 3 * i + 2),
-                          coord<SMEM>(Qf, Qd, oQ, 3 * i), coord<SMEM>(Qf, Qd, oQ, 3 * i + 1), coord<SMEM>(Qf, Qd, oQ, 3 * i + 2));
+                if (active && sel) {
+                    const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, i);
+                    m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
+                }
             }
         }
         if (active && !skip) m.kabsch(R, t);
@@ -319,19 +334,10 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             m.clear();
             int cnt = 0;
             for (int i = 0; i < n; i++) {
-                const float px = coord<SMEM>(Pf, Pd, oP, 3 * i), py = coord<SMEM>(Pf, Pd, oP, 3 * i + 1),
-                            pz = coord<SMEM>(Pf, Pd, oP, 3 * i + 2);
-                const float qx = coord<SMEM>(Qf, Qd, oQ, 3 * i), qy = coord<SMEM>(Qf, Qd, oQ, 3 * i + 1),
-                            qz = coord<SMEM>(Qf, Qd, oQ, 3 * i + 2);
-                const bool v = V ? V[i] != 0 : true;
-                if (running && v) {
-                    const float dx = px * Rf[0] + py * Rf[3] + pz * Rf[6] + tf[0] - qx;
-                    const float dy = px * Rf[1] + py * Rf[4] + pz * Rf[7] + tf[1] - qy;
-                    const float dz = px * Rf[2] + py * Rf[5] + pz * Rf[8] + tf[2] - qz;
-                    if (dx * dx + dy * dy + dz * dz <= cut2) {
-                        m.add(px, py, pz, qx, qy, qz);
-                        cnt++;
-                    }
+                const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, i);
+                if (running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2) {
+                    m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
+                    cnt++;
                 }
             }
             if (running) {
@@ -346,7 +352,9 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         // with a compensated sum; reduce_bank rescores the winner in FP64 ----
         double score = kNegInf;
         if (active && !skip) {
-            const float d0sq = (float)fmax(T.d0 * T.d0, 1e-12), sd8sq = (float)(T.sd8 * T.sd8);
+            // term 1 / fma(d2, 1/d0^2, 1): a correctly rounded reciprocal of
+            // one fused operation instead of two divisions
+            const float inv_d0sq = (float)(1.0 / fmax(T.d0 * T.d0, 1e-12)), sd8sq = (float)(T.sd8 * T.sd8);
             float Rf[9], tf[3];
 #pragma unroll
             for (int a = 0; a < 9; a++) Rf[a] = (float)R[a];
@@ -354,16 +362,11 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
             float sum = 0.f, comp = 0.f;
             for (int i = 0; i < n; i++) {
-                const bool v = V ? V[i] != 0 : true;
-                if (!v) continue;
-                const float px = coord<SMEM>(Pf, Pd, oP, 3 * i), py = coord<SMEM>(Pf, Pd, oP, 3 * i + 1),
-                            pz = coord<SMEM>(Pf, Pd, oP, 3 * i + 2);
-                const float dx = px * Rf[0] + py * Rf[3] + pz * Rf[6] + tf[0] - coord<SMEM>(Qf, Qd, oQ, 3 * i);
-                const float dy = px * Rf[1] + py * Rf[4] + pz * Rf[7] + tf[1] - coord<SMEM>(Qf, Qd, oQ, 3 * i + 1);
-                const float dz = px * Rf[2] + py * Rf[5] + pz * Rf[8] + tf[2] - coord<SMEM>(Qf, Qd, oQ, 3 * i + 2);
-                const float d2 = dx * dx + dy * dy + dz * dz;
+                const float4 pp = point<SMEM>(Pf, Pd, oP, V, i);
+                if (pp.w == 0.f) continue;
+                const float d2 = dist2_f32(pp, point<SMEM>(Qf, Qd, oQ, nullptr, i), Rf, tf);
                 if (!T.use_d8 || d2 <= sd8sq) {
-                    const float y = 1.0f / (1.0f + d2 / d0sq) - comp;
+                    const float y = __frcp_rn(fmaf(d2, inv_d0sq, 1.0f)) - comp;
                     const float s2 = sum + y;
                     comp = (s2 - sum) - y;
                     sum = s2;

@@ -19,6 +19,9 @@ change of the final TM-score against the reference:
               converted to FP32, FP32 distances / inlier tests / raw moments,
               FP32 item scores with a compensated sum, FP64 eigen-solves, the
               winner rescored in FP64; everything else FP64
+  bank32f     bank32 in the seed-bank kernel's explicit FP32 operation
+              sequence (fused transform, d2 and moment products; the item
+              score's term 1 / fma(d2, 1/d0^2, 1))
   smat32      only the score-matrix entries of dp_refine and of the SS +
               distance NW lowered, in the NW-chain kernel's form: the moved
               pred point rounded to FP32, FP32 difference, d2, cutoff test and
@@ -480,6 +483,38 @@ def _qcp64(src: str) -> str:
     return _sub(s, QCP64_CALL_OLD, QCP64_CALL_NEW)
 
 
+BANK32F_OLD_D2 = '''static float d2_32(const float *p, const float *q, const float *Rf, const float *tf) {
+    float dx = p[0] * Rf[0] + p[1] * Rf[3] + p[2] * Rf[6] + tf[0] - q[0];
+    float dy = p[0] * Rf[1] + p[1] * Rf[4] + p[2] * Rf[7] + tf[1] - q[1];
+    float dz = p[0] * Rf[2] + p[1] * Rf[5] + p[2] * Rf[8] + tf[2] - q[2];
+    return dx * dx + dy * dy + dz * dz;
+}'''
+BANK32F_NEW_D2 = '''static float d2_32(const float *p, const float *q, const float *Rf, const float *tf) {
+    float dx = fmaf(p[0], Rf[0], fmaf(p[1], Rf[3], fmaf(p[2], Rf[6], tf[0] - q[0])));
+    float dy = fmaf(p[0], Rf[1], fmaf(p[1], Rf[4], fmaf(p[2], Rf[7], tf[1] - q[1])));
+    float dz = fmaf(p[0], Rf[2], fmaf(p[1], Rf[5], fmaf(p[2], Rf[8], tf[2] - q[2])));
+    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}'''
+BANK32F_OLD_ADD = '''        for (int c = 0; c < 3; c++) m->h[3 * r + c] += p[r] * q[c];'''
+BANK32F_NEW_ADD = '''        for (int c = 0; c < 3; c++) m->h[3 * r + c] = fmaf(p[r], q[c], m->h[3 * r + c]);'''
+BANK32F_OLD_SCORE = '''    float Rf[9], tf[3], d0sq = (float)dmax(d0 * d0, 1e-12), sd8sq = (float)(sd8 * sd8), sum = 0.f, comp = 0.f;'''
+BANK32F_NEW_SCORE = '''    float Rf[9], tf[3], inv = (float)(1.0 / dmax(d0 * d0, 1e-12)), sd8sq = (float)(sd8 * sd8), sum = 0.f,
+          comp = 0.f;'''
+BANK32F_OLD_TERM = '''            float y = 1.0f / (1.0f + d2 / d0sq) - comp, s2 = sum + y;'''
+BANK32F_NEW_TERM = '''            float y = 1.0f / fmaf(d2, inv, 1.0f) - comp, s2 = sum + y;'''
+
+
+def _bank32f(src: str) -> str:
+    """bank32 with the seed-bank kernel's explicit FP32 operation sequence:
+    fused transform ((t - q) + p_z R + p_y R + p_x R), fused d2 and moment
+    products, and the item score's term 1 / fma(d2, 1/d0^2, 1)."""
+    s = _bank32(src)
+    s = _sub(s, BANK32F_OLD_D2, BANK32F_NEW_D2)
+    s = _sub(s, BANK32F_OLD_ADD, BANK32F_NEW_ADD)
+    s = _sub(s, BANK32F_OLD_SCORE, BANK32F_NEW_SCORE)
+    return _sub(s, BANK32F_OLD_TERM, BANK32F_NEW_TERM)
+
+
 def _bank32(src: str) -> str:
     """Only the seed banks lowered, in the GPU seed-bank kernel's form."""
     marker = "/* ---- seeds (indialign_c/seeds.h)"
@@ -536,6 +571,7 @@ def variant_sources(src: str) -> dict[str, str]:
         out[name] = f"#define OFFSET_MEAN {mean}\n" + s
     out["bank32"] = _bank32(src)
     out["qcp64"] = _qcp64(src)
+    out["bank32f"] = _bank32f(src)
     out["smat32"] = _smat32(src)
     out["dp32"] = _dp32(src)
     return out
