@@ -324,6 +324,28 @@ int indialign_selftest_rcp(int n, const double *x, double *y);
  * the counterpart of the reference's cov_to_rotation (indialign_c/core.h:64-90). */
 int indialign_selftest_rotation(int n, const double *H, double *R);
 
+/* ---- length buckets and kernel shapes (no counterpart in the reference,
+ * whose only shape choice is the block size of its GPU seed-bank kernel by
+ * N, indialign_c/gpu_kernels.cu:227-229).  Every pair's work runs with the
+ * kernel shapes of its length bucket; with split = 1 a batch whose pairs
+ * span buckets runs as one sub-batch per bucket, side by side on the device.
+ * Results are those of one call either way.  The table comes from
+ * tune_b200.txt beside the library (or the file named by
+ * INDIALIGN_TUNE_TABLE), written by indialign_b200/autotune.py.
+ * Rows: {max_len, bank_chunk (items per CTA chunk, multiple of 32, 32..4096),
+ * bank_cutoff_major (0/1: item order), chain_chunk (NW chains per CTA chunk,
+ * 1..256), chain_smem_trace (0/1: NW traces in shared memory when they fit
+ * without losing occupancy)}, max_len ascending (the last bucket takes every
+ * longer pair). */
+#define INDIALIGN_TUNE_BUCKETS 3
+#define INDIALIGN_TUNE_FIELDS 5
+/* The table in use: split (0/1), min_pairs (batches with fewer pairs are not
+ * split), rows [INDIALIGN_TUNE_BUCKETS][INDIALIGN_TUNE_FIELDS]. */
+int indialign_get_tuning(int *split, int *min_pairs, int *table);
+/* Replace the table for this process (table NULL: reload it from its file);
+ * INDIALIGN_E_INPUT on an invalid row. */
+int indialign_set_tuning(int split, int min_pairs, const int *table);
+
 /* Text of the last error on this thread ("" if none). */
 const char *indialign_last_error(void);
 

@@ -109,6 +109,10 @@ def load(path: str | None = None) -> ctypes.CDLL:
     lib.indialign_fp32_peak.restype = ctypes.c_int
     lib.indialign_candidate_count.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
     lib.indialign_candidate_count.restype = ctypes.c_int
+    lib.indialign_get_tuning.argtypes = [ctypes.POINTER(ctypes.c_int)] * 3
+    lib.indialign_get_tuning.restype = ctypes.c_int
+    lib.indialign_set_tuning.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.indialign_set_tuning.restype = ctypes.c_int
     lib.indialign_pair_costs.argtypes = [ctypes.c_int, ctypes.POINTER(NativePairInput),
                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
     lib.indialign_pair_costs.restype = ctypes.c_int
@@ -319,6 +323,45 @@ def search_tensors(pred, native, valid=None, pred_valid=None, native_valid=None,
     if rc != 0:
         raise IndialignError(f"indialign_tmscore_search_padded rc={rc}: {last_error()}")
     return out[:, 0], out[:, 1:10], out[:, 10:13]
+
+
+TUNE_BUCKETS = 3
+TUNE_FIELDS = ("max_len", "bank_chunk", "bank_cutoff_major", "chain_chunk", "chain_smem_trace")
+
+
+def get_tuning() -> dict:
+    """The kernel-shape table in use: {"split", "min_pairs", "rows": [dict per
+    length bucket]} (indialign_get_tuning)."""
+    lib = load()
+    split, mp = ctypes.c_int(), ctypes.c_int()
+    t = (ctypes.c_int * (TUNE_BUCKETS * len(TUNE_FIELDS)))()
+    lib.indialign_get_tuning(ctypes.byref(split), ctypes.byref(mp), t)
+    rows = [dict(zip(TUNE_FIELDS, t[b * len(TUNE_FIELDS):(b + 1) * len(TUNE_FIELDS)])) for b in range(TUNE_BUCKETS)]
+    return {"split": split.value, "min_pairs": mp.value, "rows": rows}
+
+
+def set_tuning(table: dict | None) -> None:
+    """Replace the kernel-shape table for this process (None: reload it from
+    its file), in get_tuning()'s form."""
+    lib = load()
+    if table is None:
+        rc = lib.indialign_set_tuning(0, 0, None)
+    else:
+        flat = (ctypes.c_int * (TUNE_BUCKETS * len(TUNE_FIELDS)))(
+            *[int(r[f]) for r in table["rows"] for f in TUNE_FIELDS])
+        rc = lib.indialign_set_tuning(int(table["split"]), int(table["min_pairs"]), flat)
+    if rc != 0:
+        raise IndialignError(f"indialign_set_tuning rc={rc}: {last_error()}")
+
+
+def write_tuning(table: dict, path: str, header: str = "") -> None:
+    """Write a table in the library's file format (tune_b200.txt)."""
+    with open(path, "w") as f:
+        for line in header.splitlines():
+            f.write(f"# {line}\n")
+        f.write(f"split {int(table['split'])}\nmin_pairs {int(table['min_pairs'])}\n")
+        for b, r in enumerate(table["rows"]):
+            f.write(f"bucket {b} " + " ".join(f"{k} {int(r[k])}" for k in TUNE_FIELDS) + "\n")
 
 
 def pair_costs(pairs: Sequence) -> tuple[np.ndarray, np.ndarray]:

@@ -26,17 +26,9 @@
 #include "kernels.h"
 #include "sched.cuh"
 
-// build-time knobs: minimum resident bank CTAs per SM (caps registers), and
-// the order in which a task's items are handed to the lanes: cutoff major
-// (a warp refines 32 seeds at one cutoff) measured 1.38x faster than seed
-// major on the learned16384 step, because a warp iterates until its slowest
-// item converges and the iteration counts of one cutoff are far more alike
-// than those of one seed's cutoffs
+// build-time knob: minimum resident bank CTAs per SM (caps registers)
 #ifndef IA_BANK_MINB
 #define IA_BANK_MINB 4
-#endif
-#ifndef IA_BANK_CUTOFF_MAJOR
-#define IA_BANK_CUTOFF_MAJOR 1
 #endif
 
 namespace ia {
@@ -208,7 +200,7 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
                     if (chunk_begin[mid] <= c) lo = mid + 1; else hi = mid;
                 }
                 t = lo - 1;
-                s_next = (c - chunk_begin[t]) * kBankChunkItems;
+                s_next = (c - chunk_begin[t]) * tasks[t].chunk;
             }
             ctl.chunk = c;
             ctl.task = t;
@@ -251,8 +243,8 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         // the chunk's items [cb, ce) go to the warps 32 at a time, so a warp
         // whose items converged early takes the next group instead of
         // waiting at the chunk's barrier for the others
-        const int cb = (c - chunk_begin[ti]) * kBankChunkItems;
-        const int ce = min(cb + kBankChunkItems, T.n_items);
+        const int cb = (c - chunk_begin[ti]) * T.chunk;
+        const int ce = min(cb + T.chunk, T.n_items);
         const int lane = threadIdx.x & 31;
         for (;;) {
         int gi = 0;
@@ -264,10 +256,13 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
         const int C = T.C > 0 ? T.C : 1;
         // item (seed k, cutoff ci) and its record slot li = k*C + ci: seed
         // major (the slot order), or cutoff major (a warp refines one cutoff
-        // over 32 seeds)
+        // over 32 seeds; measured 1.38x faster than seed major on the
+        // learned16384 step, because a warp iterates until its slowest item
+        // converges and the iteration counts of one cutoff are far more alike
+        // than those of one seed's cutoffs)
         int sk = 0, ci = 0;
         if (active) {
-            if (IA_BANK_CUTOFF_MAJOR) {
+            if (T.cutoff_major) {
                 const int K = T.n_items / C;
                 sk = pi % K;
                 ci = pi / K;

@@ -467,9 +467,10 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
     __shared__ double s_rt[kChainWarps][24];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // shared layout: [native points as float4][pred labels][native labels]
-    // (flag 1), then per warp the NW boundary row (flag 2) and the alignment
-    // (flag 4); the FP64 point sets are read from global memory (L1)
-    const bool coord_smem = flags & 1, bh_smem = flags & 2, al_smem = flags & 4;
+    // (flag 1), then per warp the NW boundary row (flag 2), the alignment
+    // (flag 4) and the NW trace block (flag 8, short pairs); the FP64 point
+    // sets are read from global memory (L1)
+    const bool coord_smem = flags & 1, bh_smem = flags & 2, al_smem = flags & 4, tr_smem = flags & 8;
     const uint32_t qfbytes = (uint32_t)nmax * 16u;
     const uint32_t plb = ((uint32_t)pmax + 47u) & ~15u, nlb = ((uint32_t)nmax + 47u) & ~15u;
     char *sQf = smem;
@@ -483,7 +484,9 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
     char *albase = wbase + (bh_smem ? kChainWarps * bh_bytes : 0);
     uint32_t *al = al_smem ? reinterpret_cast<uint32_t *>(albase + warp * al_bytes)
                            : gal + (size_t)gw * min(pmax, nmax);
-    uint32_t *trace = gtrace + (size_t)gw * trace_words;
+    char *trbase = albase + (al_smem ? kChainWarps * al_bytes : 0);
+    uint32_t *trace = tr_smem ? reinterpret_cast<uint32_t *>(trbase) + (size_t)warp * trace_words
+                              : gtrace + (size_t)gw * trace_words;
     uint32_t phase = 0;
     if (threadIdx.x == 0) mbar_init(&bar);
     __syncthreads();
@@ -544,8 +547,8 @@ k_chain(DevBatch b, const ChainTask *__restrict__ tasks, const int *__restrict__
             int idx = 0;
             if (lane == 0) idx = atomicAdd(&ctl.next, 1);
             idx = __shfl_sync(kFull, idx, 0);
-            const int chain = (c - chunk_begin[ti]) * kChainChunk + idx;
-            if (idx >= kChainChunk || chain >= T.n_chains) break;
+            const int chain = (c - chunk_begin[ti]) * T.chunk + idx;
+            if (idx >= T.chunk || chain >= T.n_chains) break;
             if (lane == 0) atomicAdd(b.ctr + CTR_CHAINS, 1ull);
             const int gaps = T.gaps;
             const int si = chain / gaps, g = chain % gaps;
@@ -709,6 +712,7 @@ size_t chain_smem_bytes(int pmax, int nmax, int flags) {
     }
     if (flags & 2) s += kChainWarps * ((((size_t)nmax + 1) * 8 + 15) & ~size_t(15));
     if (flags & 4) s += kChainWarps * (((size_t)min(pmax, nmax) * 4 + 15) & ~size_t(15));
+    if (flags & 8) s += kChainWarps * nw_trace_words_for(pmax, nmax) * 4;
     return s;
 }
 

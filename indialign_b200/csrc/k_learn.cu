@@ -520,7 +520,10 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
             for (int j = i; j > 0 && list[j] < list[j - 1]; j--) {
                 const int t = list[j]; list[j] = list[j - 1]; list[j - 1] = t;
             }
-        const double u = (double)(mix64(a.seed ^ mix64((unsigned long long)p + 0x9e3779b97f4a7c15ull)) >> 11) *
+        // the draw of the pair's index in the caller's batch, so that a
+        // length bucket's sub-batch audits the same pairs as the whole batch
+        const unsigned long long gp = (unsigned long long)(b.gidx ? b.gidx[p] : p);
+        const double u = (double)(mix64(a.seed ^ mix64(gp + 0x9e3779b97f4a7c15ull)) >> 11) *
                          (1.0 / 9007199254740992.0);
         if (u < a.audit_rate) {
             a.wcount[t] = -2;
@@ -545,7 +548,11 @@ __global__ void k_select(DevBatch b, SelectArgs a) {
 // detailed-search seed the best of its cutoff items.
 IA_DEV double cand_score(const CandRes &r, int kind, int det_ss, int t, int w) {
     if (kind == CAND_DET || kind == CAND_MAIN) {  // best of the seed's cutoff items
-        const BankTask &T = r.btasks[kind == CAND_DET && det_ss ? t / kDetSlots : t];
+        // the bank launch's task of list t: a DET list is (pair, slot); the
+        // SS seeds' detailed search ran one task per pair, dp_refine's (also
+        // inside the SS stage) one per slot
+        (void)det_ss;
+        const BankTask &T = r.btasks[kind == CAND_DET && r.bank_per_pair ? t / kDetSlots : t];
         double s = -INFINITY;
         for (int ci = 0; ci < T.C; ci++)
             s = fmax(s, r.item_res[((size_t)T.item_base + (size_t)w * T.C + ci) * kRec]);

@@ -733,7 +733,8 @@ __global__ void k_repack(DevBatch b, const int *off_in, const double *pred, cons
 __global__ void k_export(DevBatch b, double *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= b.n * kRec) return;
-    out[i] = b.state[i / kRec].rec[REC_BEST][i % kRec];
+    const int p = i / kRec, row = b.out_map ? b.out_map[p] : p;
+    out[(size_t)row * kRec + i % kRec] = b.state[p].rec[REC_BEST][i % kRec];
 }
 
 void launch_repack(const DevBatch &b, const int *off_in, const double *pred, const double *nat,

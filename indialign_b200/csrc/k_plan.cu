@@ -148,8 +148,11 @@ __global__ void k_plan_bank(DevBatch b, PlanCtx c) {
         break;
     }
     T.n_items = on ? T.K * T.C : 0;
+    const Tune &tn = c.tune.of(I.N);  // the shape of the pair's length bucket
+    T.chunk = tn.bank_chunk;
+    T.cutoff_major = tn.bank_cutoff_major;
     c.btasks[s] = T;
-    c.counts[s] = (T.n_items + kBankChunkItems - 1) / kBankChunkItems;
+    c.counts[s] = (T.n_items + T.chunk - 1) / T.chunk;
 }
 
 // ---- chain plans ------------------------------------------------------------
@@ -240,8 +243,9 @@ __global__ void k_plan_chain(DevBatch b, PlanCtx c) {
     // -1e30 / identity result, which the caller then rescores
     if (on && T.n_chains == 0 && (c.kind == CH_LOCAL || c.kind == CH_THREAD || c.kind == CH_SINGLE))
         rec_ident(S.rec[REC_STAGE], kScoreInit);
+    T.chunk = c.tune.of(I.N).chain_chunk;  // the shape of the pair's length bucket
     c.ctasks[s] = T;
-    c.counts[s] = (T.n_chains + kChainChunk - 1) / kChainChunk;
+    c.counts[s] = (T.n_chains + T.chunk - 1) / T.chunk;
 }
 
 // ---- chain reductions (warp per pair) ---------------------------------------

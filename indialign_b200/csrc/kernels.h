@@ -34,6 +34,10 @@ struct DevBatch {
     const uint64_t *fnv_pow;  // [maxN+1] FNV prime powers
     int *err;              // device error word
     unsigned long long *ctr;  // [kCounters] work counters (see enum Counter)
+    const int *gidx;       // [n] index of each pair in the caller's batch (a
+                           // length bucket's sub-batch), or null: p itself
+    const int *out_map;    // [n] result row of each pair in the caller's
+                           // output (sub-batch), or null: p itself
 };
 
 // Work counters, accumulated on device per batch.
@@ -164,6 +168,8 @@ struct CandRes {
     const int *det_base;
     const double *item_res;
     const BankTask *btasks;
+    int bank_per_pair;  // detailed-search items: 1 one bank task per pair (the SS
+                        // seeds' detailed search), 0 one per alignment slot
 };
 
 void launch_plan_rank(const DevBatch &b, const RankArgs &a, int *counts, cudaStream_t st);

@@ -15,6 +15,12 @@
 #pragma once
 #include <stdint.h>
 
+#ifdef __CUDACC__
+#define IA_HD_INLINE __host__ __device__ inline
+#else
+#define IA_HD_INLINE inline
+#endif
+
 namespace ia {
 
 constexpr int kMaxC = 11;          // d0 cutoffs of the main seed bank
@@ -23,12 +29,25 @@ constexpr int kMaxSeeds = 1024;    // fragment windows (<= 1+9*101) + anchors
 constexpr int kMaxBitSeeds = 32;   // anchor masks (<= 6 radii x 5) + top-k mask
 constexpr int kRec = 13;           // {score, R[9], t[3]}
 constexpr int kBankChunk = 128;    // threads of a bank CTA (4 warps x 32)
-#ifndef IA_BANK_CHUNK_ITEMS
-#define IA_BANK_CHUNK_ITEMS 256
-#endif
-constexpr int kBankChunkItems = IA_BANK_CHUNK_ITEMS;  // bank items per CTA chunk
+// Kernel shape knobs of one length bucket (tuning table, search.cu).
+struct Tune {
+    int bank_chunk = 256;       // bank items per CTA chunk (multiple of 32)
+    int bank_cutoff_major = 1;  // bank item order: 1 cutoff major, 0 seed major
+    int chain_chunk = 16;       // NW chains per CTA chunk
+    int chain_smem_trace = 1;   // NW traces in shared memory when they fit
+};
+constexpr int kTuneBuckets = 3;
+// The rows the plan kernels read: a task takes the shape of its pair's
+// length bucket (N <= max_len[0], <= max_len[1], longer).
+struct TuneRows {
+    int max_len[kTuneBuckets];
+    Tune t[kTuneBuckets];
+    IA_HD_INLINE const Tune &of(int N) const {
+        return N <= max_len[0] ? t[0] : (N <= max_len[1] ? t[1] : t[2]);
+    }
+};
 constexpr int kChainWarps = 4;     // warps per NW-chain CTA
-constexpr int kChainChunk = 16;    // chains per CTA chunk, pulled by the warps
+
 constexpr double kNegInf = -1e300; // "no candidate" marker
 constexpr double kScoreInit = -1e30;
 
@@ -95,6 +114,8 @@ struct BankTask {
     double *out;         // explicit output record (used when out_rec < 0)
     int n_items;         // K*C (0 = task inactive)
     int item_base;       // first item in the launch's item space (set by scan)
+    int chunk;           // items per CTA chunk (the pair's length bucket)
+    int cutoff_major;    // item order: 1 cutoff major, 0 seed major
 };
 
 // ---- NW chains ---------------------------------------------------------
@@ -122,6 +143,7 @@ struct ChainTask {
     double *alP, *alQ;   // EMIT: aligned coordinates (contiguous)
     int al_cap;          // capacity per EMIT start
     int n_chains;        // n_starts*gaps (0 = inactive)
+    int chunk;           // chains per CTA chunk (the pair's length bucket)
     int chain_base;      // first chain in the launch's chain space
 };
 
@@ -151,6 +173,7 @@ struct PlanCtx {
     const int *wlist;       // CH_LOCAL: per pair kMaxTopK selected windows, ascending
     int max_iter, iters;
     double early_term;
+    TuneRows tune;          // kernel shapes per length bucket
 };
 
 struct GlueArgs {

@@ -5,7 +5,9 @@
 // whole batch.  All arithmetic runs in the kernels; the host only packs,
 // plans capacities once per batch and launches.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -13,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/indialign_b200.h"
@@ -39,7 +42,10 @@ void set_last_error_text(const char *msg) { g_last_error = msg; }
         }                                     \
     } while (0)
 
-// Grow-only device buffer with 64 bytes of tail padding.
+// Grow-only device buffer with 64 bytes of tail padding, zeroed when it
+// grows.  The zeroing runs on the legacy default stream, which does not order
+// against the library's non-blocking streams, so it is waited for here:
+// otherwise it could land after the stream's first upload into the buffer.
 template <typename T>
 struct DBuf {
     T *p = nullptr;
@@ -53,7 +59,9 @@ struct DBuf {
         cudaError_t e = cudaMalloc(&p, want * sizeof(T) + 64);
         if (e != cudaSuccess) return e;
         cap = want;
-        return cudaMemset(p, 0, want * sizeof(T) + 64);
+        e = cudaMemset(p, 0, want * sizeof(T) + 64);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+        return e;
     }
 };
 
@@ -86,7 +94,7 @@ struct Ctx {
     DBuf<int> counts, begins, counter;
     DBuf<ScanOut> scan;
     DBuf<double> item_res, chain_res, alP, alQ, thread_rec, off_start, off_res, gbh, out, snap;
-    DBuf<int> lay_i;
+    DBuf<int> lay_i, gidx, omap;
     DBuf<long long> lay_l;
     DBuf<unsigned long long> ctr;
     // learned window ranker
@@ -164,6 +172,8 @@ struct Cfg {
         min_len = INDIALIGN_RANK_MIN_LEN;
     double margin = 0.02, audit = 0.02;
     unsigned long long seed = 0;
+    TuneRows tune;              // kernel shapes per length bucket (per task)
+    int chain_smem_trace = 1;  // NW traces in shared memory (the longest pair's bucket)
 };
 
 // Host view of per-pair facts after k_prep / k_anchor.
@@ -433,6 +443,20 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
                                                      smem));
     if (per_sm < 1) per_sm = 1;
     trace_words_ = nw_trace_words_for(pmax, nmax);  // NW trace block per warp (k_chain.cu)
+    // short pairs: the warps' traces in shared memory, when that keeps the
+    // number of resident CTAs
+    if (cfg_.chain_smem_trace) {
+        const size_t with = chain_smem_bytes(pmax, nmax, chain_flags_ | 8);
+        int per_sm8 = 0;
+        if (with <= kChainSmemMax &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm8, chain_kernel_ptr(), 32 * kChainWarps,
+                                                          with) == cudaSuccess &&
+            per_sm8 >= per_sm) {
+            chain_flags_ |= 8;
+            smem = with;
+        }
+        cudaGetLastError();
+    }
     long long warps = (long long)c_->sms * per_sm * kChainWarps;
     const size_t budget = (size_t)4 << 30;  // trace scratch budget
     long long cap = (long long)(budget / (trace_words_ * 4 + 1));
@@ -440,7 +464,7 @@ int Runner::build_layouts(const std::vector<PairInfo> &info) {
     chain_grid_ = (int)(warps / kChainWarps);
     if (chain_grid_ < 1) chain_grid_ = 1;
     size_t nw = (size_t)chain_grid_ * kChainWarps;
-    CK(c_->gtrace.ensure(nw * trace_words_));
+    CK(c_->gtrace.ensure((chain_flags_ & 8) ? 1 : nw * trace_words_));
     CK(c_->gbh.ensure((chain_flags_ & 2) ? 1 : nw * (nmax + 1)));
     CK(c_->gal.ensure((chain_flags_ & 4) ? 1 : nw * (pmax < nmax ? pmax : nmax)));
     CK(c_->alP.ensure(3 * 2 * (size_t)(c_->h_off.empty() ? 1 : c_->h_off.back() + 2)));
@@ -480,6 +504,7 @@ int Runner::bank(int kind, Layout &L, double *recs, int set_iter, double early, 
     pc.early_term = early >= 0 ? early : cfg_.early;
     pc.wcount = wcount;
     pc.wlist = wlist;
+    pc.tune = cfg_.tune;
     launch_plan_bank(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
     launches_ += 4;
@@ -526,6 +551,7 @@ int Runner::chain(int kind, Layout &L, int iters, double *recs, double *recs2, b
     pc.iters = iters;
     pc.wcount = wcount;
     pc.wlist = wlist;
+    pc.tune = cfg_.tune;
     launch_plan_chain(b, pc, c_->stream);
     launch_scan(c_->counts.p, c_->begins.p, L.ntasks, c_->scan.p, c_->counter.p, c_->stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -563,8 +589,10 @@ int Runner::glue(int op, double thr, const double *recs, const int *idx) {
 }
 
 // Where a detailed search's seed items are: the bank's items and tasks.
-static CandRes det_res(Ctx *c) {
-    return CandRes{nullptr, nullptr, nullptr, nullptr, c->item_res.p, c->btasks.p};
+// Item records of the bank launch just run; per_pair: its tasks are one per
+// pair (the SS seeds' detailed search) rather than one per alignment slot.
+static CandRes det_res(Ctx *c, int per_pair = 0) {
+    return CandRes{nullptr, nullptr, nullptr, nullptr, c->item_res.p, c->btasks.p, per_pair};
 }
 
 // dp_refine with fragment detailed searches (indialign_c/align.h:54-145,
@@ -695,7 +723,7 @@ int Runner::run_stages() {
     RUN(chain(CH_SS2, L_pair, 1, nullptr, nullptr, false));
     RUN(rank_stage(CAND_DET, 1));
     RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(CAND_DET, 1), sel_list(CAND_DET, 1)));
-    RUN(after_stage(CAND_DET, det_res(c_), 1));
+    RUN(after_stage(CAND_DET, det_res(c_, 1), 1));
     RUN(glue(G_SS_DET));
     RUN(dp_full(1));
     RUN(glue(G_SS_DP));
@@ -703,7 +731,7 @@ int Runner::run_stages() {
     RUN(chain(CH_SS4, L_pair, 1, nullptr, nullptr, false));
     RUN(rank_stage(CAND_DET, 1));
     RUN(bank(BK_DET_SS, L_detss, nullptr, -1, -1, sel_count(CAND_DET, 1), sel_list(CAND_DET, 1)));
-    RUN(after_stage(CAND_DET, det_res(c_), 1));
+    RUN(after_stage(CAND_DET, det_res(c_, 1), 1));
     RUN(glue(G_SS_DET));
     RUN(dp_full(1));
     RUN(glue(G_SS_DP));
@@ -820,6 +848,10 @@ struct Source {
     const double *pred = nullptr, *nat = nullptr, *lnorm = nullptr;
     const uint8_t *v = nullptr, *pv = nullptr, *nv = nullptr;
     const int *lens = nullptr;  // optional lengths (padded rows: off[p] = p * N)
+    // a length bucket's sub-batch (host arrays, or null): each pair's index
+    // in the caller's batch, and its row in the caller's outputs
+    const int *gidx = nullptr, *out_map = nullptr;
+    cudaEvent_t wait_ev = nullptr;  // work on the caller's stream to wait for
     int n() const { return host.empty() ? n_dev : (int)host.size(); }
     int len(int p) const {
         return host.empty() ? (lens ? lens[p] : off[p + 1] - off[p]) : host[p]->length;
@@ -839,6 +871,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         ~Restore() { c->stream = s; }
     } restore{c, own};
     cudaStream_t st = c->stream;
+    if (src.wait_ev) CK(cudaStreamWaitEvent(st, src.wait_ev, 0));
     // ---- pack (pair blocks padded to an even residue count) ----
     c->h_off.resize(n + 1);
     c->h_len.resize(n);
@@ -959,6 +992,18 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
     b.fnv_pow = c->fnv_pow.p;
     b.err = c->err.p;
     b.ctr = c->ctr.p;
+    b.gidx = nullptr;
+    b.out_map = nullptr;
+    if (src.gidx) {
+        CK(c->gidx.ensure(n));
+        CK(cudaMemcpyAsync(c->gidx.p, src.gidx, n * sizeof(int), cudaMemcpyHostToDevice, st));
+        b.gidx = c->gidx.p;
+    }
+    if (src.out_map && d_out) {
+        CK(c->omap.ensure(n));
+        CK(cudaMemcpyAsync(c->omap.p, src.out_map, n * sizeof(int), cudaMemcpyHostToDevice, st));
+        b.out_map = c->omap.p;
+    }
     if (!on_host) {
         // caller's offsets to the device (scratch doubles as staging), repack
         CK(cudaMemcpyAsync(c->scratch.p, src.off, (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -1078,8 +1123,17 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
             CK(cudaMemcpy(opts->win_label, c->wlabel.p, (size_t)r.windows() * sizeof(float),
                           cudaMemcpyDeviceToHost));
     }
-    if (opts && opts->stage_best && r.snap)
-        CK(cudaMemcpy(opts->stage_best, r.snap, (size_t)n * kTrace * kRec * 8, cudaMemcpyDeviceToHost));
+    if (opts && opts->stage_best && r.snap) {
+        if (src.out_map) {  // a sub-batch: rows to the caller's pair order
+            std::vector<double> tmp((size_t)n * kTrace * kRec);
+            CK(cudaMemcpy(tmp.data(), r.snap, tmp.size() * 8, cudaMemcpyDeviceToHost));
+            for (int p = 0; p < n; p++)
+                std::memcpy(opts->stage_best + (size_t)src.out_map[p] * kTrace * kRec,
+                            tmp.data() + (size_t)p * kTrace * kRec, (size_t)kTrace * kRec * 8);
+        } else {
+            CK(cudaMemcpy(opts->stage_best, r.snap, (size_t)n * kTrace * kRec * 8, cudaMemcpyDeviceToHost));
+        }
+    }
     if (opts && opts->counters) {
         unsigned long long h[kCounters];
         CK(cudaMemcpy(h, c->ctr.p, sizeof(h), cudaMemcpyDeviceToHost));
@@ -1134,7 +1188,250 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         CK(cudaStreamSynchronize(st));
     } else {
         for (int p = 0; p < n; p++)
-            std::memcpy(results + 13 * (size_t)p, state[p].rec[REC_BEST], 13 * 8);
+            std::memcpy(results + 13 * (size_t)(src.out_map ? src.out_map[p] : p), state[p].rec[REC_BEST], 13 * 8);
+    }
+    return INDIALIGN_OK;
+}
+
+// ---- length buckets ---------------------------------------------------------
+// The tuning table holds one row of kernel shapes per length bucket (N <=
+// 128, <= 512, longer): bank items per CTA chunk and their order, NW chains
+// per CTA chunk, NW traces in shared memory.  Inside one launch every task
+// takes the row of its own pair's bucket (the plan kernels look it up), so a
+// batch of mixed lengths runs each pair with its bucket's shapes in the same
+// persistent kernels.  Optionally (split = 1) a batch that spans buckets runs
+// as one sub-batch per bucket instead, each on its own context and stream
+// with launches sized by its own longest pair, side by side on the device;
+// every pair's search is independent of the rest of its batch and keeps its
+// index in the caller's batch for the learned mode's audit draw, so results
+// equal those of one call.  Measured on 2048-pair calls of the learned16384
+// workload the split is slower (its sub-batches' full-size persistent grids
+// mostly run one after another, adding per-stage tails), so it is off unless
+// the tuner finds it faster.
+constexpr int kBuckets = INDIALIGN_TUNE_BUCKETS;
+static_assert(kBuckets == kTuneBuckets, "bucket count of the C ABI and the kernels");
+
+struct TuneTable {
+    int split = 0;       // split batches that span buckets into concurrent sub-batches
+    int min_pairs = 64;  // ... of at least this many pairs
+    int max_len[kBuckets] = {128, 512, 65535};
+    Tune t[kBuckets];
+    TuneRows rows() const {
+        TuneRows r;
+        for (int b = 0; b < kBuckets; b++) {
+            r.max_len[b] = max_len[b];
+            r.t[b] = t[b];
+        }
+        return r;
+    }
+};
+
+static std::mutex g_tune_mu;
+static TuneTable g_tune;
+static bool g_tune_loaded = false;
+
+static bool tune_row_ok(const int *r) {
+    return r[0] >= 1 && r[0] <= 65535 && r[1] >= 32 && r[1] <= 4096 && r[1] % 32 == 0 && (r[2] == 0 || r[2] == 1) &&
+           r[3] >= 1 && r[3] <= 256 && (r[4] == 0 || r[4] == 1);
+}
+
+// The table file: INDIALIGN_TUNE_TABLE, else tune_b200.txt beside the
+// library.  Lines "split S", "min_pairs M" and "bucket B max_len L
+// bank_chunk C bank_cutoff_major O chain_chunk H chain_smem_trace T"; '#'
+// starts a comment.  A missing or malformed file leaves the built-in rows.
+static TuneTable read_tune_file() {
+    TuneTable tt;
+    std::string path;
+    if (const char *e = std::getenv("INDIALIGN_TUNE_TABLE")) {
+        path = e;
+    } else {
+        Dl_info info;
+        if (dladdr(reinterpret_cast<void *>(&read_tune_file), &info) && info.dli_fname) {
+            path = info.dli_fname;
+            const size_t sl = path.rfind('/');
+            path = (sl == std::string::npos ? std::string(".") : path.substr(0, sl)) + "/tune_b200.txt";
+        }
+    }
+    FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "r");
+    if (!f) return tt;
+    TuneTable out = tt;
+    char line[512];
+    bool ok = true;
+    while (ok && std::fgets(line, sizeof line, f)) {
+        char *hash = std::strchr(line, '#');
+        if (hash) *hash = 0;
+        int a = 0, r[5];
+        char k0[32], k1[32], k2[32], k3[32], k4[32], k5[32];
+        if (std::sscanf(line, " split %d", &a) == 1) {
+            out.split = a != 0;
+        } else if (std::sscanf(line, " min_pairs %d", &a) == 1) {
+            out.min_pairs = a;
+        } else if (std::sscanf(line, " bucket %d %31s %d %31s %d %31s %d %31s %d %31s %d", &a, k0, &r[0], k1, &r[1],
+                               k2, &r[2], k3, &r[3], k4, &r[4]) == 11) {
+            ok = a >= 0 && a < kBuckets && !std::strcmp(k0, "max_len") && !std::strcmp(k1, "bank_chunk") &&
+                 !std::strcmp(k2, "bank_cutoff_major") && !std::strcmp(k3, "chain_chunk") &&
+                 !std::strcmp(k4, "chain_smem_trace") && tune_row_ok(r);
+            if (ok) {
+                out.max_len[a] = r[0];
+                out.t[a].bank_chunk = r[1];
+                out.t[a].bank_cutoff_major = r[2];
+                out.t[a].chain_chunk = r[3];
+                out.t[a].chain_smem_trace = r[4];
+            }
+        } else {
+            for (const char *q = line; *q; q++)
+                if (*q != ' ' && *q != '\t' && *q != '\n' && *q != '\r') ok = false;
+        }
+    }
+    std::fclose(f);
+    return ok ? out : tt;
+}
+
+static TuneTable tune_table() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (!g_tune_loaded) {
+        g_tune = read_tune_file();
+        g_tune_loaded = true;
+    }
+    return g_tune;
+}
+
+static int bucket_of(const TuneTable &tt, int N) {
+    for (int b = 0; b < kBuckets - 1; b++)
+        if (N <= tt.max_len[b]) return b;
+    return kBuckets - 1;
+}
+
+// The search of a batch from `src`: one run, or one run per length bucket
+// side by side (see above).  Results to `results` (host) or `d_out` (device).
+static int run_search(int device, const Cfg &cfg0, const Source &src, double *results, double *d_out,
+                      const IndialignBatchOptions *opts) {
+    const TuneTable tt = tune_table();
+    const int n = src.n();
+    std::vector<int> idx[kBuckets];
+    int Lmax = 0;
+    for (int p = 0; p < n; p++) {
+        const int N = src.len(p);
+        idx[bucket_of(tt, N)].push_back(p);
+        if (N > Lmax) Lmax = N;
+    }
+    int nonempty = 0;
+    for (int b = 0; b < kBuckets; b++) nonempty += !idx[b].empty();
+    // per-candidate outputs are laid out by the whole batch's pair order
+    const bool per_cand = opts && (opts->win_feat || opts->win_label || opts->win_score || opts->win_select);
+    if (!tt.split || nonempty <= 1 || per_cand || n < tt.min_pairs) {
+        Cfg cfg = cfg0;
+        cfg.tune = tt.rows();
+        cfg.chain_smem_trace = tt.t[bucket_of(tt, Lmax)].chain_smem_trace;
+        Ctx *c = nullptr;
+        int rc = acquire(device, &c);
+        if (rc) return rc;
+        rc = run_batch(c, cfg, src, results, d_out, opts);
+        release(c);
+        return rc;
+    }
+    if (device < 0) CK(cudaGetDevice(&device));
+    CK(cudaSetDevice(device));
+    // the sub-batches wait for the caller's stream, then run on their own
+    struct Ev {
+        cudaEvent_t e = nullptr;
+        ~Ev() {
+            if (e) cudaEventDestroy(e);
+        }
+    } start;
+    if (opts && opts->stream) {
+        CK(cudaEventCreateWithFlags(&start.e, cudaEventDisableTiming));
+        CK(cudaEventRecord(start.e, static_cast<cudaStream_t>(opts->stream)));
+    }
+    struct Part {
+        Source src;
+        std::vector<int> off, len;
+        std::vector<double> lnorm;
+        IndialignBatchOptions o;
+        double stage_ms[INDIALIGN_STAGES] = {0}, kernel_ms[6] = {0};
+        long long counters[INDIALIGN_COUNTERS] = {0}, rank_stats[INDIALIGN_RANK_STATS] = {0};
+        Cfg cfg;
+        int rc = 0;
+        std::string err;
+    };
+    std::vector<Part> parts(kBuckets);
+    for (int b = 0; b < kBuckets; b++) {
+        Part &P = parts[b];
+        const std::vector<int> &I = idx[b];
+        if (I.empty()) continue;
+        P.cfg = cfg0;
+        P.cfg.tune = tt.rows();
+        P.cfg.chain_smem_trace = tt.t[b].chain_smem_trace;
+        if (!src.host.empty()) {
+            for (int p : I) P.src.host.push_back(src.host[p]);
+        } else {
+            P.off.resize(I.size() + 1);
+            P.len.resize(I.size());
+            P.lnorm.resize(I.size());
+            for (size_t k = 0; k < I.size(); k++) {
+                P.off[k] = src.off[I[k]];
+                P.len[k] = src.len(I[k]);
+                P.lnorm[k] = src.lnorm[I[k]];
+            }
+            P.off[I.size()] = 0;
+            P.src.n_dev = (int)I.size();
+            P.src.off = P.off.data();
+            P.src.lens = P.len.data();
+            P.src.pred = src.pred;
+            P.src.nat = src.nat;
+            P.src.v = src.v;
+            P.src.pv = src.pv;
+            P.src.nv = src.nv;
+            P.src.lnorm = P.lnorm.data();
+        }
+        P.src.gidx = I.data();
+        P.src.out_map = I.data();
+        P.src.wait_ev = start.e;
+        std::memset(&P.o, 0, sizeof P.o);
+        if (opts) P.o = *opts;
+        P.o.device = device;
+        P.o.stream = nullptr;
+        P.o.stage_ms = opts && opts->stage_ms ? P.stage_ms : nullptr;
+        P.o.kernel_ms = opts && opts->kernel_ms ? P.kernel_ms : nullptr;
+        P.o.counters = opts && opts->counters ? P.counters : nullptr;
+        P.o.rank_stats = opts && opts->rank_stats ? P.rank_stats : nullptr;
+    }
+    std::vector<std::thread> th;
+    for (int b = 0; b < kBuckets; b++) {
+        if (idx[b].empty()) continue;
+        th.emplace_back([&parts, b, device, results, d_out]() {
+            Part &P = parts[b];
+            Ctx *c = nullptr;
+            P.rc = acquire(device, &c);
+            if (!P.rc) {
+                P.rc = run_batch(c, P.cfg, P.src, results, d_out, &P.o);
+                release(c);
+            }
+            if (P.rc) P.err = g_last_error;
+        });
+    }
+    for (auto &t : th) t.join();
+    for (int b = 0; b < kBuckets; b++)
+        if (parts[b].rc) {
+            g_last_error = "length bucket " + std::to_string(b) + ": " + parts[b].err;
+            return parts[b].rc;
+        }
+    bool first = true;
+    for (int b = 0; b < kBuckets; b++) {
+        if (idx[b].empty()) continue;
+        const Part &P = parts[b];
+        if (opts && opts->stage_ms)  // the sub-batches run side by side: the slowest
+            for (int k = 0; k < INDIALIGN_STAGES; k++)
+                opts->stage_ms[k] = first ? P.stage_ms[k] : std::max(opts->stage_ms[k], P.stage_ms[k]);
+        if (opts && opts->kernel_ms)
+            for (int k = 0; k < 6; k++) opts->kernel_ms[k] = (first ? 0.0 : opts->kernel_ms[k]) + P.kernel_ms[k];
+        if (opts && opts->counters)
+            for (int k = 0; k < INDIALIGN_COUNTERS; k++)
+                opts->counters[k] = (first ? 0 : opts->counters[k]) + P.counters[k];
+        if (opts && opts->rank_stats)
+            for (int k = 0; k < INDIALIGN_RANK_STATS; k++)
+                opts->rank_stats[k] = (first ? 0 : opts->rank_stats[k]) + P.rank_stats[k];
+        first = false;
     }
     return INDIALIGN_OK;
 }
@@ -1218,12 +1515,8 @@ static int search_host(int n_pairs, const NativePairInput *inputs, const NativeC
         g_last_error = "no CUDA device";
         return INDIALIGN_E_NODEVICE;
     }
-    Ctx *c = nullptr;
-    int rc = acquire(opts ? opts->device : -1, &c);
-    if (rc) return rc;
     std::vector<double> res(13 * in.size());
-    rc = run_batch(c, make_cfg(cfg, opts), src, res.data(), nullptr, opts);
-    release(c);
+    int rc = run_search(opts ? opts->device : -1, make_cfg(cfg, opts), src, res.data(), nullptr, opts);
     if (rc) return rc;
     for (size_t k = 0; k < ids.size(); k++) {
         NativePairResult *o = &outputs[ids[k]];
@@ -1344,12 +1637,7 @@ int indialign_tmscore_search_device(int n_pairs, const int *off, const double *d
     src.pv = d_pv;
     src.nv = d_nv;
     src.lnorm = lnorm;
-    ia::Ctx *c = nullptr;
-    int rc = ia::acquire(opts ? opts->device : -1, &c);
-    if (rc) return rc;
-    rc = ia::run_batch(c, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
-    ia::release(c);
-    return rc;
+    return ia::run_search(opts ? opts->device : -1, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
 }
 
 int indialign_candidate_count(int plen, int nlen, int kind) {
@@ -1397,12 +1685,51 @@ int indialign_tmscore_search_padded(int n_pairs, int N, const int *lengths, cons
     src.pv = d_pv;
     src.nv = d_nv;
     src.lnorm = lnorm;
-    ia::Ctx *c = nullptr;
-    int rc = ia::acquire(opts ? opts->device : -1, &c);
-    if (rc) return rc;
-    rc = ia::run_batch(c, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
-    ia::release(c);
-    return rc;
+    return ia::run_search(opts ? opts->device : -1, ia::make_cfg(cfg, opts), src, nullptr, d_out, opts);
+}
+
+int indialign_get_tuning(int *split, int *min_pairs, int *table) {
+    const ia::TuneTable tt = ia::tune_table();
+    if (split) *split = tt.split;
+    if (min_pairs) *min_pairs = tt.min_pairs;
+    if (table)
+        for (int b = 0; b < ia::kBuckets; b++) {
+            int *r = table + b * INDIALIGN_TUNE_FIELDS;
+            r[0] = tt.max_len[b];
+            r[1] = tt.t[b].bank_chunk;
+            r[2] = tt.t[b].bank_cutoff_major;
+            r[3] = tt.t[b].chain_chunk;
+            r[4] = tt.t[b].chain_smem_trace;
+        }
+    return INDIALIGN_OK;
+}
+
+int indialign_set_tuning(int split, int min_pairs, const int *table) {
+    ia::TuneTable tt;
+    if (!table) {
+        tt = ia::read_tune_file();
+    } else {
+        tt.split = split != 0;
+        tt.min_pairs = min_pairs;
+        int prev = 0;
+        for (int b = 0; b < ia::kBuckets; b++) {
+            const int *r = table + b * INDIALIGN_TUNE_FIELDS;
+            if (!ia::tune_row_ok(r) || r[0] <= prev) {
+                ia::g_last_error = "set_tuning: invalid row " + std::to_string(b);
+                return INDIALIGN_E_INPUT;
+            }
+            prev = r[0];
+            tt.max_len[b] = r[0];
+            tt.t[b].bank_chunk = r[1];
+            tt.t[b].bank_cutoff_major = r[2];
+            tt.t[b].chain_chunk = r[3];
+            tt.t[b].chain_smem_trace = r[4];
+        }
+    }
+    std::lock_guard<std::mutex> lk(ia::g_tune_mu);
+    ia::g_tune = tt;
+    ia::g_tune_loaded = true;
+    return INDIALIGN_OK;
 }
 
 const char *indialign_last_error(void) { return ia::g_last_error.c_str(); }
