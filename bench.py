@@ -20,11 +20,11 @@ batches).
            buffers: host->device copies of the inputs and the device->host
            read of the results inside the timed region.
   roofline the dominant kernel of the learned step (by summed device time):
-           algorithmic flops / its device time against the GPU's measured FMA
-           peak of the precision the kernel's work runs in -- NW chains: FP64
-           (indialign_fp64_peak), 18 flop per NW cell + 55 per refine residue
-           visit; seed bank: FP32 (indialign_fp32_peak), 55 per residue
-           visit.
+           algorithmic flops / its device time against the GPU's measured FP32
+           FMA peak (indialign_fp32_peak) -- seed bank: 55 FP32 flop per
+           residue visit; NW chains: 18 FP32 flop per NW cell + 55 FP64 flop
+           per Kabsch / detailed-search residue visit, the FP64 flops counted
+           twice (the FP64 rate is half the FP32 rate).
   cpu_baseline  the reference's own build (oracle/_ref, OpenMP batch entry)
            on this host's cores: one batch call over a length-stratified
            sample of the timed pairs, two pairs per host thread.
@@ -62,6 +62,12 @@ METRIC = "pairs/sec on 1 B200, learned-seed vs plain GPU search at mean ΔTM ≥
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libindialign_ref.so")
 FLOP_PER_CELL = 18.0
 FLOP_PER_VISIT = 55.0
+# DRAM bytes (read + write) of the seed-bank kernel per residue visit, from
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the first
+# three k_bank launches of a 192-pair learned16384 call, divided by their
+# residue visits; the kernel's traffic is its item records and staged point
+# sets, which grow in proportion to the visits.  None: not measured.
+BANK_DRAM_BYTES_PER_VISIT = None
 STAGES = ["seeds", "seed_bank", "ss", "gapless", "local_fragment", "threading_dp",
           "dense_local_fragment", "topk", "dp_refine", "offset_dp", "weighted", "total"]
 
@@ -336,6 +342,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-split", action="store_true",
+                    help="run every call as one batch (the kernel-shape table's split flag off), e.g. so that "
+                         "a profiler's launch numbering follows one search's stage order")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -356,6 +365,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     lib = ia.load()
+    if args.no_split:
+        ia.set_tuning(dict(ia.get_tuning(), split=0))
     cfg = ia.default_config()
     blob = (np.ascontiguousarray(np.load(args.weights), np.float32) if args.weights
             else ranker.default_weights())
@@ -478,18 +489,20 @@ def main():
         kern = np.mean(lrn["kern"], 0)
         ctr = np.mean(lrn["ctr"], 0)
         step_ms = l_ms / args.steps
+        bound, peak, src = "fp32", ia.fp32_peak_tflops(local), "measured FP32 FMA rate (indialign_fp32_peak)"
         if kern[0] >= kern[1]:
-            flops = FLOP_PER_CELL * ctr[0] + FLOP_PER_VISIT * ctr[1]
+            flops = FLOP_PER_CELL * ctr[0] + 2.0 * FLOP_PER_VISIT * ctr[1]  # FP64 visits at half rate
             kname, kms = "k_chain (NW chains: score matrix + NW + Kabsch + refine)", kern[0]
-            bound, peak, src = "fp64", ia.fp64_peak_tflops(local), "measured FP64 FMA rate (indialign_fp64_peak)"
+            traffic = None
         else:
             flops = FLOP_PER_VISIT * ctr[2]
             kname, kms = "k_bank (seed x cutoff refine items)", kern[1]
-            bound, peak, src = "fp32", ia.fp32_peak_tflops(local), "measured FP32 FMA rate (indialign_fp32_peak)"
+            traffic = BANK_DRAM_BYTES_PER_VISIT * ctr[2] if BANK_DRAM_BYTES_PER_VISIT else None
         achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else None
         cyc = ctr[8:12]
         roofline = {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak if achieved else None, "traffic": None,
+                    "frac": achieved / peak if achieved else None, "traffic": traffic,
+                    "traffic_unit": "bytes per step (DRAM read + write of the kernel's launches)",
                     "peak_source": f"{src} in this run",
                     "kernel_ms_per_step": float(kms), "kernel_share": float(kms / step_ms),
                     "kernel_ms": {"k_chain": float(kern[0]), "k_bank": float(kern[1]), "k_rank": float(kern[4])},

@@ -77,6 +77,7 @@ struct Layout {
 
 struct Ctx {
     int device = 0;
+    int tag = 0;  // the kind of batch it last served (length bucket + 1, 0: whole batches)
     cudaStream_t stream = nullptr;
     int sms = 148;
     DBuf<int> off, len, bitoff, err;
@@ -113,21 +114,30 @@ static std::mutex g_pool_mu;
 static std::vector<Ctx *> g_pool;
 static std::once_flag g_attr_once[64];
 
-static int acquire(int device, Ctx **out) {
+// A pooled context of `device`, preferring one that last served the same
+// kind of batch (`tag`), so that its grow-only buffers already fit.
+static int acquire(int device, Ctx **out, int tag = 0) {
     if (device < 0) CK(cudaGetDevice(&device));
     {
         std::lock_guard<std::mutex> lk(g_pool_mu);
+        long pick = -1;
         for (size_t i = 0; i < g_pool.size(); i++)
-            if (g_pool[i]->device == device) {
-                *out = g_pool[i];
-                g_pool.erase(g_pool.begin() + (long)i);
-                CK(cudaSetDevice(device));
-                return INDIALIGN_OK;
+            if (g_pool[i]->device == device && (pick < 0 || g_pool[i]->tag == tag)) {
+                pick = (long)i;
+                if (g_pool[i]->tag == tag) break;
             }
+        if (pick >= 0) {
+            *out = g_pool[pick];
+            (*out)->tag = tag;
+            g_pool.erase(g_pool.begin() + pick);
+            CK(cudaSetDevice(device));
+            return INDIALIGN_OK;
+        }
     }
     CK(cudaSetDevice(device));
     Ctx *c = new Ctx();
     c->device = device;
+    c->tag = tag;
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     cudaError_t attr_err = cudaSuccess;
@@ -1402,7 +1412,7 @@ static int run_search(int device, const Cfg &cfg0, const Source &src, double *re
         th.emplace_back([&parts, b, device, results, d_out]() {
             Part &P = parts[b];
             Ctx *c = nullptr;
-            P.rc = acquire(device, &c);
+            P.rc = acquire(device, &c, b + 1);
             if (!P.rc) {
                 P.rc = run_batch(c, P.cfg, P.src, results, d_out, &P.o);
                 release(c);
