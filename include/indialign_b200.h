@@ -131,10 +131,12 @@ typedef struct {
     double audit_rate;       /* LEARNED: fraction of pairs refined on all candidates */
     unsigned long long seed; /* LEARNED: audit draw */
     long long *rank_stats;   /* LEARNED: optional [INDIALIGN_RANK_STATS] out, per kind
-                                8 counts summed over the batch's searches: lists
+                                10 counts summed over the batch's searches: lists
                                 ranked, margin fallbacks, audits, pruned lists,
-                                candidates, candidates refined, audit misses, lists
-                                with at most top_k candidates */
+                                candidates, candidates refined, audit misses (the
+                                top_k's best refined score below the list's best),
+                                lists with at most top_k candidates, audit misses by
+                                more than 1e-4, by more than 1e-3 */
     float *win_feat;         /* COLLECT: out [candidates][16] raw features */
     float *win_label;        /* COLLECT: out [candidates] refined score, NaN where
                                 the pair's pass did not run */
@@ -180,7 +182,7 @@ typedef struct {
  * workload: the worst TM-score changes were pairs of L < 50) */
 #define INDIALIGN_RANK_MIN_LEN 100
 #define INDIALIGN_RANKER_FLOATS 18849
-#define INDIALIGN_RANK_STATS 40
+#define INDIALIGN_RANK_STATS 50
 
 /* Stages recorded in stage_best, in search order: seed bank, SS seeds,
  * gapless threading, local fragment DP, threading DP, dense local fragment
@@ -302,6 +304,16 @@ size_t indialign_mlp_work_bytes(int n);
  * from the forward on the same rows; d_work of indialign_mlp_work_bytes(n). */
 int indialign_mlp_backward(const void *d_packed, const float *d_dy, int n, const void *d_save,
                            float *d_grad, void *d_work, void *stream);
+/* C[m][n] = A . B^T on the tcgen05 tensor cores (BF16 in, FP32 out), the
+ * product the backward's three weight/activation gradients use.  A is K-major
+ * ([m][lda] row-major, a_mn = 0) or MN-major ([k][lda], a_mn = 1, m <= 128);
+ * B is K-major ([n][ldb]) or MN-major ([k][ldb]), n <= 256; lda, ldb multiples
+ * of 8 elements, 16-byte aligned device pointers.  C has row stride ldc, or is
+ * written transposed (C[j][i] at j * ldc + i) with c_trans.  splits > 1 splits
+ * k over partial tiles in d_partial (splits x m x n floats), added in a fixed
+ * order.  INDIALIGN_E_INPUT on a shape it does not take. */
+int indialign_gemm_bf16(const void *d_a, int lda, int a_mn, const void *d_b, int ldb, int b_mn, int m, int n,
+                        int k, float *d_c, int ldc, int c_trans, float *d_partial, int splits, void *stream);
 /* One Adam step (bias-corrected, step >= 1) on the trained blob entries. */
 int indialign_mlp_adam(float *d_blob, const float *d_grad, float *d_m, float *d_v, int step,
                        float lr, float beta1, float beta2, float eps, void *stream);

@@ -31,7 +31,7 @@ CAND_KINDS = 5
 RANK_LOCAL, RANK_THREAD, RANK_DENSE, RANK_DET_SS, RANK_DET_DP, RANK_MAIN = 1, 2, 4, 8, 16, 32
 CAND_NAMES = ("local", "threading", "dense", "detailed", "seed_bank")
 RANKER_FLOATS = 18849
-RANK_STATS = 40
+RANK_STATS = 50
 RANK_STAT_NAMES = ("gated", "fallback", "audit", "pruned", "windows", "refined",
                    "audit_miss", "small")
 FEATURES = 16
@@ -133,6 +133,9 @@ def load(path: str | None = None) -> ctypes.CDLL:
             ("indialign_mlp_forward", [vp, vp, ctypes.c_int, vp, vp, vp], ctypes.c_int),
             ("indialign_mlp_loss", [vp, vp, ctypes.c_int, ctypes.c_float, vp, vp, vp], ctypes.c_int),
             ("indialign_mlp_backward", [vp, vp, ctypes.c_int, vp, vp, vp, vp], ctypes.c_int),
+            ("indialign_gemm_bf16", [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int,
+                                     vp], ctypes.c_int),
             ("indialign_mlp_adam", [vp, vp, vp, vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_float, vp], ctypes.c_int)):
         f = getattr(lib, name)
@@ -171,7 +174,7 @@ def learned_options(opts: BatchOptions, ranker: np.ndarray, top_k: int = 8, marg
     opts.rank_mask = int(rank_mask)
     opts.rank_min_len = int(rank_min_len)
     if rank_stats is not None:
-        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [5][8]
+        assert rank_stats.dtype == np.int64 and rank_stats.size >= RANK_STATS  # [5][10]
         opts.rank_stats = rank_stats.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
     return opts
 

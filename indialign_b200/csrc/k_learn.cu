@@ -587,7 +587,11 @@ __global__ void k_audit(DevBatch b, SelectArgs a, CandRes r) {
         full = fmax(full, __shfl_xor_sync(kAllLanes, full, o));
         sel = fmax(sel, __shfl_xor_sync(kAllLanes, sel, o));
     }
-    if (lane == 0 && sel < full) atomicAdd(a.stats + RS_AUDIT_MISS, 1ull);
+    if (lane == 0 && sel < full) {
+        atomicAdd(a.stats + RS_AUDIT_MISS, 1ull);
+        if (sel < full - 1e-4) atomicAdd(a.stats + RS_AUDIT_MISS_1E4, 1ull);
+        if (sel < full - 1e-3) atomicAdd(a.stats + RS_AUDIT_MISS_1E3, 1ull);
+    }
 }
 
 // Training labels: every candidate's refined score for pairs that ran the
@@ -699,16 +703,19 @@ __global__ void __launch_bounds__(1024) k_mlp_loss(const float *__restrict__ y, 
     }
 }
 
-// Head backward: dz2 = dy w3 gelu'(z2) (bf16), db2 = colsum(dz2),
-// dw3 = sum_b dy gelu(z2), db3 = sum dy.  Block = 32 columns x 8 row groups.
+// Head backward over row block blockIdx.y (rows [r0, r1)): dz2 = dy w3
+// gelu'(z2) (bf16) and the block's partial sums of dz2 (db2), dy gelu(z2)
+// (dw3) and dy (db3) at red[blockIdx.y * kBwdRedStride + {0, 128, 256}].
+// Block = 32 columns x 8 row groups; grid (4, row blocks).
 __global__ void __launch_bounds__(256) k_mlp_head_bwd(const MlpPacked *mlp, const float *__restrict__ dy,
-                                                      const float *__restrict__ z2, int n, uint16_t *dz2,
-                                                      float *grad) {
+                                                      const float *__restrict__ z2, int n, int rows_per,
+                                                      uint16_t *dz2, float *red) {
     __shared__ float r_b2[8][33], r_w3[8][33];
     const int col = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * rows_per, r1 = min(n, r0 + rows_per);
     const float w3 = mlp->w3[col];
     float sb = 0.f, sw = 0.f;
-    for (int r = rg; r < n; r += 8) {
+    for (int r = r0 + rg; r < r1; r += 8) {
         const float z = z2[(size_t)r * kHidden + col], d = dy[r];
         const float dz = d * w3 * gelu_grad(z);
         dz2[(size_t)r * kHidden + col] = __bfloat16_as_ushort(__float2bfloat16_rn(dz));
@@ -718,123 +725,58 @@ __global__ void __launch_bounds__(256) k_mlp_head_bwd(const MlpPacked *mlp, cons
     r_b2[rg][threadIdx.x & 31] = sb;
     r_w3[rg][threadIdx.x & 31] = sw;
     __syncthreads();
+    float *out = red + (size_t)blockIdx.y * kBwdRedStride;
     if (rg == 0) {
         float b2 = 0.f, w = 0.f;
         for (int k = 0; k < 8; k++) {
             b2 += r_b2[k][threadIdx.x];
             w += r_w3[k][threadIdx.x];
         }
-        grad[kBlobB2 + col] = b2;
-        grad[kBlobW3 + col] = w;
+        out[col] = b2;
+        out[kHidden + col] = w;
     }
     if (blockIdx.x == 0 && rg == 1) {
-        float s = 0.f;
-        for (int r = threadIdx.x & 31; r < n; r += 32) s += dy[r];
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(kAllLanes, s, o);
-        if ((threadIdx.x & 31) == 0) grad[kBlobB3] = s;
+        float t = 0.f;
+        for (int r = r0 + (threadIdx.x & 31); r < r1; r += 32) t += dy[r];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kAllLanes, t, o);
+        if ((threadIdx.x & 31) == 0) out[2 * kHidden] = t;
     }
 }
 
-// dz = dh gelu'(z) (bf16) and its column sums.
+// dz = dh gelu'(z) (bf16) over row block blockIdx.y and the block's partial
+// column sums at red[blockIdx.y * kBwdRedStride].
 __global__ void __launch_bounds__(256) k_mlp_act_bwd(const float *__restrict__ dh, const float *__restrict__ z,
-                                                     int n, uint16_t *dz, float *dbias) {
-    __shared__ float red[8][33];
+                                                     int n, int rows_per, uint16_t *dz, float *red) {
+    __shared__ float r_s[8][33];
     const int col = blockIdx.x * 32 + (threadIdx.x & 31), rg = threadIdx.x >> 5;
+    const int r0 = blockIdx.y * rows_per, r1 = min(n, r0 + rows_per);
     float s = 0.f;
-    for (int r = rg; r < n; r += 8) {
+    for (int r = r0 + rg; r < r1; r += 8) {
         const size_t i = (size_t)r * kHidden + col;
         const float v = dh[i] * gelu_grad(z[i]);
         dz[i] = __bfloat16_as_ushort(__float2bfloat16_rn(v));
         s += v;
     }
-    red[rg][threadIdx.x & 31] = s;
+    r_s[rg][threadIdx.x & 31] = s;
     __syncthreads();
     if (rg == 0) {
         float t = 0.f;
-        for (int k = 0; k < 8; k++) t += red[k][threadIdx.x];
-        dbias[col] = t;
+        for (int k = 0; k < 8; k++) t += r_s[k][threadIdx.x];
+        red[(size_t)blockIdx.y * kBwdRedStride + col] = t;
     }
 }
 
-// BF16 GEMM tile kernel: 64 x 64 output tile per CTA (2 x 2 warps of 32 x 32),
-// K in steps of 32 staged through shared memory; gridDim.z splits K.
-constexpr int kGBM = 64, kGBN = 64, kGBK = 32, kGStride = kGBK + 8;
-__global__ void __launch_bounds__(128) k_gemm_bf16(const uint16_t *__restrict__ A, int ta,
-                                                   const uint16_t *__restrict__ B, int tb, int M, int N, int K,
-                                                   int kper, float *out) {
-    __shared__ __align__(16) uint16_t As[kGBM][kGStride];
-    __shared__ __align__(16) uint16_t Bs[kGBN][kGStride];
-    const int m0 = blockIdx.y * kGBM, n0 = blockIdx.x * kGBN;
-    const int kbeg = blockIdx.z * kper, kend = min(K, kbeg + kper);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32, g = lane >> 2, c = lane & 3;
-    float acc[2][4][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[i][j][e] = 0.f;
-    for (int k0 = kbeg; k0 < kend; k0 += kGBK) {
-        for (int e = tid; e < kGBM * kGBK; e += 128) {
-            int m, k;
-            if (ta) { k = e / kGBM; m = e % kGBM; } else { m = e / kGBK; k = e % kGBK; }
-            const int gm = m0 + m, gk = k0 + k;
-            uint16_t v = 0;
-            if (gm < M && gk < kend) v = ta ? A[(size_t)gk * M + gm] : A[(size_t)gm * K + gk];
-            As[m][k] = v;
-        }
-        for (int e = tid; e < kGBN * kGBK; e += 128) {
-            int nn, k;
-            if (tb) { nn = e / kGBK; k = e % kGBK; } else { k = e / kGBN; nn = e % kGBN; }
-            const int gn = n0 + nn, gk = k0 + k;
-            uint16_t v = 0;
-            if (gn < N && gk < kend) v = tb ? B[(size_t)gn * K + gk] : B[(size_t)gk * N + gn];
-            Bs[nn][k] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kGBK; kk += 16) {
-            uint32_t a[2][4];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const int r = wm + 16 * i + g;
-                a[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * c]);
-                a[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * c]);
-                a[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][kk + 2 * c + 8]);
-                a[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][kk + 2 * c + 8]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int cn = wn + 8 * j + g;
-                const uint32_t b0 = *reinterpret_cast<const uint32_t *>(&Bs[cn][kk + 2 * c]);
-                const uint32_t b1 = *reinterpret_cast<const uint32_t *>(&Bs[cn][kk + 2 * c + 8]);
-#pragma unroll
-                for (int i = 0; i < 2; i++) mma_bf16(acc[i][j], a[i], b0, b1);
-            }
-        }
-        __syncthreads();
-    }
-    float *o = out + (size_t)blockIdx.z * M * N;
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r = m0 + wm + 16 * i + g, cc = n0 + wn + 8 * j + 2 * c;
-#pragma unroll
-            for (int e = 0; e < 4; e++) {
-                const int rr = r + (e >> 1) * 8, col = cc + (e & 1);
-                if (rr < M && col < N) o[(size_t)rr * N + col] = acc[i][j][e];
-            }
-        }
-}
-
-__global__ void k_splitk_sum(const float *__restrict__ part, int splits, int mn, float *C) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= mn) return;
-    float s = 0.f;
-    for (int z = 0; z < splits; z++) s += part[(size_t)z * mn + i];
-    C[i] = s;
+// out[j] = sum over row blocks b (in order) of red[b * kBwdRedStride + j],
+// j < width, to dst[j] with dst = d0 (j < 128), d1 (j < 256), d2 (j = 256).
+__global__ void k_bwd_reduce(const float *__restrict__ red, int nblocks, int width, float *d0, float *d1,
+                             float *d2) {
+    const int j = threadIdx.x;
+    if (j >= width) return;
+    float t = 0.f;
+    for (int b = 0; b < nblocks; b++) t += red[(size_t)b * kBwdRedStride + j];
+    if (j < kHidden) d0[j] = t;
+    else if (j < 2 * kHidden) d1[j - kHidden] = t;
+    else d2[0] = t;
 }
 
 // Adam with bias correction factors bc1 = 1 - b1^t, bc2 = 1 - b2^t.
@@ -904,30 +846,24 @@ void launch_mlp_loss(const float *y, const float *t, int n, float lambda, float 
     k_mlp_loss<<<1, 1024, 0, st>>>(y, t, n, lambda, dy, loss);
 }
 
+int bwd_row_blocks(int n) {
+    const int b = (n + kBwdRows - 1) / kBwdRows;
+    return b < 1 ? 1 : (b > kBwdBlocksMax ? kBwdBlocksMax : b);
+}
+
 void launch_mlp_head_bwd(const MlpPacked *mlp, const float *dy, const float *z2, int n, uint16_t *dz2,
-                         float *grad, cudaStream_t st) {
-    k_mlp_head_bwd<<<kHidden / 32, 256, 0, st>>>(mlp, dy, z2, n, dz2, grad);
+                         float *red, float *grad, cudaStream_t st) {
+    const int nb = bwd_row_blocks(n), rows_per = (n + nb - 1) / nb;
+    k_mlp_head_bwd<<<dim3(kHidden / 32, nb), 256, 0, st>>>(mlp, dy, z2, n, rows_per, dz2, red);
+    k_bwd_reduce<<<1, 2 * kHidden + 32, 0, st>>>(red, nb, 2 * kHidden + 1, grad + kBlobB2, grad + kBlobW3,
+                                                 grad + kBlobB3);
 }
 
-void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *dbias,
+void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *red, float *dbias,
                         cudaStream_t st) {
-    k_mlp_act_bwd<<<kHidden / 32, 256, 0, st>>>(dh, z, n, dz, dbias);
-}
-
-void launch_gemm_bf16(const uint16_t *A, int ta, const uint16_t *B, int tb, int M, int N, int K,
-                      float *C, float *partial, int splits, cudaStream_t st) {
-    if (splits < 1) splits = 1;
-    int kper = (K + splits - 1) / splits;
-    kper = (kper + kGBK - 1) / kGBK * kGBK;
-    splits = (K + kper - 1) / kper;
-    if (splits < 1) splits = 1;
-    dim3 grid((N + kGBN - 1) / kGBN, (M + kGBM - 1) / kGBM, splits);
-    if (splits == 1) {
-        k_gemm_bf16<<<grid, 128, 0, st>>>(A, ta, B, tb, M, N, K, kper, C);
-        return;
-    }
-    k_gemm_bf16<<<grid, 128, 0, st>>>(A, ta, B, tb, M, N, K, kper, partial);
-    k_splitk_sum<<<(M * N + 255) / 256, 256, 0, st>>>(partial, splits, M * N, C);
+    const int nb = bwd_row_blocks(n), rows_per = (n + nb - 1) / nb;
+    k_mlp_act_bwd<<<dim3(kHidden / 32, nb), 256, 0, st>>>(dh, z, n, rows_per, dz, red);
+    k_bwd_reduce<<<1, kHidden, 0, st>>>(red, nb, kHidden, dbias, nullptr, nullptr);
 }
 
 void launch_adam(float *w, const float *g, float *m, float *v, int n, int first, float lr, float b1,

@@ -188,17 +188,24 @@ void launch_mlp_forward(const MlpPacked *mlp, const float *x, int n, float *y, c
 void launch_mlp_loss(const float *y, const float *t, int n, float lambda, float *dy, float *loss,
                      cudaStream_t st);
 // dZ = dH (or dy x w3) * gelu'(Z) as bf16, with column sums (bias gradients)
-// and, for the head, the w3 / b3 gradients.
-void launch_mlp_head_bwd(const MlpPacked *mlp, const float *dy, const float *z2, int n,
-                         uint16_t *dz2, float *grad, cudaStream_t st);
-void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *dbias,
+// and, for the head, the w3 / b3 gradients.  Rows are split into up to
+// kBwdBlocksMax blocks of >= kBwdRows rows whose partial sums go to `red`
+// (kBwdBlocksMax x kBwdRedStride floats) and are added in block order.
+constexpr int kBwdRows = 128, kBwdBlocksMax = 64, kBwdRedStride = 2 * kHidden + 4;
+int bwd_row_blocks(int n);
+void launch_mlp_head_bwd(const MlpPacked *mlp, const float *dy, const float *z2, int n, uint16_t *dz2,
+                         float *red, float *grad, cudaStream_t st);
+void launch_mlp_act_bwd(const float *dh, const float *z, int n, uint16_t *dz, float *red, float *dbias,
                         cudaStream_t st);
-// C[M][N] = op(A)[M][K] op(B)[K][N] on BF16 tensor cores, FP32 out; A is
-// [M][K] (ta = 0) or [K][M] (ta = 1) row-major, B is [K][N] (tb = 0) or
-// [N][K] (tb = 1).  K is split over `splits` partial products summed in a
-// fixed order into C.
-void launch_gemm_bf16(const uint16_t *A, int ta, const uint16_t *B, int tb, int M, int N, int K,
-                      float *C, float *partial, int splits, cudaStream_t st);
+// k_tcgen05.cu: C[M][N] = A[M][K] . B[N][K]^T on the tcgen05 tensor cores,
+// BF16 in, FP32 out.  A is K-major ([M][lda], a_mn = 0) or MN-major
+// ([K][lda], a_mn = 1, M <= 128); B likewise with N (N <= 256); lda, ldb
+// multiples of 8 elements, 16-byte aligned pointers.  C has row stride ldc,
+// or is written transposed (C[n][m], c_trans = 1).  K is split over `splits`
+// partial tiles in `partial` (splits x M x N floats) summed in a fixed order.
+// Returns 0, -1 (arguments), -2 (tensor map) or -3 (launch).
+int launch_gemm_tc(const uint16_t *A, int lda, int a_mn, const uint16_t *B, int ldb, int b_mn, int M, int N,
+                   int K, float *C, int ldc, int c_trans, float *partial, int splits, int *err, cudaStream_t st);
 void launch_adam(float *w, const float *g, float *m, float *v, int n, int first, float lr, float b1,
                  float b2, float eps, float bc1, float bc2, cudaStream_t st);
 

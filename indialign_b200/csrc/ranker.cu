@@ -14,6 +14,8 @@ namespace ia {
 
 namespace {
 
+static_assert(offsetof(MlpPacked, W2) % 16 == 0, "the packed W2 is a TMA source: 16-byte aligned");
+
 constexpr size_t kAlign = 256;
 size_t up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 size_t rows16(int n) { return (size_t)((n + 15) / 16 * 16); }
@@ -38,10 +40,11 @@ size_t save_bytes(int n) {
 }
 
 constexpr int kSplitsMax = 64;
-// Work buffer: dz2 bf16 [n16][128] | dh1 f32 [n16][128] | dz1 bf16 [n16][128] | split-K partials
+// Work buffer: dz2 bf16 [n16][128] | dh1 f32 [n16][128] | dz1 bf16 [n16][128] | split-K partials |
+// row-block partial sums of the bias gradients
 struct Work {
     uint16_t *dz2, *dz1;
-    float *dh1, *part;
+    float *dh1, *part, *red;
 };
 Work work_view(void *base, int n) {
     const size_t r = rows16(n);
@@ -54,12 +57,14 @@ Work work_view(void *base, int n) {
     w.dz1 = reinterpret_cast<uint16_t *>(p);
     p += up(r * kHidden * 2);
     w.part = reinterpret_cast<float *>(p);
+    p += up((size_t)kSplitsMax * kHidden * kHidden * 4);
+    w.red = reinterpret_cast<float *>(p);
     return w;
 }
 size_t work_bytes(int n) {
     const size_t r = rows16(n);
     return up(r * kHidden * 2) + up(r * kHidden * 4) + up(r * kHidden * 2) +
-           up((size_t)kSplitsMax * kHidden * kHidden * 4);
+           up((size_t)kSplitsMax * kHidden * kHidden * 4) + up((size_t)kBwdBlocksMax * kBwdRedStride * 4);
 }
 
 // K splits of a weight-gradient GEMM (K = batch rows): >= 256 rows per split.
@@ -126,18 +131,40 @@ int indialign_mlp_backward(const void *d_packed, const float *d_dy, int n, const
     const Work w = work_view(d_work, n);
     if (cudaMemsetAsync(d_grad, 0, kBlobW1 * sizeof(float), st) != cudaSuccess) return status("mlp_backward");
     // head: dz2, db2, dw3, db3
-    launch_mlp_head_bwd(mlp, d_dy, sv.z2, n, w.dz2, d_grad, st);
-    // dW2 = h1^T dz2
-    launch_gemm_bf16(sv.h1, 1, w.dz2, 0, kHidden, kHidden, n, d_grad + kBlobW2, w.part, splits_for(n), st);
-    // dh1 = dz2 W2^T (W2 stored [in][out] = [n][k] of this product)
+    launch_mlp_head_bwd(mlp, d_dy, sv.z2, n, w.dz2, w.red, d_grad, st);
+    // The three products on the tcgen05 tensor cores, each operand read in
+    // the layout it is stored in (h1, dz2, dz1, xn are [rows][features]:
+    // MN-major for the weight gradients, K-major for dh1).
+    int rc = 0;
+    // dW2[i][j] = sum_r h1[r][i] dz2[r][j]   (M = N = 128, K = n, split over rows)
+    rc |= launch_gemm_tc(sv.h1, kHidden, 1, w.dz2, kHidden, 1, kHidden, kHidden, n, d_grad + kBlobW2, kHidden, 0,
+                         w.part, splits_for(n), nullptr, st);
+    // dh1[r][i] = sum_j dz2[r][j] W2[i][j]   (W2 packed [in][out]: K-major B)
     const uint16_t *W2 = reinterpret_cast<const uint16_t *>(reinterpret_cast<const char *>(mlp) +
                                                             offsetof(MlpPacked, W2));
-    launch_gemm_bf16(w.dz2, 0, W2, 1, n, kHidden, kHidden, w.dh1, w.part, 1, st);
+    rc |= launch_gemm_tc(w.dz2, kHidden, 0, W2, kHidden, 0, n, kHidden, kHidden, w.dh1, kHidden, 0, nullptr, 1,
+                         nullptr, st);
     // dz1, db1
-    launch_mlp_act_bwd(w.dh1, sv.z1, n, w.dz1, d_grad + kBlobB1, st);
-    // dW1 = xn^T dz1
-    launch_gemm_bf16(sv.xn, 1, w.dz1, 0, kFeatures, kHidden, n, d_grad + kBlobW1, w.part, splits_for(n), st);
+    launch_mlp_act_bwd(w.dh1, sv.z1, n, w.dz1, w.red, d_grad + kBlobB1, st);
+    // dW1[f][i] = sum_r xn[r][f] dz1[r][i], computed as its transpose
+    // (M = 128 hidden units on the TMEM lanes, N = 16 features) and stored transposed
+    rc |= launch_gemm_tc(w.dz1, kHidden, 1, sv.xn, kFeatures, 1, kHidden, kFeatures, n, d_grad + kBlobW1, kHidden,
+                         1, w.part, splits_for(n), nullptr, st);
+    if (rc != 0) return bad("mlp_backward: tensor-core GEMM rejected its operands (alignment or tensor map)");
     return status("mlp_backward");
+}
+
+int indialign_gemm_bf16(const void *d_a, int lda, int a_mn, const void *d_b, int ldb, int b_mn, int m, int n,
+                        int k, float *d_c, int ldc, int c_trans, float *d_partial, int splits, void *stream) {
+    using namespace ia;
+    const int rc = launch_gemm_tc(static_cast<const uint16_t *>(d_a), lda, a_mn ? 1 : 0,
+                                  static_cast<const uint16_t *>(d_b), ldb, b_mn ? 1 : 0, m, n, k, d_c, ldc,
+                                  c_trans ? 1 : 0, d_partial, splits, nullptr, static_cast<cudaStream_t>(stream));
+    if (rc == -1) return bad("gemm_bf16: bad shape, stride, alignment or missing partial buffer");
+    if (rc == -2) return bad("gemm_bf16: tensor map encoding failed");
+    const int st = status("gemm_bf16");
+    if (rc != 0 && st == INDIALIGN_OK) return bad("gemm_bf16: kernel attributes could not be set");
+    return st;
 }
 
 int indialign_mlp_adam(float *d_blob, const float *d_grad, float *d_m, float *d_v, int step, float lr,

@@ -213,3 +213,56 @@ def train(feat: np.ndarray, label: np.ndarray, group: np.ndarray, epochs: int = 
         if log:
             log(f"epoch {ep + 1}/{epochs}: {nb} steps, mean loss {float(acc.item()) / max(nb, 1):.5f}")
     return tr.numpy_blob()
+
+
+def time_epoch(rows: int = 1 << 20, batch: int = 8192, groups: int = 4096, seed: int = 0,
+               warmup: int = 3) -> dict:
+    """Device time of one training epoch (the train() loop body: row gather,
+    forward, loss, backward, Adam, repack) over `rows` synthetic feature rows
+    in `groups` candidate lists, batch `batch`, after `warmup` untimed steps;
+    plus the backward's share, timed with events around each backward call
+    on the same stream."""
+    import torch
+    rng = np.random.default_rng(seed)
+    feat = rng.standard_normal((rows, FEATURES)).astype(np.float32)
+    label = rng.uniform(0.0, 1.0, rows).astype(np.float32)
+    group = np.sort(rng.integers(0, groups, rows))
+    tr = Trainer(init_blob(feat.mean(0), feat.std(0), seed), batch=batch)
+    X = torch.tensor(feat, device="cuda")
+    T = torch.tensor(label, device="cuda")
+    pairs = pair_rows(group, rng)
+    idx_all = torch.tensor(pairs.reshape(-1), device="cuda")
+    half = batch // 2
+    starts = list(range(0, pairs.shape[0] - half + 1, half))
+    for s in starts[:warmup]:
+        idx = idx_all[2 * s:2 * (s + half)]
+        tr.step(X[idx].contiguous(), T[idx].contiguous())
+    torch.cuda.synchronize()
+    lib, st = tr.lib, tr.stream
+    bw = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for s in starts:
+        idx = idx_all[2 * s:2 * (s + half)]
+        x, t = X[idx].contiguous(), T[idx].contiguous()
+        n = int(x.shape[0])
+        y = tr.forward(x, save=True)
+        tr._ck(lib.indialign_mlp_loss(y.data_ptr(), t.data_ptr(), n, ctypes.c_float(tr.lam), tr.dy.data_ptr(),
+                                      tr.loss.data_ptr(), st), "mlp_loss")
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        tr._ck(lib.indialign_mlp_backward(tr.packed.data_ptr(), tr.dy.data_ptr(), n, tr.save.data_ptr(),
+                                          tr.grad.data_ptr(), tr.work.data_ptr(), st), "mlp_backward")
+        b1.record()
+        bw.append((b0, b1))
+        tr.steps += 1
+        f = ctypes.c_float
+        tr._ck(lib.indialign_mlp_adam(tr.blob.data_ptr(), tr.grad.data_ptr(), tr.m.data_ptr(), tr.v.data_ptr(),
+                                      tr.steps, f(tr.lr), f(tr.beta1), f(tr.beta2), f(tr.eps), st), "mlp_adam")
+        tr.pack()
+    ev1.record()
+    torch.cuda.synchronize()
+    bw_ms = [a.elapsed_time(b) for a, b in bw]
+    return {"rows": rows, "batch": batch, "steps": len(starts), "epoch_ms": ev0.elapsed_time(ev1),
+            "backward_ms_per_step": float(np.mean(bw_ms)), "backward_ms_min": float(np.min(bw_ms)),
+            "loss": float(tr.loss.item()), "grad_finite": bool(torch.isfinite(tr.grad).all().item())}

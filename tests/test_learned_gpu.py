@@ -89,7 +89,7 @@ def test_mlp_loss_matches_oracle(torch_cuda):
     np.testing.assert_allclose(dy.cpu().numpy(), dyo, atol=1e-7, rtol=1e-4)
 
 
-@pytest.mark.parametrize("n", [256, 8192])
+@pytest.mark.parametrize("n", [77, 256, 1000, 8192])
 def test_mlp_backward_gradient_check(torch_cuda, n):
     """Gradients of the BF16 tensor-core backward vs the oracle (same
     rounding points, FP64 sums)."""
@@ -222,7 +222,7 @@ def _learned_run(pairs, blob, k=8, margin=0.02, audit=0.02, seed=0, outputs=True
     cfg = ia.default_config()
     rc = lib.indialign_tmscore_search_batch_ex(pk.n, pk.arr, ctypes.byref(cfg), ctypes.byref(opts), res)
     assert rc == 0, ia.last_error()
-    return abi.results_to_numpy(res, pk.n), stats.reshape(ia.CAND_KINDS, 8), score, sel, off
+    return abi.results_to_numpy(res, pk.n), stats.reshape(ia.CAND_KINDS, -1), score, sel, off
 
 
 def _lists(kind, n, off):
@@ -336,7 +336,7 @@ def test_learned_mode_with_full_fallback_is_the_plain_search():
         np.testing.assert_array_equal(s, s0)
         np.testing.assert_array_equal(R, R0)
         np.testing.assert_array_equal(t, t0)
-        st = stats.reshape(ia.CAND_KINDS, 8)
+        st = stats.reshape(ia.CAND_KINDS, -1)
         if mask == 0:
             assert st[:, 0].sum() > 0 and st[:, 3].sum() == 0  # ranked, never pruned
         else:
