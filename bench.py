@@ -63,11 +63,13 @@ REF_SO = os.path.join(ROOT, "oracle", "_ref", "libindialign_ref.so")
 FLOP_PER_CELL = 18.0
 FLOP_PER_VISIT = 55.0
 # DRAM bytes (read + write) of the seed-bank kernel per residue visit, from
-# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the first
-# three k_bank launches of a 192-pair learned16384 call, divided by their
-# residue visits; the kernel's traffic is its item records and staged point
-# sets, which grow in proportion to the visits.  None: not measured.
-BANK_DRAM_BYTES_PER_VISIT = None
+# an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of all nine
+# k_bank launches of one 192-pair learned16384 call (`bench.py --step-pairs
+# 192 --steps 1 --warmup 0 --no-cpu-baseline --no-e2e --no-plain --no-split`):
+# 511.1 MB over that call's 13.08 G residue visits.  The traffic is the item
+# records (13 doubles per item) and the staged point sets, which grow in
+# proportion to the visits.
+BANK_DRAM_BYTES_PER_VISIT = 511.1e6 / 13.084e9
 STAGES = ["seeds", "seed_bank", "ss", "gapless", "local_fragment", "threading_dp",
           "dense_local_fragment", "topk", "dp_refine", "offset_dp", "weighted", "total"]
 
@@ -515,13 +517,14 @@ def main():
         # MLP weight pack
         per_call = 2 + (1 if learned_mode else 0)
         launches = int(sum(int(c[7]) + per_call for c in lrn["ctr"]))
-        rst = np.sum(lrn["rst"], 0).reshape(ia.CAND_KINDS, 8)
+        rst = np.sum(lrn["rst"], 0).reshape(ia.CAND_KINDS, -1)
         rank_info = {}
         for k, nm in enumerate(ia.CAND_NAMES):
             g = max(int(rst[k, 0]), 1)
             rank_info[nm] = {"pairs": int(rst[k, 0]), "fallback_rate": rst[k, 1] / g, "audit_rate": rst[k, 2] / g,
                              "pruned_rate": rst[k, 3] / g, "refined_fraction": rst[k, 5] / max(int(rst[k, 4]), 1),
-                             "audit_misses": int(rst[k, 6])}
+                             "audits": int(rst[k, 2]), "audit_misses": int(rst[k, 6]),
+                             "audit_misses_1e-4": int(rst[k, 8]), "audit_misses_1e-3": int(rst[k, 9])}
         cpu = None
         if not args.no_cpu_baseline:
             timed_pairs = [p for b in batches[args.warmup:] for p in b]
@@ -575,7 +578,11 @@ def compact_line(line: dict) -> dict:
         lists = sum(v["pairs"] for v in r.values())
         out["rank"] = {"lists": lists,
                        "fallback_rate": sum(v["fallback_rate"] * v["pairs"] for v in r.values()) / max(lists, 1),
-                       "audit_misses": sum(v["audit_misses"] for v in r.values())}
+                       "audits": sum(v.get("audits", 0) for v in r.values()),
+                       "audit_misses": sum(v["audit_misses"] for v in r.values()),
+                       "audit_misses_1e-4": sum(v.get("audit_misses_1e-4", 0) for v in r.values()),
+                       "miss_rate_1e-4": {k: round(v.get("audit_misses_1e-4", 0) / v["audits"], 3)
+                                          for k, v in r.items() if v.get("audits")}}
     rf = line.get("roofline")
     if rf:
         out["roofline"] = {k: rf[k] for k in ("kernel", "bound", "achieved", "peak", "unit", "frac", "traffic",

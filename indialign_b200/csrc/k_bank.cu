@@ -30,6 +30,11 @@
 #ifndef IA_BANK_MINB
 #define IA_BANK_MINB 4
 #endif
+// build-time knob: cutoff passes accumulate inliers by select (every lane
+// runs the accumulate, outliers add zeros) instead of a branch
+#ifndef IA_BANK_SELECT_ACC
+#define IA_BANK_SELECT_ACC 0
+#endif
 
 namespace ia {
 
@@ -56,6 +61,19 @@ struct MomentsF {
         h[3] = fmaf(py, qx, h[3]); h[4] = fmaf(py, qy, h[4]); h[5] = fmaf(py, qz, h[5]);
         h[6] = fmaf(pz, qx, h[6]); h[7] = fmaf(pz, qy, h[7]); h[8] = fmaf(pz, qz, h[8]);
         w++;
+    }
+    // The same sums with (p, q) replaced by zeros unless `in`: zero terms
+    // leave every sum unchanged, and a non-finite coordinate of an outlier
+    // never reaches them (it is selected away, not multiplied by zero).
+    IA_DEV void add_if(bool in, float px, float py, float pz, float qx, float qy, float qz) {
+        px = in ? px : 0.f; py = in ? py : 0.f; pz = in ? pz : 0.f;
+        qx = in ? qx : 0.f; qy = in ? qy : 0.f; qz = in ? qz : 0.f;
+        sp[0] += px; sp[1] += py; sp[2] += pz;
+        sq[0] += qx; sq[1] += qy; sq[2] += qz;
+        h[0] = fmaf(px, qx, h[0]); h[1] = fmaf(px, qy, h[1]); h[2] = fmaf(px, qz, h[2]);
+        h[3] = fmaf(py, qx, h[3]); h[4] = fmaf(py, qy, h[4]); h[5] = fmaf(py, qz, h[5]);
+        h[6] = fmaf(pz, qx, h[6]); h[7] = fmaf(pz, qy, h[7]); h[8] = fmaf(pz, qz, h[8]);
+        w += in ? 1 : 0;
     }
     // Kabsch in FP64 from these sums (identity below 3 pairs)
     IA_DEV void kabsch(double *R, double *t) const {
@@ -330,11 +348,19 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             int cnt = 0;
             for (int i = 0; i < n; i++) {
                 const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, i);
+#if IA_BANK_SELECT_ACC
+                m.add_if(running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2, pp.x, pp.y, pp.z, qq.x,
+                         qq.y, qq.z);
+#else
                 if (running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2) {
                     m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
                     cnt++;
                 }
+#endif
             }
+#if IA_BANK_SELECT_ACC
+            cnt = m.w;
+#endif
             if (running) {
                 if (cnt >= 3) m.kabsch(R, t);
                 ++iter;

@@ -232,6 +232,8 @@ enum RankStat {
     RS_AUDIT_MISS,     // audited pairs whose top-k windows miss the best window score
     RS_SMALL,          // gated lists with at most k candidates or of a pair shorter than
                        // the ranking length threshold (all refined)
+    RS_AUDIT_MISS_1E4, // audited pairs whose top-k best is more than 1e-4 below the best
+    RS_AUDIT_MISS_1E3, // ... more than 1e-3 below
     kRankStats
 };
 

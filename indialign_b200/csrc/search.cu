@@ -1103,6 +1103,7 @@ static int run_batch(Ctx *c, const Cfg &cfg, const Source &src, double *results,
         g_last_error = "device error flag " + std::to_string(err);
         return INDIALIGN_E_DEVICE;
     }
+    static_assert(kCandKinds * kRankStats == INDIALIGN_RANK_STATS, "rank_stats layout: [kinds][kRankStats]");
     if (cfg.mode == INDIALIGN_MODE_LEARNED && opts->rank_stats) {
         unsigned long long h[kCandKinds * kRankStats];
         CK(cudaMemcpy(h, c->rstats.p, sizeof(h), cudaMemcpyDeviceToHost));
