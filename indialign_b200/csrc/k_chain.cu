@@ -100,9 +100,19 @@ IA_DEV T smat_entry(float inv_d0sq, float cut2, float mx, float my, float mz, ui
 // diagonal zero) and a gap move out of a diagonal cell pays the penalty;
 // without one the bit is irrelevant and H is kept plain.  Ties prefer diag,
 // then left, then up.  Selects only, so a step is one basic block.
-template <bool GAPZ, typename T>
+// MAXF: the matrix holds no NaN and no -0 (the distance-score mode: entries
+// are 1/(1 + d2/d0^2) or +0, sums of them start at +0), so the choice can be
+// written with two max operations: diag wins iff diag >= max(left, up), and
+// H = max(diag, max(left, up)) equals the selected value (equal candidates
+// are the same number).
+template <bool GAPZ, typename T, bool MAXF = false>
 IA_DEV T nw_cell(T diag_src, T sc, T up_enc, T left_enc, T gap, uint32_t &dir) {
     const T diag = diag_src + sc;
+    if (GAPZ && MAXF) {
+        const T m = fmax(left_enc, up_enc);
+        dir = diag >= m ? 0u : (left_enc >= up_enc ? 2u : 1u);
+        return fmax(diag, m);
+    }
     T up, left;
     if (GAPZ) {
         up = up_enc;
@@ -159,8 +169,10 @@ IA_DEV size_t trace_word(int i, int w, int P, int G) {
 // step earlier, since P >= 64).  Per step a lane computes two independent
 // cells with one shuffle and one shared-memory column load.  Cells outside
 // the matrix are computed on clamped indices and never read by a valid one
-// (a row's state is reset when it enters a stripe, and its neighbours only
-// read its in-range cells), so the step has no per-cell branches.
+// (a row's state is reset when it enters a stripe, its neighbours only read
+// its in-range cells, and row 1's column-0 cell, which column 1 reads as its
+// left neighbour, is replaced by the boundary +0), so the step has no
+// per-cell branches.
 // Out of line: inside the chain kernel (register-capped) an inlined fill
 // shares the register budget with the caller's live state and spilled inside
 // its step loop (measured: ~4 local loads per step); as a call it has the
@@ -188,8 +200,13 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
     uint8_t l0 = 0, l1 = 0, ln1 = 0;
     T h0 = 0, h1 = 0, h0prev = 0, up0prev = 0;
     float q1x = 0, q1y = 0, q1z = 0;  // column of row 1 (previous step's row-0 column)
+    // direction bits enter at the top and move down 2 bits a step, so after
+    // the word's 16th step the bits of its step t sit at 2*(t%16); a word
+    // stored after m < 16 of its steps is shifted down by 32 - 2m
     uint32_t acc0 = 0, acc1 = 0;
     bool r0ok = false, r1ok = false;
+    bool st31 = false;  // lane 31 writes the stripe's boundary row
+    bool ld0 = false;   // lane 0 reads the previous stripe's boundary row
     // this lane's two rows in the current stripe's block: word g of them at
     // blk[g * 64 + 2 * lane], blk[g * 64 + 2 * lane + 1]; g0 = (k*P)/16
     uint2 *blk = reinterpret_cast<uint2 *>(trace) + lane;
@@ -201,8 +218,10 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
         T up0 = __shfl_up_sync(kFull, h1, 1);
         if (j0 > P) {  // next stripe (rare): flush the finished rows' last words
             const int w = (step - 1) >> 4;
-            if (((step - 1) & 15) != 15 && k < S)  // else stored (and cleared) last step
-                blk[(size_t)(w - g0) * 32] = make_uint2(acc0, acc1);
+            if (((step - 1) & 15) != 15 && k < S) {  // else stored (and cleared) last step
+                const int sh = 30 - 2 * ((step - 1) & 15);
+                blk[(size_t)(w - g0) * 32] = make_uint2(acc0 >> sh, acc1 >> sh);
+            }
             j0 -= P;
             k++;
             i0 += 64;
@@ -214,6 +233,8 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
             acc0 = acc1 = 0;
             r0ok = k < S && i0 <= plen;
             r1ok = k < S && i0 + 1 <= plen;
+            st31 = lane == 31 && k + 1 < S && r1ok;
+            ld0 = k > 0 && r0ok;
             const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
             const double *p0 = x.P + 3 * a0, *p1 = x.P + 3 * a1;
             if (SMODE != SMAT_SS2 && SMODE != SMAT_EXPLICIT) {
@@ -228,46 +249,51 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
                 l1 = pr.Lp[a1];
             }
         }
-        const int jc = min(max(j0, 1), nlen) - 1;  // clamped 0-based column
+        // 0-based column; a cell outside the matrix (j0 < 1 or > nlen) is
+        // computed on column nlen-1 and never read by a valid one (row 1's
+        // column-0 cell is replaced by the boundary below)
+        const int jc = (int)min((unsigned)(j0 - 1), (unsigned)(nlen - 1));
         float q0x = 0, q0y = 0, q0z = 0;
         if (SMODE == SMAT_DP || SMODE == SMAT_SS4) {
             const float4 q = native_f32(pr, x, jc);
             q0x = q.x; q0y = q.y; q0z = q.z;
         }
         const uint8_t ln0 = (SMODE == SMAT_SS2 || SMODE == SMAT_SS4) ? pr.Ln[jc] : (uint8_t)0;
-        const bool v0 = r0ok && j0 >= 1 && j0 <= nlen;
-        if (lane == 0) up0 = (k > 0 && v0) ? bH[j0] : T(0);
+        if (lane == 0) up0 = (ld0 && (unsigned)(j0 - 1) < (unsigned)nlen) ? bH[j0] : T(0);
         uint32_t d0, d1;
         T sc0, sc1;
         if (SMODE == SMAT_EXPLICIT) {
             const int a0 = min(i0, plen) - 1, a1 = min(i0 + 1, plen) - 1;
-            const int jc1 = min(max(j0 - 1, 1), nlen) - 1;
+            const int jc1 = (int)min((unsigned)(j0 - 2), (unsigned)(nlen - 1));
             sc0 = (T)pr.smat[(size_t)a0 * nlen + jc];
             sc1 = (T)pr.smat[(size_t)a1 * nlen + jc1];
         } else {
             sc1 = smat_entry<SMODE, T>(inv_d0sq, cut2, m1x, m1y, m1z, l1, q1x, q1y, q1z, ln1);
             sc0 = smat_entry<SMODE, T>(inv_d0sq, cut2, m0x, m0y, m0z, l0, q0x, q0y, q0z, ln0);
         }
-        const T n1 = nw_cell<GAPZ, T>(h0prev, sc1, h0, h1, gap, d1);
-        const T n0 = nw_cell<GAPZ, T>(up0prev, sc0, up0, h0, gap, d0);
-        const int sh = 2 * (step & 15);
-        acc0 |= d0 << sh;
-        acc1 |= d1 << sh;
-        if (lane == 31 && k + 1 < S && r1ok && j0 >= 2 && j0 <= nlen + 1) bH[j0 - 1] = n1;
+        const T n1 = nw_cell<GAPZ, T, SMODE == SMAT_DP>(h0prev, sc1, h0, h1, gap, d1);
+        const T n0 = nw_cell<GAPZ, T, SMODE == SMAT_DP>(up0prev, sc0, up0, h0, gap, d0);
+        acc0 = __funnelshift_r(acc0, d0, 2);
+        acc1 = __funnelshift_r(acc1, d1, 2);
+        if (st31 && (unsigned)(j0 - 2) < (unsigned)nlen) bH[j0 - 1] = n1;
         if ((step & 15) == 15) {  // uniform: the warp stores one 256-byte line
             if (k < S) blk[(size_t)((step >> 4) - g0) * 32] = make_uint2(acc0, acc1);
             acc0 = acc1 = 0;
         }
         h0prev = hval<GAPZ, T>(h0);
         up0prev = hval<GAPZ, T>(up0);
-        h1 = n1;
+        // on a stripe's first step row 1 sits on column 0: keep the boundary
+        // H(i, 0) = +0 as its left neighbour for column 1
+        h1 = j0 == 1 ? T(0) : n1;
         h0 = n0;
         q1x = q0x; q1y = q0y; q1z = q0z;
         ln1 = ln0;
         j0++;
     }
-    if (((total_steps - 1) & 15) != 15 && k < S)  // flush the last rows' pending words
-        blk[(size_t)(((total_steps - 1) >> 4) - g0) * 32] = make_uint2(acc0, acc1);
+    if (((total_steps - 1) & 15) != 15 && k < S) {  // flush the last rows' pending words
+        const int sh = 30 - 2 * ((total_steps - 1) & 15);
+        blk[(size_t)(((total_steps - 1) >> 4) - g0) * 32] = make_uint2(acc0 >> sh, acc1 >> sh);
+    }
     __syncwarp();
     const long long clk1 = clock64();
     // traceback from (plen, nlen): diag emits a pair, up steps i, else j.
