@@ -30,11 +30,7 @@
 #ifndef IA_BANK_MINB
 #define IA_BANK_MINB 4
 #endif
-// build-time knob: cutoff passes accumulate inliers by select (every lane
-// runs the accumulate, outliers add zeros) instead of a branch
-#ifndef IA_BANK_SELECT_ACC
-#define IA_BANK_SELECT_ACC 0
-#endif
+
 
 namespace ia {
 
@@ -62,19 +58,6 @@ struct MomentsF {
         h[6] = fmaf(pz, qx, h[6]); h[7] = fmaf(pz, qy, h[7]); h[8] = fmaf(pz, qz, h[8]);
         w++;
     }
-    // The same sums with (p, q) replaced by zeros unless `in`: zero terms
-    // leave every sum unchanged, and a non-finite coordinate of an outlier
-    // never reaches them (it is selected away, not multiplied by zero).
-    IA_DEV void add_if(bool in, float px, float py, float pz, float qx, float qy, float qz) {
-        px = in ? px : 0.f; py = in ? py : 0.f; pz = in ? pz : 0.f;
-        qx = in ? qx : 0.f; qy = in ? qy : 0.f; qz = in ? qz : 0.f;
-        sp[0] += px; sp[1] += py; sp[2] += pz;
-        sq[0] += qx; sq[1] += qy; sq[2] += qz;
-        h[0] = fmaf(px, qx, h[0]); h[1] = fmaf(px, qy, h[1]); h[2] = fmaf(px, qz, h[2]);
-        h[3] = fmaf(py, qx, h[3]); h[4] = fmaf(py, qy, h[4]); h[5] = fmaf(py, qz, h[5]);
-        h[6] = fmaf(pz, qx, h[6]); h[7] = fmaf(pz, qy, h[7]); h[8] = fmaf(pz, qz, h[8]);
-        w += in ? 1 : 0;
-    }
     // Kabsch in FP64 from these sums (identity below 3 pairs)
     IA_DEV void kabsch(double *R, double *t) const {
         Moments m;
@@ -96,13 +79,21 @@ struct MomentsF {
 // float4 (x, y, z, w) with w = 1 for a valid residue of the cutoff and score
 // passes (V[i] != 0, or no mask) and 0 otherwise.
 //
+// The shared FP32 copy holds residues in pairs, so one paired FP32
+// instruction (f32x2) serves two residues: pair k = residues 2k, 2k+1 is two
+// float4 blocks {x_2k, x_2k+1, y_2k, y_2k+1} {z_2k, z_2k+1, w_2k, w_2k+1}; an
+// odd set ends with a zero point of w = 0.
+//
 // Point i of a set in the centred FP32 frame: the converted shared copy, or
 // converted on load from the FP64 global array (point sets too large for
 // shared memory).  Both give the same floats, so a pair's results do not
 // depend on which path its batch takes.
 template <bool SMEM>
 IA_DEV float4 point(const float4 *f, const double *d, const double *off, const uint8_t *V, int i) {
-    if constexpr (SMEM) return f[i];
+    if constexpr (SMEM) {
+        const float *e = reinterpret_cast<const float *>(f) + (i >> 1) * 8 + (i & 1);
+        return make_float4(e[0], e[2], e[4], e[6]);
+    }
     else return make_float4((float)(d[3 * i] - off[0]), (float)(d[3 * i + 1] - off[1]),
                             (float)(d[3 * i + 2] - off[2]), (V == nullptr || V[i] != 0) ? 1.f : 0.f);
 }
@@ -115,6 +106,35 @@ IA_DEV float dist2_f32(const float4 &p, const float4 &q, const float *Rf, const 
     const float dy = fmaf(p.x, Rf[1], fmaf(p.y, Rf[4], fmaf(p.z, Rf[7], tf[1] - q.y)));
     const float dz = fmaf(p.x, Rf[2], fmaf(p.y, Rf[5], fmaf(p.z, Rf[8], tf[2] - q.z)));
     return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+}
+
+// A transform with every entry duplicated, the operand form of paired FP32
+// instructions.
+struct XformF2 {
+    float2 r[9], t[3];
+    IA_DEV void set(const double *R, const double *t_) {
+#pragma unroll
+        for (int a = 0; a < 9; a++) r[a] = make_float2((float)R[a], (float)R[a]);
+#pragma unroll
+        for (int a = 0; a < 3; a++) t[a] = make_float2((float)t_[a], (float)t_[a]);
+    }
+};
+
+// dist2_f32 of the two residues of a staged pair (P blocks PA, PB; Q blocks
+// QA, QB), element by element the same operations in the same order, two
+// residues per paired instruction (t - q is the single rounding of
+// q * (-1) + t).
+IA_DEV float2 dist2_pair(const float4 &PA, const float4 &PB, const float4 &QA, const float4 &QB,
+                         const XformF2 &X) {
+    const float2 px = make_float2(PA.x, PA.y), py = make_float2(PA.z, PA.w), pz = make_float2(PB.x, PB.y);
+    const float2 m1 = make_float2(-1.f, -1.f);
+    float2 ax = __ffma2_rn(make_float2(QA.x, QA.y), m1, X.t[0]);
+    float2 ay = __ffma2_rn(make_float2(QA.z, QA.w), m1, X.t[1]);
+    float2 az = __ffma2_rn(make_float2(QB.x, QB.y), m1, X.t[2]);
+    ax = __ffma2_rn(px, X.r[0], __ffma2_rn(py, X.r[3], __ffma2_rn(pz, X.r[6], ax)));
+    ay = __ffma2_rn(px, X.r[1], __ffma2_rn(py, X.r[4], __ffma2_rn(pz, X.r[7], ay)));
+    az = __ffma2_rn(px, X.r[2], __ffma2_rn(py, X.r[5], __ffma2_rn(pz, X.r[8], az)));
+    return __ffma2_rn(az, az, __ffma2_rn(ay, ay, __fmul2_rn(ax, ax)));
 }
 
 // CTA-wide FP64 mean of the finite values of n points, per axis, into
@@ -162,11 +182,14 @@ IA_DEV void points_mean(const double *src, int n, double *out, double *red) {
 }
 
 // CTA-wide in-place conversion of n staged FP64 points (at src, inside the
-// region that starts at dst) to centred FP32 float4 at dst, w from the
-// validity bytes V (null: all valid).  Round r reads points [128r, 128r+128)
-// before any thread writes them; its writes end at byte 16*128(r+1), at or
-// below the first byte (24*128(r+1)) that a later round reads.
-IA_DEV void points_to_f32(const double *src, float4 *dst, int n, const double *off, const uint8_t *V) {
+// region that starts at dst) to centred FP32 residue pairs at dst (layout
+// above), w from the validity bytes V (null: all valid).  Round r reads
+// points [128r, 128r+128) before any thread writes them; its writes end at
+// byte 16*128(r+1) + 16, below the first byte (24*128(r+1)) that a later
+// round reads; the pairs of n points take 32*ceil(n/2) <= 16n + 16 bytes,
+// inside the 24n + 32 bytes of the staged region.
+IA_DEV void points_to_f32(const double *src, float4 *dst4, int n, const double *off, const uint8_t *V) {
+    float *dst = reinterpret_cast<float *>(dst4);
     for (int base = 0; base < n; base += kBankChunk) {
         const int i = base + (int)threadIdx.x;
         double x = 0.0, y = 0.0, z = 0.0;
@@ -178,7 +201,13 @@ IA_DEV void points_to_f32(const double *src, float4 *dst, int n, const double *o
             w = (V == nullptr || V[i] != 0) ? 1.f : 0.f;
         }
         __syncthreads();
-        if (i < n) dst[i] = make_float4((float)x, (float)y, (float)z, w);
+        if (i < n || (i == n && (n & 1))) {  // residue i, or the zero point after an odd set
+            float *e = dst + (i >> 1) * 8 + (i & 1);
+            e[0] = (float)x;
+            e[2] = (float)y;
+            e[4] = (float)z;
+            e[6] = w;
+        }
     }
     __syncthreads();
 }
@@ -346,21 +375,32 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
             for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
             m.clear();
             int cnt = 0;
-            for (int i = 0; i < n; i++) {
-                const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, i);
-#if IA_BANK_SELECT_ACC
-                m.add_if(running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2, pp.x, pp.y, pp.z, qq.x,
-                         qq.y, qq.z);
-#else
-                if (running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2) {
-                    m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
-                    cnt++;
+            if constexpr (SMEM) {
+                // two residues per step: distances by paired instructions,
+                // the accumulate per residue in residue order
+                XformF2 X;
+                X.set(R, t);
+                for (int k2 = 0; k2 < (n + 1) >> 1; k2++) {
+                    const float4 PA = Pf[2 * k2], PB = Pf[2 * k2 + 1], QA = Qf[2 * k2], QB = Qf[2 * k2 + 1];
+                    const float2 d2 = dist2_pair(PA, PB, QA, QB, X);
+                    if (running && PB.z != 0.f && d2.x <= cut2) {
+                        m.add(PA.x, PA.z, PB.x, QA.x, QA.z, QB.x);
+                        cnt++;
+                    }
+                    if (running && PB.w != 0.f && d2.y <= cut2) {
+                        m.add(PA.y, PA.w, PB.y, QA.y, QA.w, QB.y);
+                        cnt++;
+                    }
                 }
-#endif
+            } else {
+                for (int i = 0; i < n; i++) {
+                    const float4 pp = point<SMEM>(Pf, Pd, oP, V, i), qq = point<SMEM>(Qf, Qd, oQ, nullptr, i);
+                    if (running && pp.w != 0.f && dist2_f32(pp, qq, Rf, tf) <= cut2) {
+                        m.add(pp.x, pp.y, pp.z, qq.x, qq.y, qq.z);
+                        cnt++;
+                    }
+                }
             }
-#if IA_BANK_SELECT_ACC
-            cnt = m.w;
-#endif
             if (running) {
                 if (cnt >= 3) m.kabsch(R, t);
                 ++iter;
@@ -382,15 +422,28 @@ k_bank(const BankTask *__restrict__ tasks, const int *__restrict__ chunk_begin,
 #pragma unroll
             for (int a = 0; a < 3; a++) tf[a] = (float)t[a];
             float sum = 0.f, comp = 0.f;
-            for (int i = 0; i < n; i++) {
-                const float4 pp = point<SMEM>(Pf, Pd, oP, V, i);
-                if (pp.w == 0.f) continue;
-                const float d2 = dist2_f32(pp, point<SMEM>(Qf, Qd, oQ, nullptr, i), Rf, tf);
+            auto add_term = [&](float d2) {
                 if (!T.use_d8 || d2 <= sd8sq) {
                     const float y = __frcp_rn(fmaf(d2, inv_d0sq, 1.0f)) - comp;
                     const float s2 = sum + y;
                     comp = (s2 - sum) - y;
                     sum = s2;
+                }
+            };
+            if constexpr (SMEM) {
+                XformF2 X;
+                X.set(R, t);
+                for (int k2 = 0; k2 < (n + 1) >> 1; k2++) {
+                    const float4 PA = Pf[2 * k2], PB = Pf[2 * k2 + 1], QA = Qf[2 * k2], QB = Qf[2 * k2 + 1];
+                    const float2 d2 = dist2_pair(PA, PB, QA, QB, X);
+                    if (PB.z != 0.f) add_term(d2.x);
+                    if (PB.w != 0.f) add_term(d2.y);
+                }
+            } else {
+                for (int i = 0; i < n; i++) {
+                    const float4 pp = point<SMEM>(Pf, Pd, oP, V, i);
+                    if (pp.w == 0.f) continue;
+                    add_term(dist2_f32(pp, point<SMEM>(Qf, Qd, oQ, nullptr, i), Rf, tf));
                 }
             }
             score = (double)sum / fmax(T.lnorm, 1.0);

@@ -208,7 +208,9 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
     bool st31 = false;  // lane 31 writes the stripe's boundary row
     bool ld0 = false;   // lane 0 reads the previous stripe's boundary row
     // this lane's two rows in the current stripe's block: word g of them at
-    // blk[g * 64 + 2 * lane], blk[g * 64 + 2 * lane + 1]; g0 = (k*P)/16
+    // blk[g * 64 + 2 * lane], blk[g * 64 + 2 * lane + 1]; g0 = (k*P)/16.
+    // Only lanes with a row inside the matrix store (a short window leaves
+    // most of its stripe's lanes without one)
     uint2 *blk = reinterpret_cast<uint2 *>(trace) + lane;
     int g0 = 0;
     const int last_lane = ((plen - 1) & 63) >> 1;
@@ -218,7 +220,7 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
         T up0 = __shfl_up_sync(kFull, h1, 1);
         if (j0 > P) {  // next stripe (rare): flush the finished rows' last words
             const int w = (step - 1) >> 4;
-            if (((step - 1) & 15) != 15 && k < S) {  // else stored (and cleared) last step
+            if (((step - 1) & 15) != 15 && r0ok) {  // else stored (and cleared) last step
                 const int sh = 30 - 2 * ((step - 1) & 15);
                 blk[(size_t)(w - g0) * 32] = make_uint2(acc0 >> sh, acc1 >> sh);
             }
@@ -277,7 +279,7 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
         acc1 = __funnelshift_r(acc1, d1, 2);
         if (st31 && (unsigned)(j0 - 2) < (unsigned)nlen) bH[j0 - 1] = n1;
         if ((step & 15) == 15) {  // uniform: the warp stores one 256-byte line
-            if (k < S) blk[(size_t)((step >> 4) - g0) * 32] = make_uint2(acc0, acc1);
+            if (r0ok) blk[(size_t)((step >> 4) - g0) * 32] = make_uint2(acc0, acc1);
             acc0 = acc1 = 0;
         }
         h0prev = hval<GAPZ, T>(h0);
@@ -290,7 +292,7 @@ IA_NW_ATTR int nw_align_t(const Pts &x, const NWParams &pr, const double *R, con
         ln1 = ln0;
         j0++;
     }
-    if (((total_steps - 1) & 15) != 15 && k < S) {  // flush the last rows' pending words
+    if (((total_steps - 1) & 15) != 15 && r0ok) {  // flush the last rows' pending words
         const int sh = 30 - 2 * ((total_steps - 1) & 15);
         blk[(size_t)(((total_steps - 1) >> 4) - g0) * 32] = make_uint2(acc0 >> sh, acc1 >> sh);
     }

@@ -34,6 +34,8 @@ def replay(plen, nlen):
     stored = {}  # address -> (stripe, row in stripe, step word, step of the store)
 
     def store(l, k, g0, gw, step):
+        if 64 * k + 2 * l + 1 > plen:  # the lane has no row inside the matrix: no store
+            return
         for r in (0, 1):
             a = (k * G + gw - g0) * 64 + 2 * l + r
             assert 0 <= a < size, (plen, nlen, l, k, gw)
@@ -105,6 +107,8 @@ def replay_bits(plen, nlen):
         acc = [0, 0]
 
         def store(w, vals):
+            if 64 * k + 2 * l + 1 > plen:  # no row inside the matrix: no store
+                return
             for r in (0, 1):
                 mem[(k * G + w - g0) * 64 + 2 * l + r] = vals[r]
 
