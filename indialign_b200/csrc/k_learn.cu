@@ -194,29 +194,40 @@ IA_DEV void window_features(const Pts &x, const uint8_t *Lp, const uint8_t *Ln, 
     warp_kabsch_window(x, ps, ns, flen, R, t);
     const double d0sq = I.d0 * I.d0, inv = 1.0 / d0sq;
     double sd2 = 0.0, stm = 0.0, sp = 0.0, sn = 0.0;
-    for (int i = lane; i < flen; i += 32) {
-        const double *p = x.P + 3 * (ps + i), *q = x.Q + 3 * (ns + i);
-        const double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
-        sd2 += d2;
-        stm += 1.0 / (1.0 + d2 * inv);
-        if (Lp) {
-            sp += Lp[ps + i] != 'L' ? 1.0 : 0.0;
-            sn += Ln[ns + i] != 'L' ? 1.0 : 0.0;
-        }
-    }
+    // one pass over pred residues i: the segment [ps, ps + flen) and the
+    // diagonal [lo, hi) pair i with native i + s (the segment lies on that
+    // diagonal), the same-index sum pairs i < ml with native i; each moved
+    // pred point is computed once for all three
     const int s = ns - ps;
     const int lo = s < 0 ? -s : 0, hi = plen < nlen - s ? plen : nlen - s;
     double dtm = 0.0, c1 = 0.0, c2 = 0.0, tm0 = 0.0;
-    for (int i = lo + lane; i < hi; i += 32) {
-        const double *p = x.P + 3 * i, *q = x.Q + 3 * (i + s);
-        const double d2 = dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]);
-        dtm += 1.0 / (1.0 + d2 * inv);
-        c1 += d2 < d0sq ? 1.0 : 0.0;
-        c2 += d2 < 4.0 * d0sq ? 1.0 : 0.0;
-    }
-    for (int i = lane; i < ml; i += 32) {
-        const double *p = x.P + 3 * i, *q = x.Q + 3 * i;
-        tm0 += 1.0 / (1.0 + dist2(R, t, p[0], p[1], p[2], q[0], q[1], q[2]) * inv);
+    const int i_end = hi > ml ? hi : ml;
+    for (int i = lane; i < i_end; i += 32) {
+        const double *p = x.P + 3 * i;
+        double mx, my, mz;
+        xform(R, t, p[0], p[1], p[2], mx, my, mz);
+        if (i >= lo && i < hi) {
+            const double *q = x.Q + 3 * (i + s);
+            const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            const double term = 1.0 / (1.0 + d2 * inv);
+            dtm += term;
+            c1 += d2 < d0sq ? 1.0 : 0.0;
+            c2 += d2 < 4.0 * d0sq ? 1.0 : 0.0;
+            if (i >= ps && i < ps + flen) {
+                sd2 += d2;
+                stm += term;
+                if (Lp) {
+                    sp += Lp[i] != 'L' ? 1.0 : 0.0;
+                    sn += Ln[i + s] != 'L' ? 1.0 : 0.0;
+                }
+            }
+        }
+        if (i < ml) {
+            const double *q = x.Q + 3 * i;
+            const double dx = mx - q[0], dy = my - q[1], dz = mz - q[2];
+            tm0 += 1.0 / (1.0 + (dx * dx + dy * dy + dz * dz) * inv);
+        }
     }
     sd2 = warp_sum(sd2);
     stm = warp_sum(stm);

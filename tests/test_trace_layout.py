@@ -251,3 +251,79 @@ def test_wavefront_fill_equals_row_by_row_fill(plen, nlen, gap, seed):
     d2, h2 = direct_fill(S, gap)
     assert d1 == d2
     assert h1 == h2
+
+
+def replay_fill_rows(S, gap, R):
+    """The wavefront fill with R rows per lane (stripes of 32R rows): row r
+    of a lane computes column j0 - r, its up and diagonal inputs are row
+    r-1's values from one and two steps earlier (row 0: the previous lane's
+    last row, by a shuffle, or the boundary row), a row's column-0 cell is
+    replaced by the boundary +0, and the period is max(nlen + R - 1, 32R).
+    Returns the (i, j) -> dir map and the plain H of the last row."""
+    plen, nlen = S.shape
+    RS = 32 * R
+    P = max(nlen + R - 1, RS)
+    nS = (plen + RS - 1) // RS
+    last_lane = ((plen - 1) % RS) // R
+    total = (nS - 1) * P + R * last_lane + R - 1 + nlen
+    bH = [0.0] * (nlen + 1)
+    st = [dict(k=0, j0=1 - R * l, i0=R * l + 1, h=[0.0] * R, hp=[0.0] * R, up0prev=0.0, ok=[False] * R,
+               st31=False, ld0=False) for l in range(32)]
+    dirs, last_row = {}, {}
+    hv = (lambda h: h) if gap == 0.0 else abs
+    for step in range(total):
+        ups = [st[l - 1]["h"][R - 1] if l > 0 else st[0]["h"][R - 1] for l in range(32)]
+        writes = []
+        for l in range(32):
+            c = st[l]
+            up0 = ups[l]
+            if c["j0"] > P:
+                c["j0"] -= P
+                c["k"] += 1
+                c["i0"] += RS
+            if c["j0"] == 1:
+                c["h"], c["hp"], c["up0prev"] = [0.0] * R, [0.0] * R, 0.0
+                c["ok"] = [c["k"] < nS and c["i0"] + r <= plen for r in range(R)]
+                c["st31"] = l == 31 and c["k"] + 1 < nS and c["ok"][R - 1]
+                c["ld0"] = c["k"] > 0 and c["ok"][0]
+            j0, i0 = c["j0"], c["i0"]
+            if l == 0:
+                up0 = bH[j0] if (c["ld0"] and 1 <= j0 <= nlen) else 0.0
+            new = []
+            for r in range(R):
+                a = min(i0 + r, plen) - 1
+                jc = min((j0 - r - 1) % (1 << 32), nlen - 1)
+                if r == 0:
+                    n, d = _cell(c["up0prev"], S[a, jc], up0, c["h"][0], gap)
+                else:
+                    n, d = _cell(c["hp"][r - 1], S[a, jc], c["h"][r - 1], c["h"][r], gap)
+                new.append(n)
+                i, j = i0 + r, j0 - r
+                if c["k"] < nS and i <= plen and 1 <= j <= nlen:
+                    dirs[(i, j)] = d
+                    if i == plen:
+                        last_row[j] = hv(n)
+            if c["st31"] and 1 <= j0 - (R - 1) <= nlen:
+                writes.append((j0 - (R - 1), new[R - 1]))
+            c["up0prev"] = hv(up0)
+            c["hp"] = [hv(v) for v in c["h"]]
+            c["h"] = [0.0 if (r >= 1 and j0 == r) else new[r] for r in range(R)]
+            c["j0"] += 1
+        for j, v in writes:
+            bH[j] = v
+    return dirs, last_row
+
+
+@pytest.mark.parametrize("R", [2, 4])
+@pytest.mark.parametrize("plen,nlen,gap,seed", [(3, 3, 0.0, 1), (7, 40, 0.0, 2), (64, 64, 0.0, 3),
+                                                (65, 70, 0.0, 4), (130, 65, -0.6, 5), (129, 63, -0.6, 6),
+                                                (200, 90, 0.0, 7), (140, 140, -1.0, 8), (300, 20, 0.0, 9),
+                                                (257, 130, -0.6, 10)])
+def test_wavefront_fill_with_r_rows_per_lane(plen, nlen, gap, seed, R):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    S = rng.integers(-2, 5, size=(plen, nlen)).astype(np.float64) / 4.0
+    d1, h1 = replay_fill_rows(S, gap, R)
+    d2, h2 = direct_fill(S, gap)
+    assert d1 == d2
+    assert h1 == h2
