@@ -114,8 +114,21 @@ static std::mutex g_pool_mu;
 static std::vector<Ctx *> g_pool;
 static std::once_flag g_attr_once[64];
 
+// Stream priority of a context serving `tag`: a length-bucket sub-batch (tag
+// = bucket + 1) gets a priority that grows with the bucket's lengths.  The
+// sub-batches of one call run side by side and the longest pairs are their
+// critical path, so their pending work is scheduled first whenever SMs free
+// up; whole batches (tag 0) get the default.
+static int stream_priority(int tag) {
+    int least = 0, greatest = 0;
+    if (tag <= 0 || cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess || greatest >= least)
+        return 0;
+    return std::max(greatest, least - (tag - 1) * std::max(1, (least - greatest) / 2));
+}
+
 // A pooled context of `device`, preferring one that last served the same
-// kind of batch (`tag`), so that its grow-only buffers already fit.
+// kind of batch (`tag`), so that its grow-only buffers already fit; a
+// context taken over from another tag gets a stream of this tag's priority.
 static int acquire(int device, Ctx **out, int tag = 0) {
     if (device < 0) CK(cudaGetDevice(&device));
     {
@@ -127,10 +140,19 @@ static int acquire(int device, Ctx **out, int tag = 0) {
                 if (g_pool[i]->tag == tag) break;
             }
         if (pick >= 0) {
-            *out = g_pool[pick];
-            (*out)->tag = tag;
+            Ctx *c = g_pool[pick];
             g_pool.erase(g_pool.begin() + pick);
             CK(cudaSetDevice(device));
+            if (c->tag != tag) {  // its stream is idle: the last call synchronized it
+                int prio = 0;
+                CK(cudaStreamGetPriority(c->stream, &prio));
+                if (prio != stream_priority(tag)) {
+                    CK(cudaStreamDestroy(c->stream));
+                    CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, stream_priority(tag)));
+                }
+            }
+            c->tag = tag;
+            *out = c;
             return INDIALIGN_OK;
         }
     }
@@ -138,7 +160,7 @@ static int acquire(int device, Ctx **out, int tag = 0) {
     Ctx *c = new Ctx();
     c->device = device;
     c->tag = tag;
-    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, stream_priority(tag)));
     CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     cudaError_t attr_err = cudaSuccess;
     std::call_once(g_attr_once[device & 63], [&]() {
