@@ -3,9 +3,9 @@
 Workload (default, learned16384): the learned-vs-plain configuration --
 16384 synthetic pairs, L ~ U(40,1000), sigma ~ U(0.5,14) A, random rigid
 transform, 5 % invalid residues per mask, lnorm = L, default NativeConfig.
-A step is one search call over a batch of --step-pairs pairs (2048: eight
+A step is one search call over a batch of --step-pairs pairs (4096: four
 steps cover the 16384 pairs; warm-up and timed steps take consecutive
-batches).
+batches, cycling through the workload).
 
   value    pairs/s of the LEARNED search (the rescue passes refine the
            ranker's top-8 candidates per pair, margin 0.02, 2 % audit), inputs
@@ -19,12 +19,13 @@ batches).
   e2e      the learned search through the C-ABI batch call with host
            buffers: host->device copies of the inputs and the device->host
            read of the results inside the timed region.
-  roofline the dominant kernel of the learned step (by summed device time):
-           algorithmic flops / its device time against the GPU's measured FP32
-           FMA peak (indialign_fp32_peak) -- seed bank: 55 FP32 flop per
-           residue visit; NW chains: 18 FP32 flop per NW cell + 55 FP64 flop
-           per Kabsch / detailed-search residue visit, the FP64 flops counted
-           twice (the FP64 rate is half the FP32 rate).
+  roofline the learned step's two hot kernels (`kernels`), and the larger
+           by summed device time as `kernel`: algorithmic flops / device time
+           against the GPU's measured FP32 FMA peak (indialign_fp32_peak) --
+           seed bank: 55 FP32 flop per residue visit; NW chains: 18 FP32 flop
+           per NW cell + 55 FP64 flop per Kabsch / detailed-search residue
+           visit, the FP64 flops counted twice (the FP64 rate is half the
+           FP32 rate).
   cpu_baseline  the reference's own build (oracle/_ref, OpenMP batch entry)
            on this host's cores: one batch call over a length-stratified
            sample of the timed pairs, two pairs per host thread.
@@ -330,7 +331,8 @@ def main():
     ap.add_argument("--workload", default="learned16384")
     ap.add_argument("--mode", default="learned", choices=["learned", "plain"],
                     help="search timed for `value`; with learned, the plain search is timed beside it")
-    ap.add_argument("--step-pairs", type=int, default=2048)
+    ap.add_argument("--step-pairs", type=int, default=4096,
+                    help="pairs per search call (default: 4 timed steps cover the 16384-pair workload once)")
     ap.add_argument("--top-k", type=int, default=8)
     ap.add_argument("--margin", type=float, default=0.02)
     ap.add_argument("--audit", type=float, default=0.02)
