@@ -91,7 +91,7 @@ def test_single_thread_reference_rate():
     assert r["same_pairs_all_cores"] > 0 and "shortest" in r["sample"]
 
 
-def test_compact_line_keeps_the_verdict_fields_in_a_short_line():
+def test_compact_line_keeps_the_key_fields_in_a_short_line():
     """stdout's line keeps the learned-vs-plain ratio and the per-pair TM
     change, the roofline, the CPU baseline, e2e and clocks, and stays well
     under a few-KB output tail even with the full record's breakdowns."""
