@@ -117,8 +117,8 @@ def main():
         with open(a.log, "w") as f:
             f.write("# Kernel-shape tuning of the length buckets\n\nCommand:\n\n```\npython -m "
                     f"indialign_b200.autotune --pairs {a.pairs} --mixed-pairs {a.mixed_pairs} "
-                    f"--repeats {a.repeats} --seed {a.seed} "
-                    "--out indialign_b200/tune_b200.txt --log profiles/autotune_b200.md\n```\n\n"
+                    f"--repeats {a.repeats} --seed {a.seed}"
+                    + (f" --out {a.out}" if a.out else "") + f" --log {a.log}\n```\n\n"
                     "Learned search (shipped ranker), wall time per synchronous call, minimum of the repeats.\n\n```\n")
             f.write("\n".join(lines) + "\n```\n")
 
