@@ -240,7 +240,7 @@ int indialign_nw_align(const double *d_smat, int np, int nn, double gap, int *d_
  * scratch lives in a fixed device array of about 1.1 MB that every GPU using
  * the library keeps until exit.  Limit: 1 <= np, nn <= 2048, else
  * INDIALIGN_E_INPUT.  The first call on a device looks the array up with
- * cudaGetSymbolAddress (make it before any stream capture).  All calls share
+ * cudaGetSymbolAddress.  All calls share
  * the array: calls whose work overlaps on the GPU race.  stream NULL is the
  * legacy default stream; the call returns after the stream synchronizes. */
 int indialign_nw_align_noalloc(const double *d_smat, int np, int nn, double gap, int *d_ap,

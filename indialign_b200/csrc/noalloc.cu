@@ -16,8 +16,7 @@
 // itself and writes every trace word it later reads, so no state carries over
 // from the previous call; the counters are never read.  The first call on a
 // device looks up the array's device address (cudaGetSymbolAddress) with
-// that device current; make that first call before any stream capture.  The
-// call returns after `stream` synchronizes.
+// that device current.  The call returns after `stream` synchronizes.
 #include <cuda_runtime.h>
 
 #include <mutex>
