@@ -73,6 +73,15 @@ FLOP_PER_VISIT = 55.0
 # records (13 doubles per item) and the staged point sets, which grow in
 # proportion to the visits.
 BANK_DRAM_BYTES_PER_VISIT = 511.1e6 / 13.084e9
+# DRAM bytes (read + write) of the NW chain kernel per NW cell, from the same
+# kind of capture of all eleven k_chain launches of one plain batch64 step
+# (`bench.py --workload batch64 --mode plain --steps 1 --warmup 0
+# --no-cpu-baseline --no-e2e --no-split`): 1.873 GB read + 20.290 GB written
+# over that step's 21.999 G NW cells.  Most of it is the chain body's stack
+# traffic around its out-of-line calls beside the 2-bit trace; the stack part
+# grows with the chain steps rather than the cells, so on longer matrices
+# the figure overstates the traffic.
+CHAIN_DRAM_BYTES_PER_CELL = 22.163e9 / 21.9986e9
 STAGES = ["seeds", "seed_bank", "ss", "gapless", "local_fragment", "threading_dp",
           "dense_local_fragment", "topk", "dp_refine", "offset_dp", "weighted", "total"]
 
@@ -507,7 +516,8 @@ def main():
         # both hot kernels, algorithmic FP32 flops over their event time
         # (FP64 chain visits counted at the FP64 half rate)
         per_kernel = {
-            "k_chain": (FLOP_PER_CELL * ctr[0] + 2.0 * FLOP_PER_VISIT * ctr[1], kern[0], None,
+            "k_chain": (FLOP_PER_CELL * ctr[0] + 2.0 * FLOP_PER_VISIT * ctr[1], kern[0],
+                        CHAIN_DRAM_BYTES_PER_CELL * ctr[0],
                         "k_chain (NW chains: score matrix + NW + Kabsch + refine)"),
             "k_bank": (FLOP_PER_VISIT * ctr[2], kern[1],
                        BANK_DRAM_BYTES_PER_VISIT * ctr[2] if BANK_DRAM_BYTES_PER_VISIT else None,
