@@ -333,6 +333,44 @@ class DeviceBatch:
         self.out = torch.zeros(self.n * 13, dtype=torch.float64, device="cuda")
 
 
+def roofline_record(kern, ctr, step_ms: float, peak: float, peak_source: str) -> dict:
+    """The bench line's `roofline` object from one step's mean kernel event
+    times (`kern`: k_chain, k_bank, ..., k_rank at index 4; ms) and work
+    counters (`ctr`: NW cells, FP64 chain residue visits, seed-bank residue
+    visits, ..., warp-cycle split at 8..11).  Both hot kernels are reported,
+    algorithmic FP32 flops over their event time (FP64 chain visits counted
+    at the FP64 half rate) against `peak` (TFLOP/s), with DRAM traffic per
+    step scaled from their captures; the top-level figures are the larger
+    kernel's."""
+    per_kernel = {
+        "k_chain": (FLOP_PER_CELL * ctr[0] + 2.0 * FLOP_PER_VISIT * ctr[1], kern[0],
+                    CHAIN_DRAM_BYTES_PER_CELL * ctr[0],
+                    "k_chain (NW chains: score matrix + NW + Kabsch + refine)"),
+        "k_bank": (FLOP_PER_VISIT * ctr[2], kern[1], BANK_DRAM_BYTES_PER_VISIT * ctr[2],
+                   "k_bank (seed x cutoff refine items)"),
+    }
+    top = "k_chain" if kern[0] >= kern[1] else "k_bank"
+    flops, kms, traffic, kname = per_kernel[top]
+    achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else None
+    both = {}
+    for nm, (fl, ms, tr, _) in per_kernel.items():
+        ach = fl / (ms / 1e3) / 1e12 if ms > 0 else None
+        both[nm] = {"ms_per_step": round(float(ms), 1), "achieved": ach,
+                    "frac": ach / peak if ach else None, "traffic": tr}
+    cyc = np.asarray(ctr[8:12], dtype=np.float64)
+    return {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None, "traffic": traffic,
+            "traffic_unit": "bytes per step (DRAM read + write of the kernel's launches)",
+            "peak_source": peak_source,
+            "kernel_ms_per_step": float(kms), "kernel_share": float(kms / step_ms),
+            "kernels": both,
+            "kernel_ms": {"k_chain": float(kern[0]), "k_bank": float(kern[1]), "k_rank": float(kern[4])},
+            "nw_cells_per_step": int(ctr[0]), "chain_visits_per_step": int(ctr[1]),
+            "bank_visits_per_step": int(ctr[2]),
+            "warp_cycle_split": dict(zip(["nw_fill", "traceback", "detailed", "kabsch"],
+                                         [float(x) for x in cyc / max(1.0, cyc.sum())]))}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,37 +550,9 @@ def main():
         kern = np.mean(lrn["kern"], 0)
         ctr = np.mean(lrn["ctr"], 0)
         step_ms = l_ms / args.steps
-        bound, peak, src = "fp32", ia.fp32_peak_tflops(local), "measured FP32 FMA rate (indialign_fp32_peak)"
-        # both hot kernels, algorithmic FP32 flops over their event time
-        # (FP64 chain visits counted at the FP64 half rate)
-        per_kernel = {
-            "k_chain": (FLOP_PER_CELL * ctr[0] + 2.0 * FLOP_PER_VISIT * ctr[1], kern[0],
-                        CHAIN_DRAM_BYTES_PER_CELL * ctr[0],
-                        "k_chain (NW chains: score matrix + NW + Kabsch + refine)"),
-            "k_bank": (FLOP_PER_VISIT * ctr[2], kern[1],
-                       BANK_DRAM_BYTES_PER_VISIT * ctr[2] if BANK_DRAM_BYTES_PER_VISIT else None,
-                       "k_bank (seed x cutoff refine items)"),
-        }
-        top = "k_chain" if kern[0] >= kern[1] else "k_bank"
-        flops, kms, traffic, kname = per_kernel[top]
-        achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else None
-        both = {}
-        for nm, (fl, ms, tr, _) in per_kernel.items():
-            ach = fl / (ms / 1e3) / 1e12 if ms > 0 else None
-            both[nm] = {"ms_per_step": round(float(ms), 1), "achieved": ach,
-                        "frac": ach / peak if ach else None, "traffic": tr}
-        cyc = ctr[8:12]
-        roofline = {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak if achieved else None, "traffic": traffic,
-                    "traffic_unit": "bytes per step (DRAM read + write of the kernel's launches)",
-                    "peak_source": f"{src} in this run",
-                    "kernel_ms_per_step": float(kms), "kernel_share": float(kms / step_ms),
-                    "kernels": both,
-                    "kernel_ms": {"k_chain": float(kern[0]), "k_bank": float(kern[1]), "k_rank": float(kern[4])},
-                    "nw_cells_per_step": int(ctr[0]), "chain_visits_per_step": int(ctr[1]),
-                    "bank_visits_per_step": int(ctr[2]),
-                    "warp_cycle_split": dict(zip(["nw_fill", "traceback", "detailed", "kabsch"],
-                                                 [float(x) for x in cyc / max(1.0, cyc.sum())]))}
+        peak = ia.fp32_peak_tflops(local)
+        roofline = roofline_record(kern, ctr, step_ms, peak,
+                                   "measured FP32 FMA rate (indialign_fp32_peak) in this run")
         # the library counts its stage launches (counter 7); the device entry
         # adds the input repack and the result export, the learned search the
         # MLP weight pack

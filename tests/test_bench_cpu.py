@@ -1,6 +1,6 @@
 """bench.py pieces that need no GPU: the reference arm (the reference build on
 the host cores) and its one-line JSON contract, rank gating under torchrun,
-the workload batching, and the clock-record parsing."""
+the workload batching, the clock-record parsing and the roofline record."""
 from __future__ import annotations
 
 import json
@@ -125,6 +125,29 @@ def test_compact_line_keeps_the_key_fields_in_a_short_line():
     assert c["cpu_baseline"]["cpu"] == "Xeon" and c["e2e"]["value"] == 1733.0
     assert c["rank"]["lists"] == sum(v["pairs"] for v in kinds.values())
     assert list(c)[:3] == ["metric", "value", "unit"]
+
+
+def test_roofline_record_from_counters():
+    """Both hot kernels' figures come from the step's work counters and event
+    times: algorithmic flops per unit x units / time against the peak, and
+    DRAM traffic scaled from each kernel's capture by the same units; the
+    top-level figures are the larger kernel's."""
+    kern = [600.0, 750.0, 0.0, 0.0, 120.0]        # ms per step: k_chain, k_bank, ..., k_rank
+    ctr = [2.0e10, 1.0e9, 2.5e11, 0, 0, 0, 0, 150, 3.0, 1.0, 0.0, 0.0]
+    r = bench.roofline_record(kern, ctr, 1400.0, 67.5, "measured")
+    bank = 55.0 * 2.5e11 / 0.75 / 1e12
+    chain = (18.0 * 2.0e10 + 2 * 55.0 * 1.0e9) / 0.6 / 1e12
+    assert r["kernel"].startswith("k_bank") and r["achieved"] == pytest.approx(bank)
+    assert r["frac"] == pytest.approx(bank / 67.5) and r["kernel_share"] == pytest.approx(750 / 1400)
+    assert r["traffic"] == pytest.approx(bench.BANK_DRAM_BYTES_PER_VISIT * 2.5e11)
+    k = r["kernels"]
+    assert k["k_chain"]["achieved"] == pytest.approx(chain)
+    assert k["k_chain"]["traffic"] == pytest.approx(bench.CHAIN_DRAM_BYTES_PER_CELL * 2.0e10)
+    assert 1.0 < bench.CHAIN_DRAM_BYTES_PER_CELL < 1.02 and 0.03 < bench.BANK_DRAM_BYTES_PER_VISIT < 0.05
+    assert r["warp_cycle_split"]["nw_fill"] == pytest.approx(0.75)
+    # the plain step: the chain kernel is the larger one
+    r2 = bench.roofline_record([6000.0, 10.0, 0, 0, 0], ctr, 7000.0, 67.5, "measured")
+    assert r2["kernel"].startswith("k_chain") and r2["traffic"] == k["k_chain"]["traffic"]
 
 
 def test_reference_arm_fills_the_host():
