@@ -318,6 +318,8 @@ int launch_gemm_tc(const uint16_t *A, int lda, int a_mn, const uint16_t *B, int 
     if ((reinterpret_cast<uintptr_t>(A) & 15) || (reinterpret_cast<uintptr_t>(B) & 15)) return -1;
     if (a_mn ? (M > kTcBM || lda < M) : lda < K) return -1;  // an MN-major A is one 128-row tile
     if (b_mn ? ldb < N : ldb < K) return -1;
+    // output rows may not overlap, and the split-K sum indexes M x N in int
+    if (ldc < (c_trans ? M : N) || (long long)M * N > 0x7fffffffLL) return -1;
     const int nmma = nmma_of(N, b_mn);
     CUtensorMap ma, mb;
     const bool okA = a_mn ? make_map(&ma, A, M, K, lda, 64, kTcBK) : make_map(&ma, A, K, M, lda, kTcBK, kTcBM);

@@ -123,6 +123,28 @@ def test_padded_entry_rejects_bad_lengths_before_device_work():
     assert rc == -4
 
 
+def test_gemm_rejects_bad_arguments_before_device_work():
+    """indialign_gemm_bf16 checks shapes, strides and alignment on the host
+    before its first CUDA call: each case returns INDIALIGN_E_INPUT."""
+    lib = ia.load()
+    p = 1 << 12  # 16-byte aligned, never dereferenced
+    cases = [
+        # lda, a_mn, ldb, b_mn, m, n, k, ldc, c_trans, a_ptr
+        (64, 0, 64, 0, 128, 300, 64, 300, 0, p),        # n > 256
+        (60, 0, 64, 0, 128, 64, 64, 64, 0, p),          # lda not a multiple of 8
+        (64, 1, 64, 0, 200, 64, 64, 64, 0, p),          # MN-major A beyond one 128-row tile
+        (32, 0, 64, 0, 128, 64, 64, 64, 0, p),          # K-major lda < k
+        (64, 0, 64, 0, 128, 64, 64, 64, 0, p + 2),      # operand not 16-byte aligned
+        (64, 0, 64, 0, 128, 64, 64, 63, 0, p),          # ldc < n: output rows overlap
+        (64, 0, 64, 0, 128, 64, 64, 127, 1, p),         # transposed store, ldc < m
+        (64, 0, 64, 0, 1 << 24, 256, 64, 256, 0, p),    # m x n beyond int range
+    ]
+    for lda, a_mn, ldb, b_mn, m, n, k, ldc, c_trans, a in cases:
+        rc = lib.indialign_gemm_bf16(a, lda, a_mn, p, ldb, b_mn, m, n, k, p, ldc, c_trans, None, 1, None)
+        assert rc == -4, (lda, a_mn, m, n, k, ldc, c_trans, rc)
+        assert "gemm_bf16" in ia.last_error()
+
+
 def test_batch_options_layout_matches_header(tmp_path):
     """The Python mirror of IndialignBatchOptions has the C struct's size and
     field offsets (a C program compiled against the header prints them)."""
