@@ -21,8 +21,11 @@
 //             stage's reduction keeps the reference's first-max rule).
 //   k_audit   audited pairs: did the top-k contain the best refined score?
 //   training  forward with saved activations, MSE + pairwise ranking loss,
-//             backward through BF16 tensor-core GEMMs (split-K, fixed-order
-//             sums), Adam on FP32 master weights.
+//             backward: the three weight / activation products on the
+//             tcgen05 tensor cores (k_gemm_tc in k_tcgen05.cu: TMA-staged
+//             BF16 operands, TMEM accumulators, split-K with a fixed-order
+//             sum), the bias and head gradients here over row blocks summed
+//             in block order; Adam on FP32 master weights.
 #include <cuda_bf16.h>
 
 #include "dmath.cuh"
