@@ -333,6 +333,14 @@ class DeviceBatch:
         self.out = torch.zeros(self.n * 13, dtype=torch.float64, device="cuda")
 
 
+def plain_steps(batches, steps: int, step_pairs: int) -> int:
+    """Timed steps of the plain comparison leg: enough step_pairs-pair calls
+    to cover the workload's distinct pairs once (the batches cycle through
+    them), at most the learned leg's `steps` and at least one."""
+    n_distinct = len({id(p) for b in batches for p in b})
+    return max(1, min(steps, -(-n_distinct // max(step_pairs, 1))))
+
+
 def roofline_record(kern, ctr, step_ms: float, peak: float, peak_source: str) -> dict:
     """The bench line's `roofline` object from one step's mean kernel event
     times (`kern`: k_chain, k_bank, ..., k_rank at index 4; ms) and work
@@ -504,8 +512,7 @@ def main():
         # pair's results do not change between calls), after min(W, 3)
         # warm-up steps: its throughput and the learned search's TM change
         # on every distinct timed pair
-        n_distinct = len({id(p) for b in batches for p in b})
-        p_steps = max(1, min(args.steps, -(-n_distinct // max(args.step_pairs, 1))))
+        p_steps = plain_steps(batches, args.steps, args.step_pairs)
         pl = run_mode(False, steps=p_steps, warmup=min(args.warmup, 3))
         p_n = sum(dev[args.warmup + k].n for k in range(p_steps))
         p_ms = max_over_ranks(float(np.sum(pl["ms"])))

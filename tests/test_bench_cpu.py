@@ -61,6 +61,16 @@ def test_workload_batches():
         bench.workload("nonsense", 4, 1)
 
 
+def test_plain_leg_covers_the_distinct_pairs_once():
+    # 3 warm-up + 4 timed batches of 4 cycling through 12 pairs: 3 plain steps
+    batches, _ = bench.workload("batch12", 4, 7)
+    assert bench.plain_steps(batches, 4, 4) == 3
+    timed = [id(p) for b in batches[3:3 + 3] for p in b]
+    assert len(set(timed)) == 12 and len(timed) == 12  # the first 3 timed batches hold every pair once
+    assert bench.plain_steps(batches, 2, 4) == 2       # never more than the learned leg's steps
+    assert bench.plain_steps(batches[:1], 4, 64) == 1
+
+
 def test_clock_summary_parsing():
     c = bench.Clocks(0)
     rows = ["0, 1965, 1965, 640.5, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
