@@ -22,6 +22,10 @@ change of the final TM-score against the reference:
   bank32f     bank32 in the seed-bank kernel's explicit FP32 operation
               sequence (fused transform, d2 and moment products; the item
               score's term 1 / fma(d2, 1/d0^2, 1))
+  bank32p     bank32f with the cutoff passes' moments summed in two FP32
+              partial sets (even / odd residues) combined in FP64: the
+              rounding of an accumulate by paired FP32 instructions (an
+              estimate for a possible kernel change, not the kernel's form)
   smat32      only the score-matrix entries of dp_refine and of the SS +
               distance NW lowered, in the NW-chain kernel's form: the moved
               pred point rounded to FP32, FP32 difference, d2, cutoff test and
@@ -515,6 +519,59 @@ def _bank32f(src: str) -> str:
     return _sub(s, BANK32F_OLD_TERM, BANK32F_NEW_TERM)
 
 
+BANK32P_OLD_LOOP = '''        mom32 m;
+        int c = 0;
+        memset(&m, 0, sizeof m);
+        rt32(R, t, Rf, tf);
+        for (int i = 0; i < N; i++) {
+            if (!v[i]) continue;
+            if (d2_32(P + 3 * i, Q + 3 * i, Rf, tf) <= cut2) { m32_add(&m, P + 3 * i, Q + 3 * i); c++; }
+        }
+        if (c >= 3) m32_kabsch(&m, R, t);'''
+BANK32P_NEW_LOOP = '''        mom32 m, mo;
+        int c = 0;
+        memset(&m, 0, sizeof m);
+        memset(&mo, 0, sizeof mo);
+        rt32(R, t, Rf, tf);
+        for (int i = 0; i < N; i++) {
+            if (!v[i]) continue;
+            if (d2_32(P + 3 * i, Q + 3 * i, Rf, tf) <= cut2) {
+                m32_add((i & 1) ? &mo : &m, P + 3 * i, Q + 3 * i);
+                c++;
+            }
+        }
+        if (c >= 3) m32_kabsch2(&m, &mo, R, t);'''
+BANK32P_MARKER = "static float d2_32(const float *p, const float *q, const float *Rf, const float *tf) {"
+BANK32P_KABSCH2 = r"""/* Kabsch from two FP32 partial moment sets (even and odd residues),
+   combined in FP64 */
+static void m32_kabsch2(const mom32 *a, const mom32 *b, double *R, double *t) {
+    double sp[3], sq[3], cP[3], cQ[3], H[3][3], w = (double)(a->w + b->w);
+    if (a->w + b->w < 3) { memcpy(R, IDENT, sizeof IDENT); t[0] = t[1] = t[2] = 0; return; }
+    for (int d = 0; d < 3; d++) {
+        sp[d] = (double)a->sp[d] + (double)b->sp[d];
+        sq[d] = (double)a->sq[d] + (double)b->sq[d];
+        cP[d] = sp[d] / w;
+        cQ[d] = sq[d] / w;
+    }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) H[r][c] = ((double)a->h[3 * r + c] + (double)b->h[3 * r + c]) - sp[r] * cQ[c];
+    cov_to_rotation((const double(*)[3])H, R);
+    for (int d = 0; d < 3; d++) t[d] = cQ[d] - (cP[0] * R[d] + cP[1] * R[3 + d] + cP[2] * R[6 + d]);
+}
+"""
+
+
+def _bank32p(src: str) -> str:
+    """bank32f with the cutoff passes' moments accumulated in two FP32
+    partial sets, even and odd residue indices, combined in FP64 before the
+    eigen-solve: the rounding of a seed-bank accumulate that adds the two
+    residues of a staged pair with paired FP32 instructions (an estimate for
+    that kernel change; the kernel does not do this)."""
+    s = _bank32f(src)
+    s = _sub(s, BANK32P_MARKER, BANK32P_KABSCH2 + BANK32P_MARKER)
+    return _sub(s, BANK32P_OLD_LOOP, BANK32P_NEW_LOOP)
+
+
 def _bank32(src: str) -> str:
     """Only the seed banks lowered, in the GPU seed-bank kernel's form."""
     marker = "/* ---- seeds (indialign_c/seeds.h)"
@@ -572,6 +629,7 @@ def variant_sources(src: str) -> dict[str, str]:
     out["bank32"] = _bank32(src)
     out["qcp64"] = _qcp64(src)
     out["bank32f"] = _bank32f(src)
+    out["bank32p"] = _bank32p(src)
     out["smat32"] = _smat32(src)
     out["dp32"] = _dp32(src)
     return out

@@ -21,7 +21,7 @@ from indialign_b200 import workloads as W  # noqa: E402
 def test_variant_sources_apply():
     src = open(os.path.join(ROOT, "oracle", "indialign_oracle.c")).read()
     out = ps.variant_sources(src)
-    assert sorted(out) == ["bank32", "bank32f", "dist32", "dp32", "kahan32", "plain32", "qcp64", "raw32",
+    assert sorted(out) == ["bank32", "bank32f", "bank32p", "dist32", "dp32", "kahan32", "plain32", "qcp64", "raw32",
                            "raw32c", "smat32"]
     for name, s in out.items():
         assert s != src, name
