@@ -1,7 +1,7 @@
 """Precision study of the search (design evidence; test infrastructure only).
 
 Rebuilds the C oracle (indialign_oracle.c) with its arithmetic lowered to
-FP32 in six ways, and once with its eigen-solve replaced; runs each
+FP32 in several ways, and once with its eigen-solve replaced; runs each
 variant's batch search beside the reference build (_ref/libindialign_ref.so),
 rescores every variant's final (R, t) in FP64 with the reference's own
 tm_score_no_d8 (_ref/libindialign_ref_stages.so) and prints the per-pair
